@@ -1,0 +1,348 @@
+#!/usr/bin/env python
+"""Benchmark of the fused filter -> join -> group-by path on B200.
+
+Workload (default, "join_group"): build side 10M rows (pk = permutation of
+[0,10M), cat U[0,1000)), probe side 100M rows (fk U[0,12M), qty U[1,100],
+price U[1,500)); filter qty > 10, inner join fk = pk, group by cat with
+SUM(price), COUNT -- one td_execute of one DAG (teide_b200's single-graph
+filter -> join -> group form).  A step is one such query.  Seeded synthetic
+data; inputs (2.56 GB) are larger than L2, so no flush is needed between steps.
+
+  value  rows/s of probe rows with both tables resident in HBM (td_gpu_pin)
+  e2e    the same query from host tables: every step uploads both tables
+         (page-locked host memory) and reads the result back
+  roofline  the fused probe + aggregate kernel: algorithmic bytes per launch
+         (24 B per probe row: fk, qty, price) / its CUDA-event duration
+
+Other workloads (--workload): "group_radix" (200M rows, Zipf keys over 2^24,
+filter v1 > 0, COUNT/SUM/MIN/MAX/AVG) and "readme_group" (10M rows, filter
+flag == 0, group by region, SUM(amount)).
+
+--impl reference runs Teide's own CPU engine (compiled from its sources into
+oracle/_ref/) on a bounded sample of the same workload per step, with every
+host thread.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "fused filter/join/group-by rows/s & %HBM peak; served q/s + p99 vs plain"
+REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libteide_ref.so")
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def profile_traffic(name):
+    """Per-launch DRAM bytes from the committed ncu summary, if present."""
+    p = os.path.join(ROOT, "profiles", name)
+    if not os.path.exists(p):
+        return None
+    m = re.search(r"traffic_per_launch_bytes\s*=\s*([0-9.eE+]+)", open(p).read())
+    return float(m.group(1)) if m else None
+
+
+class Clocks:
+    """Samples SM clocks and throttle reasons with nvidia-smi while running."""
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---- workloads through the td.h API ------------------------------------------------
+
+def make_tables(td, workload, rank, device):
+    from teide_b200 import workloads
+    if workload == "join_group":
+        b, p = workloads.config3(seed=3 + 1000 * rank, device=device)
+        bt, pt = td.table(b), td.table(p)
+        return {"build": bt, "probe": pt}, len(p["fk"]), 16 * len(b["pk"]) + 24 * len(p["fk"]), 24 * len(p["fk"])
+    if workload == "group_radix":
+        c = workloads.config2(seed=2 + 1000 * rank, device=device)
+        t = td.table(c)
+        return {"t": t}, len(c["key"]), 24 * len(c["key"]), 24 * len(c["key"])
+    c = workloads.config1(seed=1 + 1000 * rank)
+    t = td.table(c)
+    return {"t": t}, len(c["flag"]), 24 * len(c["flag"]), 24 * len(c["flag"])
+
+
+def run_query(td, workload, tabs):
+    from gpu_pipelines import fused_join_group, readme_group
+    from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
+    if workload == "join_group":
+        return fused_join_group(td, tabs["build"], tabs["probe"], ("qty", "gt", 10), "fk", "pk", ["cat"],
+                                [(OP_SUM, "price"), (OP_COUNT, "price")])
+    if workload == "group_radix":
+        return readme_group(td, tabs["t"], ("v1", "gt", 0), ["key"],
+                            [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")])
+    return readme_group(td, tabs["t"], ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+
+
+def stats_of(td):
+    import ctypes as C
+
+    class St(C.Structure):
+        _fields_ = [("h2d", C.c_uint64), ("d2h", C.c_uint64), ("calls", C.c_uint64), ("live", C.c_uint64),
+                    ("peak", C.c_uint64), ("gm", C.c_int32), ("jm", C.c_int32), ("fused", C.c_int32),
+                    ("pad", C.c_int32)]
+    s = St()
+    td.lib.td_gpu_last_stats(C.byref(s))
+    return s
+
+
+# ---- CPU reference ---------------------------------------------------------------------
+
+def reference_sample(workload, scale_rows):
+    """Teide's CPU engine on a bounded sample of the workload: returns
+    (seconds per query, rows per query, description)."""
+    from gpu_pipelines import join_then_group, two_graph_group
+    from teide_b200 import workloads
+    from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM, Td
+    td = Td(REF_LIB)
+    if workload == "join_group":
+        b, p = workloads.config3(n_build=10_000_000, n_probe=scale_rows, seed=33)
+        bt, pt = td.table(b), td.table(p)
+
+        def q():
+            join_then_group(td, bt, pt, ("qty", "gt", 10), "fk", "pk", ["cat"],
+                            [(OP_SUM, "price"), (OP_COUNT, "price")])
+        desc = f"build 10M rows + probe {scale_rows / 1e6:g}M rows per query (probe side sampled from 100M)"
+    elif workload == "group_radix":
+        c = workloads.config2(n=scale_rows, seed=32)
+        t = td.table(c)
+
+        def q():
+            two_graph_group(td, t, ("v1", "gt", 0), ["key"],
+                            [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")])
+        desc = f"{scale_rows / 1e6:g}M of 200M rows per query"
+    else:
+        c = workloads.config1(n=scale_rows, seed=31)
+        t = td.table(c)
+
+        def q():
+            two_graph_group(td, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+        desc = f"{scale_rows / 1e6:g}M rows per query"
+    return td, q, desc
+
+
+def reference_arm(args):
+    if int(os.environ.get("RANK", "0")) != 0:
+        return
+    if not os.path.exists(REF_LIB):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libteide_ref.so not built"}))
+        return
+    rows = {"join_group": 10_000_000, "group_radix": 20_000_000, "readme_group": 10_000_000}[args.workload]
+    td, q, desc = reference_sample(args.workload, rows)
+    for _ in range(args.warmup):
+        q()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        q()
+    dt = (time.perf_counter() - t0) / args.steps
+    v = rows / dt
+    cores = os.cpu_count()
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "rows/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+        "config": {"workload": args.workload, "sample": desc},
+        "cpu_baseline": {"value": v, "unit": "rows/s", "cores": cores, "kind": "reference", "sample": desc},
+        "e2e": {"value": v, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+# ---- GPU arm -------------------------------------------------------------------------------
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="teide_b200", choices=["teide_b200", "reference"])
+    ap.add_argument("--workload", default="join_group", choices=["join_group", "group_radix", "readme_group"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    os.environ["TD_GPU_DEVICE"] = str(local)
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    import teide_b200
+    td = teide_b200.load()
+    L = td.lib
+    L.tdg_set_timing.argtypes = [__import__("ctypes").c_int32]
+    L.tdg_last_main_ms.restype = __import__("ctypes").c_float
+    L.tdg_last_build_ms.restype = __import__("ctypes").c_float
+    L.tdg_launch_count.restype = __import__("ctypes").c_uint64
+    L.td_gpu_pin.argtypes = [__import__("ctypes").c_void_p]
+    L.td_gpu_unpin.argtypes = [__import__("ctypes").c_void_p]
+    L.tdg_set_timing(1)
+
+    tabs, rows, alg_bytes, main_bytes = make_tables(td, args.workload, rank, "cuda")
+    torch.cuda.empty_cache()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- resident: tables pinned in HBM ----
+    for t in tabs.values():
+        st = L.td_gpu_pin(t)
+        if st:
+            raise RuntimeError(f"td_gpu_pin failed: {st}")
+    for _ in range(args.warmup):
+        run_query(td, args.workload, tabs)
+    barrier()
+    l0 = L.tdg_launch_count()
+    main_ms, build_ms = [], []
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record()
+        for _ in range(args.steps):
+            run_query(td, args.workload, tabs)
+            main_ms.append(L.tdg_last_main_ms())
+            build_ms.append(L.tdg_last_build_ms())
+        ev1.record()
+        torch.cuda.synchronize()
+    elapsed = ev0.elapsed_time(ev1) / 1e3
+    launches = L.tdg_launch_count() - l0
+    s_res = stats_of(td)
+    barrier()
+    elapsed = max_over_ranks(elapsed)
+    value = rows * world * args.steps / elapsed
+
+    # ---- end to end: host tables, uploads inside every step ----
+    for t in tabs.values():
+        L.td_gpu_unpin(t)
+    L.td_gpu_trim()
+    e2e_steps = args.e2e_steps or args.steps
+    run_query(td, args.workload, tabs)          # page-locks the host columns once
+    barrier()
+    ev0.record()
+    for _ in range(e2e_steps):
+        run_query(td, args.workload, tabs)
+    ev1.record()
+    torch.cuda.synchronize()
+    e2e_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    s_e2e = stats_of(td)
+    e2e_value = rows * world * e2e_steps / e2e_elapsed
+
+    hbm, peak_kind = peaks()
+    mean_main = sum(main_ms) / len(main_ms) if main_ms else 0.0
+    achieved = main_bytes / (mean_main / 1e3) / 1e9 if mean_main > 0 else None
+    prof = {"join_group": "fused_join_group_cfg3.md", "group_radix": "group_radix_cfg2.md",
+            "readme_group": "readme_group_cfg1.md"}[args.workload]
+    line = {
+        "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+        "config": {"workload": args.workload, "rows_per_gpu_per_step": rows,
+                   "algorithmic_bytes_per_step": alg_bytes, "l2": "inputs larger than L2 (no flush)",
+                   "tables": "resident in HBM (td_gpu_pin)", "parallelism": f"replicas{world}"},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None, "traffic": profile_traffic(prof),
+                     "kernel": "k_group<fused probe + aggregate>", "bytes_per_launch": main_bytes,
+                     "mean_launch_ms": mean_main, "peak_source": peak_kind,
+                     "step_frac": alg_bytes / (elapsed / args.steps) / 1e9 / hbm,
+                     "build_ms": (sum(build_ms) / len(build_ms)) if build_ms and build_ms[0] else None},
+        "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": int(s_e2e.h2d),
+                "d2h_bytes_per_step": int(s_e2e.d2h), "steps": e2e_steps},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(),
+        "resident_h2d_bytes_per_step": int(s_res.h2d),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
+        rows_s = {"join_group": 10_000_000, "group_radix": 20_000_000, "readme_group": 10_000_000}[args.workload]
+        rtd, q, desc = reference_sample(args.workload, rows_s)
+        q()
+        t0 = time.perf_counter()
+        n = 0
+        while n < 3 or time.perf_counter() - t0 < 10:
+            q()
+            n += 1
+        dt = (time.perf_counter() - t0) / n
+        line["cpu_baseline"] = {"value": rows_s / dt, "unit": "rows/s", "cores": os.cpu_count(),
+                                "kind": "reference", "sample": desc + f", median of {n} runs"}
+    if rank == 0:
+        print(json.dumps(line))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

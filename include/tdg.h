@@ -1,0 +1,253 @@
+/*
+ * tdg.h -- C ABI of the sm_100a kernels behind td_execute.
+ *
+ * Plain C: device pointers, sizes, status codes and an opaque stream handle
+ * (a cudaStream_t passed as void*).  No C++ or torch types cross this line.
+ * The host executor (teide_b200/csrc/host/exec.c) lowers a Teide DAG into
+ * these calls; tests and the benchmark call them directly through ctypes.
+ *
+ * Each entry point replaces one executor loop of Teide's CPU engine
+ * (src/ops/exec.c in TeideDB/teide); the replaced lines are cited beside it.
+ * Status codes are td_err_t values (0 = ok).
+ *
+ * Memory: the caller owns every buffer.  Functions that need scratch memory
+ * come with a *_plan call that reports the bytes required; the caller passes
+ * a device buffer of at least that size as `ws`.  Nothing here allocates
+ * device memory except the tdg_*_static entry point documented at its
+ * declaration, which allocates nothing at all.
+ */
+#ifndef TDG_H
+#define TDG_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t tdg_status;
+
+/* A device-resident column: element data in Teide's td_t layout (dense,
+ * element size from the type tag, SYM width from attrs). */
+typedef struct tdg_col {
+    const void* data;
+    int8_t      type;      /* TD_I64, TD_F64, TD_I32, TD_SYM, ... */
+    uint8_t     attrs;     /* TD_SYM_W* for TD_SYM */
+    uint8_t     side;      /* join/group inputs: 0 = probe (left) row, 1 = build (right) row */
+    uint8_t     pad[5];
+} tdg_col;
+
+/* ---- expression programs --------------------------------------------------
+ * A predicate or computed value is a straight-line program of at most
+ * TDG_MAX_INS instructions; instruction k writes register k.  Values are I64
+ * or F64 (kind 0 / 1) as in Teide's expression VM (exec.c:760-918): columns
+ * load as I64 unless F64, mixed comparisons and arithmetic promote to F64,
+ * DIV always yields F64, comparisons and AND/OR/NOT yield 0/1 as I64. */
+enum {
+    TDG_X_COL = 1,   /* imm = column index into cols[]          */
+    TDG_X_CONST,     /* imm = value bits (I64, or F64 bits)      */
+    TDG_X_EQ, TDG_X_NE, TDG_X_LT, TDG_X_LE, TDG_X_GT, TDG_X_GE,
+    TDG_X_AND, TDG_X_OR, TDG_X_NOT,
+    TDG_X_ADD, TDG_X_SUB, TDG_X_MUL, TDG_X_DIV, TDG_X_MOD,
+    TDG_X_NEG, TDG_X_ABS, TDG_X_MIN2, TDG_X_MAX2,
+    TDG_X_TOF64, TDG_X_TOI64
+};
+#define TDG_MAX_INS   24
+#define TDG_MAX_XCOLS 8
+
+typedef struct tdg_ins {
+    uint8_t op;        /* TDG_X_* */
+    uint8_t a, b;      /* source registers */
+    uint8_t kind;      /* result kind: 0 = I64, 1 = F64 */
+    uint8_t pad[4];
+    int64_t imm;
+} tdg_ins;
+
+typedef struct tdg_expr {
+    int32_t n_ins;
+    int32_t n_cols;
+    int32_t out;       /* result register */
+    int32_t pad;
+    tdg_col cols[TDG_MAX_XCOLS];
+    tdg_ins ins[TDG_MAX_INS];
+} tdg_expr;
+
+/* ---- basic services --------------------------------------------------------- */
+
+/* min and max over n rows of an integer-class column, written as two int64
+ * to d_out[0..1] (INT64_MAX / INT64_MIN when n == 0).  Feeds the
+ * direct-array decision of exec_group (exec.c:5970-6010, minmax_scan_fn
+ * 4544-4604). */
+tdg_status tdg_minmax(tdg_col col, int64_t n, int64_t* d_out, void* stream);
+
+/* Evaluate `e` over n rows into a dense column `out` of kind 0 (int64),
+ * 1 (double) or 2 (bool bytes).  Replaces expr_eval_full (exec.c:1254-1273). */
+tdg_status tdg_eval(const tdg_expr* e, int64_t n, void* out, int32_t out_kind, void* stream);
+
+/* ---- selection (filter) -----------------------------------------------------
+ * A row is selected when `pred` (may be NULL) is non-zero and, if `sel_in` is
+ * given, its bit in that TD_SEL bit array is set. */
+
+/* TD_SEL block body on the device for n rows: bits[ceil(n/64)],
+ * seg_flags[ceil(n/1024)], seg_popcnt[ceil(n/1024)] and total (one int64).
+ * Replaces expr_eval_full + td_sel_from_pred + td_sel_recompute
+ * (exec.c:11717-11731, sel.c:77-161). */
+tdg_status tdg_select_bitmap(int64_t n, const tdg_expr* pred, const uint64_t* sel_in,
+                             uint64_t* bits, uint8_t* seg_flags, uint16_t* seg_popcnt,
+                             int64_t* d_total, void* stream);
+
+/* Stable compaction of the selected rows of n_cols columns.  Two calls:
+ * tdg_select_count fills ws (tdg_select_ws_bytes(n) bytes) and writes the
+ * number of selected rows to d_count; tdg_select_gather then writes the
+ * selected rows, in row order, to dst[c] (element size of src[c]).
+ * Replaces exec_filter / sel_compact / multi_gather_fn (exec.c:2065-2224,
+ * 2328-2480, 1852-1899). */
+size_t     tdg_select_ws_bytes(int64_t n);
+tdg_status tdg_select_count(int64_t n, const tdg_expr* pred, const uint64_t* sel_in,
+                            void* ws, int64_t* d_count, void* stream);
+tdg_status tdg_select_gather(int64_t n, const tdg_expr* pred, const uint64_t* sel_in,
+                             const void* ws, int32_t n_cols, const tdg_col* src,
+                             void* const* dst, void* stream);
+
+/* ---- group-by ----------------------------------------------------------------
+ * Keys and aggregate inputs are columns (side 0 for a plain group-by).
+ * Aggregates: OP_SUM, OP_COUNT, OP_MIN, OP_MAX, OP_AVG (td.h opcodes).
+ * Output: one row per non-empty group; key columns keep their element type,
+ * SUM is I64 (F64 for F64 input), COUNT I64, AVG F64, MIN/MAX the input
+ * type class (I64 or F64) -- emit_agg_columns, exec.c:4632-4773.
+ * Integer SUM wraps (two's complement) exactly like the CPU loops. */
+#define TDG_MAX_KEYS 8
+#define TDG_MAX_AGGS 8
+
+typedef struct tdg_agg {
+    int32_t op;
+    int32_t pad;
+    tdg_col in;        /* ignored for OP_COUNT */
+} tdg_agg;
+
+typedef struct tdg_group_desc {
+    int64_t nrows;
+    int32_t n_keys;
+    int32_t n_aggs;
+    tdg_col keys[TDG_MAX_KEYS];
+    tdg_agg aggs[TDG_MAX_AGGS];
+    /* key statistics: when have_range is set, key k lies in
+     * [key_min[k], key_max[k]] for every row (from tdg_minmax or table
+     * statistics).  Enables the direct-array method. */
+    int32_t have_range;
+    int32_t pad;
+    int64_t key_min[TDG_MAX_KEYS];
+    int64_t key_max[TDG_MAX_KEYS];
+} tdg_group_desc;
+
+enum { TDG_GROUP_DIRECT = 1, TDG_GROUP_HASH = 2 };
+
+typedef struct tdg_group_plan {
+    int32_t method;        /* TDG_GROUP_DIRECT or TDG_GROUP_HASH */
+    int32_t smem;          /* 1 when accumulators are privatized in shared memory */
+    int64_t n_slots;       /* direct-array slots or hash-table capacity */
+    int64_t max_groups;    /* capacity each output column must have */
+    size_t  ws_bytes;      /* scratch the run needs */
+} tdg_group_plan;
+
+typedef struct tdg_group_out {
+    void*    keys[TDG_MAX_KEYS];   /* max_groups elements of the key's type */
+    void*    aggs[TDG_MAX_AGGS];   /* max_groups 8-byte values */
+    int64_t* d_n_groups;           /* one int64: groups written */
+} tdg_group_out;
+
+/* Choose the method and size the scratch for a group-by.  `hint_groups` is
+ * an upper bound on the number of groups if the caller knows one (else 0).
+ * Replaces exec_group's dispatch (exec.c:5542-6879: DA at 5948-6404,
+ * radix hash table at 6406-6667). */
+tdg_status tdg_group_plan_make(const tdg_group_desc* d, int64_t hint_groups,
+                               tdg_group_plan* plan);
+
+/* Run a fused select + group-by over d->nrows rows and emit the groups.
+ * Direct arrays emit in ascending composite-key order; the hash method emits
+ * in table order.  Returns TD_ERR_RANGE if the hash table overflowed (the
+ * caller re-plans with a larger hint) and TD_ERR_DOMAIN if a key fell outside
+ * the declared range. */
+tdg_status tdg_group_run(const tdg_group_desc* d, const tdg_expr* pred, const uint64_t* sel_in,
+                         const tdg_group_plan* plan, void* ws, const tdg_group_out* out,
+                         void* stream);
+
+/* ---- join ----------------------------------------------------------------------
+ * Equi-join of a probe (left) side against a build (right) side on n_keys
+ * key columns.  join_type 0 = inner, 1 = left outer, 2 = full outer.
+ * Row ids are int32 (Teide caps both sides at INT32_MAX rows, exec.c:8139). */
+typedef struct tdg_join_desc {
+    int64_t n_left;
+    int64_t n_right;
+    int32_t n_keys;
+    int32_t join_type;
+    tdg_col lkeys[TDG_MAX_KEYS];
+    tdg_col rkeys[TDG_MAX_KEYS];
+    /* single integer key statistics of the build side (enables a direct map) */
+    int32_t have_range;
+    int32_t pad;
+    int64_t rkey_min, rkey_max;
+} tdg_join_desc;
+
+enum { TDG_JOIN_DIRECT = 1, TDG_JOIN_HASH = 2 };
+
+typedef struct tdg_join_plan {
+    int32_t method;        /* TDG_JOIN_DIRECT (key - min indexes the map) or TDG_JOIN_HASH */
+    int32_t pad;
+    int64_t n_slots;
+    size_t  ws_bytes;
+} tdg_join_plan;
+
+/* Replaces radix_join_bits / the partition plan (exec.c:7456-7471, 8179-8200). */
+tdg_status tdg_join_plan_make(const tdg_join_desc* d, tdg_join_plan* plan);
+
+/* Build the device hash table over the build side.  Replaces
+ * join_radix_partition + the build half of join_radix_build_probe_fn
+ * (exec.c:7626-7742, 7824-7950) and join_build_fn (7974-8006). */
+tdg_status tdg_join_build(const tdg_join_desc* d, const tdg_join_plan* plan, void* ws, void* stream);
+
+/* Materialized join, two calls.  tdg_join_count writes the number of output
+ * rows to d_count; tdg_join_emit writes them: left columns gathered by probe
+ * row, right columns by build row (zero-filled where a side is unmatched in
+ * an outer join).  Output order is probe-row order, then unmatched build rows
+ * (full join).  Replaces the probe + consolidation + gather of exec_join
+ * (exec.c:8296-8368, 8607-8728). */
+tdg_status tdg_join_count(const tdg_join_desc* d, const tdg_join_plan* plan, void* ws,
+                          const tdg_expr* lpred, const uint64_t* lsel, int64_t* d_count,
+                          void* stream);
+tdg_status tdg_join_emit(const tdg_join_desc* d, const tdg_join_plan* plan, void* ws,
+                         const tdg_expr* lpred, const uint64_t* lsel,
+                         int32_t n_lcols, const tdg_col* lsrc, void* const* ldst,
+                         int32_t n_rcols, const tdg_col* rsrc, void* const* rdst,
+                         void* stream);
+
+/* Fused probe + group-by: every joined row (probe rows passing lpred/lsel)
+ * is aggregated directly, with no join output materialized.  Key and
+ * aggregate columns of `g` name their side (tdg_col.side).  g->nrows is
+ * ignored.  Replaces exec_join followed by exec_group on its result. */
+tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_plan* jplan, void* jws,
+                              const tdg_expr* lpred, const uint64_t* lsel,
+                              const tdg_group_desc* g, const tdg_group_plan* gplan, void* gws,
+                              const tdg_group_out* out, void* stream);
+
+/* Device properties used by the planners (SM count, shared memory). */
+int32_t tdg_device_sm_count(void);
+
+/* ---- instrumentation ----------------------------------------------------------
+ * With timing on, each tdg_group_run / tdg_join_group_run records CUDA events
+ * around its main streaming kernel (the fused select [+ probe] + aggregate
+ * launch) on the stream it was given, and tdg_join_build around its build
+ * kernel; the last durations are read back here in milliseconds.  Timing
+ * adds no synchronization beyond the one each call already does. */
+void     tdg_set_timing(int32_t on);
+float    tdg_last_main_ms(void);
+float    tdg_last_build_ms(void);
+/* Kernels launched by this library since the process started. */
+uint64_t tdg_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TDG_H */

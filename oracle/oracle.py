@@ -1,0 +1,220 @@
+"""CPU oracle for the filter -> join -> group-by path.  TEST INFRASTRUCTURE ONLY.
+
+A numpy restatement of what Teide's executor computes on this path (TeideDB/
+teide, src/ops/exec.c), used by tests/, __graft_entry__.smoke() and the CPU
+baseline leg of bench.py as the checker.  The product (teide_b200) never
+imports it.
+
+It is pinned two ways (tests/test_oracle.py):
+  * against the known answers of Teide's own unit tests (test/test_exec.c,
+    test_graph.c, test_pool.c, test_sel.c), and
+  * against Teide itself: oracle/_ref/libteide_ref.so, compiled from the
+    reference's sources by oracle/Makefile, runs the same DAGs, and the
+    committed fixtures in tests/golden/ hold its outputs.
+
+Semantics restated here, with the lines they follow:
+  * comparisons: I64 vs I64 compare as integers, anything involving F64
+    compares as double (expr_compile type promotion, exec.c:872-895);
+  * selection = AND of the predicates of chained filters (td_sel_and,
+    sel.c:167-189; exec.c:11717-11731);
+  * group-by output: one row per distinct key tuple; key columns keep their
+    type; SUM is I64 (wrapping) or F64, COUNT I64, AVG = sum / count as
+    double, MIN/MAX keep the input type; names "<col>_sum", "_count",
+    "_mean", "_min", "_max" (emit_agg_columns, exec.c:4632-4773).  Rows are
+    returned in ascending key order (the direct-array order, exec.c:6330-6391);
+    compare hash-method results after sorting by key;
+  * join: every (left, right) pair with equal keys (join_keys_eq,
+    exec.c:7754-7768); output = all left columns then right non-key columns
+    (exec.c:8635-8655); LEFT keeps unmatched left rows, FULL also unmatched
+    right rows, with the missing side zero-filled (gather_fn, exec.c:1910-1939).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+OP_SUM, OP_MIN, OP_MAX, OP_COUNT, OP_AVG = 50, 52, 53, 54, 55
+SUFFIX = {OP_SUM: "_sum", OP_COUNT: "_count", OP_AVG: "_mean", OP_MIN: "_min", OP_MAX: "_max"}
+
+CMP = {
+    "eq": np.equal, "ne": np.not_equal, "lt": np.less,
+    "le": np.less_equal, "gt": np.greater, "ge": np.greater_equal,
+}
+
+
+def compare(op: str, a, b) -> np.ndarray:
+    """Element-wise comparison with Teide's promotion: int vs int stays
+    integer, any float operand promotes both to double."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    if a.dtype.kind == "f" or b.dtype.kind == "f":
+        a = a.astype(np.float64)
+        b = b.astype(np.float64)
+    else:
+        a = a.astype(np.int64)
+        b = b.astype(np.int64)
+    return CMP[op](a, b)
+
+
+def conj(cols: dict, terms) -> np.ndarray:
+    """AND of (column, op, constant) terms."""
+    n = len(next(iter(cols.values())))
+    m = np.ones(n, dtype=bool)
+    for name, op, k in terms:
+        m &= compare(op, cols[name], k)
+    return m
+
+
+def _key_ids(keys):
+    """Dense ids of key tuples in ascending key order, plus the unique keys."""
+    if len(keys) == 1:
+        k = keys[0]
+        if k.dtype.kind == "f":
+            k = np.where(k == 0, 0.0, k)          # -0.0 groups with +0.0
+        uniq, inv = np.unique(k, return_inverse=True)
+        return inv.ravel(), [uniq]
+    # lexicographic: first key most significant
+    cols = [np.where(k == 0, 0.0, k) if k.dtype.kind == "f" else k for k in keys]
+    order = np.lexsort(cols[::-1])
+    sk = [c[order] for c in cols]
+    if len(order):
+        new = np.zeros(len(order), dtype=bool)
+        new[0] = True
+        for c in sk:
+            new[1:] |= c[1:] != c[:-1]
+        gid_sorted = np.cumsum(new) - 1
+    else:
+        new = np.zeros(0, dtype=bool)
+        gid_sorted = np.zeros(0, dtype=np.int64)
+    inv = np.empty(len(order), dtype=np.int64)
+    inv[order] = gid_sorted
+    uniq = [c[new] for c in sk]
+    return inv, uniq
+
+
+def group(keys: dict, aggs, mask=None) -> dict:
+    """Group-by.  keys: {name: array}; aggs: [(op, name, array or None)].
+    Returns {column name: array} in ascending key order."""
+    names = list(keys)
+    karr = [np.asarray(keys[k]) for k in names]
+    n = len(karr[0]) if karr else (len(aggs[0][2]) if aggs and aggs[0][2] is not None else 0)
+    if mask is None:
+        mask = np.ones(n, dtype=bool)
+    sel = np.nonzero(mask)[0]
+    out = {}
+    if karr:
+        inv, uniq = _key_ids([k[sel] for k in karr])
+        ng = len(uniq[0])
+        for nm, u, k in zip(names, uniq, karr):
+            out[nm] = u.astype(k.dtype)
+    else:
+        inv = np.zeros(len(sel), dtype=np.int64)
+        ng = 1 if len(sel) else 0
+    cnt = np.bincount(inv, minlength=ng).astype(np.int64)
+    order = np.argsort(inv, kind="stable")
+    starts = np.searchsorted(inv[order], np.arange(ng)) if ng else np.zeros(0, np.int64)
+    for op, nm, arr in aggs:
+        col = f"{nm}{SUFFIX[op]}"
+        if op == OP_COUNT:
+            out[col] = cnt
+            continue
+        v = np.asarray(arr)[sel][order]
+        isf = v.dtype.kind == "f"
+        if op in (OP_SUM, OP_AVG):
+            if ng == 0:
+                s = np.zeros(0, np.float64 if isf else np.int64)
+            elif isf:
+                s = np.add.reduceat(v.astype(np.float64), starts)
+            else:
+                with np.errstate(over="ignore"):
+                    s = np.add.reduceat(v.astype(np.int64), starts)
+            out[col] = s if op == OP_SUM else s.astype(np.float64) / cnt
+        elif op == OP_MIN:
+            out[col] = np.minimum.reduceat(v, starts) if ng else v[:0]
+        elif op == OP_MAX:
+            out[col] = np.maximum.reduceat(v, starts) if ng else v[:0]
+    return out
+
+
+def _join_ids(lkeys, rkeys):
+    """Map key tuples of both sides onto shared dense ids."""
+    nl = len(lkeys[0])
+    both = [np.concatenate([np.asarray(a), np.asarray(b)]) for a, b in zip(lkeys, rkeys)]
+    inv, _ = _key_ids(both)
+    return inv[:nl], inv[nl:]
+
+
+def join_pairs(lkeys, rkeys, join_type=0, lmask=None):
+    """(left row, right row) pairs of an equi-join; -1 marks the missing side
+    of an outer-join row.  Pairs come in left-row order, then right-row order
+    within a left row, then unmatched right rows (full join)."""
+    nl = len(lkeys[0])
+    nr = len(rkeys[0])
+    lsel = np.arange(nl) if lmask is None else np.nonzero(lmask)[0]
+    if nr == 0 or len(lsel) == 0:
+        li = lsel if join_type >= 1 else np.zeros(0, np.int64)
+        ri = -np.ones(len(li), np.int64)
+        if join_type == 2 and nr:
+            li = np.concatenate([li, -np.ones(nr, np.int64)])
+            ri = np.concatenate([ri, np.arange(nr)])
+        return li.astype(np.int64), ri.astype(np.int64)
+    lid, rid = _join_ids([np.asarray(k)[lsel] for k in lkeys], rkeys)
+    nan_l = np.zeros(len(lsel), bool)
+    nan_r = np.zeros(nr, bool)
+    for a, b in zip(lkeys, rkeys):
+        a = np.asarray(a)[lsel]
+        if a.dtype.kind == "f":
+            nan_l |= np.isnan(a)
+        b = np.asarray(b)
+        if b.dtype.kind == "f":
+            nan_r |= np.isnan(b)
+    rid = np.where(nan_r, -2, rid)
+    ro = np.argsort(rid, kind="stable")
+    rs = rid[ro]
+    lo = np.searchsorted(rs, lid, "left")
+    hi = np.searchsorted(rs, lid, "right")
+    cnt = np.where(nan_l, 0, hi - lo)
+    emit = np.where((cnt == 0) & (join_type >= 1), 1, cnt)
+    li = np.repeat(lsel, emit)
+    starts = np.repeat(lo, emit)
+    within = np.arange(len(li)) - np.repeat(np.cumsum(emit) - emit, emit)
+    matched = np.repeat(cnt > 0, emit)
+    ri = np.where(matched, ro[np.minimum(starts + within, nr - 1)], -1)
+    if join_type == 2:
+        hit = np.zeros(nr, bool)
+        hit[ri[ri >= 0]] = True
+        un = np.nonzero(~hit)[0]
+        li = np.concatenate([li, -np.ones(len(un), np.int64)])
+        ri = np.concatenate([ri, un])
+    return li.astype(np.int64), ri.astype(np.int64)
+
+
+def gather(arr, idx):
+    arr = np.asarray(arr)
+    out = np.zeros(len(idx), arr.dtype)
+    ok = idx >= 0
+    out[ok] = arr[idx[ok]]
+    return out
+
+
+def join(left: dict, right: dict, lkey_names, rkey_names, join_type=0, lmask=None) -> dict:
+    li, ri = join_pairs([left[k] for k in lkey_names], [right[k] for k in rkey_names],
+                        join_type, lmask)
+    out = {nm: gather(c, li) for nm, c in left.items()}
+    for nm, c in right.items():
+        if nm in rkey_names:
+            continue
+        out.setdefault(nm, gather(c, ri))
+    return out
+
+
+def canonical(d: dict, by=None) -> dict:
+    """Rows sorted by the given columns (default: all, in column order)."""
+    cols = list(d) if by is None else list(by)
+    if not cols or len(d[cols[0]]) == 0:
+        return {k: np.asarray(v) for k, v in d.items()}
+    keys = []
+    for c in cols:
+        v = np.asarray(d[c])
+        keys.append(v.view(np.int64) if v.dtype == np.float64 else v)
+    order = np.lexsort(keys[::-1])
+    return {k: np.asarray(v)[order] for k, v in d.items()}

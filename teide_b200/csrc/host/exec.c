@@ -1,0 +1,1003 @@
+/*
+ * td_execute: walks a Teide DAG and runs its relational operators on the GPU.
+ *
+ * The walk mirrors exec_node (Teide src/ops/exec.c:11561-12321), with every
+ * compute step lowered to the kernels behind tdg.h and no CPU execution path:
+ *
+ *   OP_SCAN / OP_CONST     host objects, uploaded on first use (or resident)
+ *   element-wise ops       compiled to a tdg_expr program (exec.c:760-918);
+ *                          evaluated on the device when a value is needed
+ *   OP_FILTER on a table   lazy: the table plus a predicate program, like
+ *                          Teide's g->selection (exec.c:11674-11739); the
+ *                          consumer fuses it, or the final step compacts it
+ *   OP_FILTER on a vector  lazy filtered vector; consumed by OP_GROUP it
+ *                          defines the README pipeline (below), otherwise
+ *                          compacted
+ *   OP_GROUP               fused select + group-by (exec_group 5542-6879)
+ *   OP_JOIN                build + probe + gather (exec_join 8130-8741)
+ *   OP_COUNT/SUM/MIN/MAX/AVG  scalar reductions on the device
+ *
+ * Two DAG shapes get defined semantics here that Teide's CPU executor does
+ * not give them:
+ *   1. The README pipeline -- OP_GROUP whose key and aggregate inputs are
+ *      td_filter(td_scan(col), pred) vectors sharing one predicate -- groups
+ *      the rows that pass the predicate.  (Teide's exec_group reads such
+ *      vectors past their end, exec.c:5560 with 5654-5663.)  Columns are
+ *      named after the scanned column, as the filter-then-group pipeline
+ *      names them.
+ *   2. Filter -> join -> group in one graph: when OP_GROUP runs in a graph
+ *      bound to no table (td_graph_new(NULL)) that holds exactly one OP_JOIN,
+ *      the group reads the join's output -- the same hookup Teide makes for
+ *      a factorized OP_EXPAND (exec.c:11768-11800).  Its scans name columns
+ *      of the join output (left columns, then right non-key columns) and the
+ *      join is never materialized.  In Teide this graph fails with
+ *      TD_ERR_SCHEMA.
+ *
+ * Results are host td_t objects.  Device copies of result columns stay
+ * resident until the host column is freed, so a second graph over a result
+ * (the two-call join -> group chain) uploads nothing.
+ */
+
+#include "internal.h"
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+    td_t*           obj;       /* retained host table, vector or atom */
+    int             lazy;      /* rows of obj are filtered by pred / dsel */
+    int             has_pred;
+    tdg_expr        pred;      /* over the rows of obj (vectors: rows of rows_tbl) */
+    const uint64_t* dsel;      /* device TD_SEL bits */
+} val_t;
+
+typedef struct {
+    td_graph_t* g;
+    tdb_ctx     c;
+} ex_t;
+
+static val_t vnone(void) { val_t v; memset(&v, 0, sizeof(v)); return v; }
+static void vfree(val_t* v) { if (v->obj && !TD_IS_ERR(v->obj)) td_release(v->obj); v->obj = NULL; }
+#define CALL(expr) (tdb_note_kernel(), (expr))
+
+/* ---- expression compilation ----------------------------------------------------- */
+typedef struct {
+    ex_t*     x;
+    td_t*     tbl;             /* table scans resolve against */
+    tdg_expr* e;
+    uint32_t  ids[TDG_MAX_INS];
+    int       regs[TDG_MAX_INS];
+    int       n_memo;
+    int       err;
+} xc_t;
+
+static td_t* scan_table_of(ex_t* x, td_op_ext_t* ext, td_t* dflt) {
+    uint16_t tid = 0;
+    memcpy(&tid, ext->base.pad, sizeof(tid));
+    if (tid > 0 && x->g->tables && tid - 1 < x->g->n_tables) return x->g->tables[tid - 1];
+    return dflt;
+}
+
+static int emit_ins(xc_t* xc, uint8_t op, int a, int b, int kind, int64_t imm) {
+    tdg_expr* e = xc->e;
+    if (e->n_ins >= TDG_MAX_INS) { xc->err = TD_ERR_NYI; return -1; }
+    tdg_ins* I = &e->ins[e->n_ins];
+    memset(I, 0, sizeof(*I));
+    I->op = op; I->a = (uint8_t)(a < 0 ? 0 : a); I->b = (uint8_t)(b < 0 ? 0 : b);
+    I->kind = (uint8_t)kind; I->imm = imm;
+    return e->n_ins++;
+}
+
+static int add_col(xc_t* xc, const tdb_devcol* d) {
+    tdg_expr* e = xc->e;
+    for (int i = 0; i < e->n_cols; i++) if (e->cols[i].data == d->dptr) return i;
+    if (e->n_cols >= TDG_MAX_XCOLS) { xc->err = TD_ERR_NYI; return -1; }
+    tdg_col* c = &e->cols[e->n_cols];
+    memset(c, 0, sizeof(*c));
+    c->data = d->dptr; c->type = d->type; c->attrs = d->attrs;
+    return e->n_cols++;
+}
+
+static int to_kind(xc_t* xc, int r, int kind) {
+    if (r < 0) return r;
+    int k = xc->e->ins[r].kind;
+    if (k == kind) return r;
+    return emit_ins(xc, kind == 1 ? TDG_X_TOF64 : TDG_X_TOI64, r, 0, kind, 0);
+}
+
+static int xc_node(xc_t* xc, td_op_t* op) {
+    if (!op || xc->err) { if (!xc->err) xc->err = TD_ERR_NYI; return -1; }
+    for (int i = 0; i < xc->n_memo; i++) if (xc->ids[i] == op->id) return xc->regs[i];
+    int r = -1;
+    td_graph_t* g = xc->x->g;
+    switch (op->opcode) {
+        case OP_SCAN: {
+            td_op_ext_t* ext = tdb_find_ext(g, op->id);
+            td_t* tbl = ext ? scan_table_of(xc->x, ext, xc->tbl) : NULL;
+            td_t* col = tbl ? td_table_get_col(tbl, ext->sym) : NULL;
+            if (!col) { xc->err = TD_ERR_SCHEMA; return -1; }
+            if (col->len != td_table_nrows(xc->tbl)) { xc->err = TD_ERR_LENGTH; return -1; }
+            tdb_devcol d;
+            int st = tdb_col_device(&xc->x->c, col, 0, &d);
+            if (st) { xc->err = st; return -1; }
+            int ci = add_col(xc, &d);
+            if (ci < 0) return -1;
+            r = emit_ins(xc, TDG_X_COL, 0, 0, col->type == TD_F64 ? 1 : 0, ci);
+            break;
+        }
+        case OP_CONST: {
+            td_op_ext_t* ext = tdb_find_ext(g, op->id);
+            td_t* lit = ext ? ext->literal : NULL;
+            double f; int64_t i; int isf;
+            if (lit && tdb_atom_numeric(lit, &f, &i, &isf)) {
+                int64_t bits;
+                if (isf) memcpy(&bits, &f, 8); else bits = i;
+                r = emit_ins(xc, TDG_X_CONST, 0, 0, isf, bits);
+            } else if (lit && lit->type == TD_ATOM_STR) {
+                /* string constant compares as its symbol id (exec.c:829-839);
+                 * an unknown string matches no symbol, whose ids are >= 0 */
+                int64_t sid = td_sym_find(td_str_ptr(lit), td_str_len(lit));
+                r = emit_ins(xc, TDG_X_CONST, 0, 0, 0, sid < 0 ? -1 : sid);
+            } else {
+                xc->err = TD_ERR_NYI;
+                return -1;
+            }
+            break;
+        }
+        case OP_ALIAS: case OP_MATERIALIZE:
+            r = xc_node(xc, op->inputs[0]);
+            break;
+        case OP_EQ: case OP_NE: case OP_LT: case OP_LE: case OP_GT: case OP_GE: {
+            int a = xc_node(xc, op->inputs[0]), b = xc_node(xc, op->inputs[1]);
+            if (a < 0 || b < 0) return -1;
+            int kind = (xc->e->ins[a].kind || xc->e->ins[b].kind) ? 1 : 0;
+            a = to_kind(xc, a, kind); b = to_kind(xc, b, kind);
+            if (a < 0 || b < 0) return -1;
+            r = emit_ins(xc, (uint8_t)(TDG_X_EQ + (op->opcode - OP_EQ)), a, b, 0, 0);
+            break;
+        }
+        case OP_AND: case OP_OR: {
+            int a = xc_node(xc, op->inputs[0]), b = xc_node(xc, op->inputs[1]);
+            if (a < 0 || b < 0) return -1;
+            r = emit_ins(xc, op->opcode == OP_AND ? TDG_X_AND : TDG_X_OR, a, b, 0, 0);
+            break;
+        }
+        case OP_NOT: {
+            int a = xc_node(xc, op->inputs[0]);
+            if (a < 0) return -1;
+            r = emit_ins(xc, TDG_X_NOT, a, 0, 0, 0);
+            break;
+        }
+        case OP_NEG: case OP_ABS: {
+            int a = xc_node(xc, op->inputs[0]);
+            if (a < 0) return -1;
+            r = emit_ins(xc, op->opcode == OP_NEG ? TDG_X_NEG : TDG_X_ABS, a, 0, xc->e->ins[a].kind, 0);
+            break;
+        }
+        case OP_CAST: {
+            int a = xc_node(xc, op->inputs[0]);
+            if (a < 0) return -1;
+            r = to_kind(xc, a, op->out_type == TD_F64 ? 1 : 0);
+            break;
+        }
+        case OP_ADD: case OP_SUB: case OP_MUL: case OP_DIV: case OP_MOD:
+        case OP_MIN2: case OP_MAX2: {
+            int a = xc_node(xc, op->inputs[0]), b = xc_node(xc, op->inputs[1]);
+            if (a < 0 || b < 0) return -1;
+            int kind = (op->opcode == OP_DIV || xc->e->ins[a].kind || xc->e->ins[b].kind) ? 1 : 0;
+            a = to_kind(xc, a, kind); b = to_kind(xc, b, kind);
+            if (a < 0 || b < 0) return -1;
+            static const uint8_t map[] = {
+                [OP_ADD] = TDG_X_ADD, [OP_SUB] = TDG_X_SUB, [OP_MUL] = TDG_X_MUL, [OP_DIV] = TDG_X_DIV,
+                [OP_MOD] = TDG_X_MOD, [OP_MIN2] = TDG_X_MIN2, [OP_MAX2] = TDG_X_MAX2 };
+            r = emit_ins(xc, map[op->opcode], a, b, kind, 0);
+            break;
+        }
+        default:
+            xc->err = TD_ERR_NYI;
+            return -1;
+    }
+    if (r >= 0 && xc->n_memo < TDG_MAX_INS) {
+        xc->ids[xc->n_memo] = op->id;
+        xc->regs[xc->n_memo++] = r;
+    }
+    return r;
+}
+
+static int compile_expr(ex_t* x, td_t* tbl, td_op_t* op, tdg_expr* e) {
+    memset(e, 0, sizeof(*e));
+    if (!tbl || tbl->type != TD_TABLE) return TD_ERR_SCHEMA;
+    xc_t xc;
+    memset(&xc, 0, sizeof(xc));
+    xc.x = x; xc.tbl = tbl; xc.e = e;
+    int r = xc_node(&xc, op);
+    if (xc.err) return xc.err;
+    if (r < 0) return TD_ERR_NYI;
+    e->out = r;
+    return TD_OK;
+}
+
+/* p = p AND q */
+static int expr_and(tdg_expr* p, const tdg_expr* q) {
+    if (p->n_ins == 0) { *p = *q; return TD_OK; }
+    if (q->n_ins == 0) return TD_OK;
+    if (p->n_ins + q->n_ins + 1 > TDG_MAX_INS) return TD_ERR_NYI;
+    int colmap[TDG_MAX_XCOLS];
+    for (int i = 0; i < q->n_cols; i++) {
+        int found = -1;
+        for (int j = 0; j < p->n_cols; j++) if (p->cols[j].data == q->cols[i].data) found = j;
+        if (found < 0) {
+            if (p->n_cols >= TDG_MAX_XCOLS) return TD_ERR_NYI;
+            p->cols[p->n_cols] = q->cols[i];
+            found = p->n_cols++;
+        }
+        colmap[i] = found;
+    }
+    int base = p->n_ins;
+    for (int k = 0; k < q->n_ins; k++) {
+        tdg_ins I = q->ins[k];
+        if (I.op == TDG_X_COL) I.imm = colmap[I.imm];
+        else if (I.op != TDG_X_CONST) { I.a = (uint8_t)(I.a + base); I.b = (uint8_t)(I.b + base); }
+        p->ins[p->n_ins++] = I;
+    }
+    tdg_ins* A = &p->ins[p->n_ins];
+    memset(A, 0, sizeof(*A));
+    A->op = TDG_X_AND; A->a = (uint8_t)p->out; A->b = (uint8_t)(base + q->out);
+    p->out = p->n_ins++;
+    return TD_OK;
+}
+
+/* ---- host result construction ------------------------------------------------------ */
+
+/* New host vector of n elements with the element type of `like`. */
+static td_t* vec_like(int8_t type, uint8_t attrs, int64_t n) {
+    td_t* v = type == TD_SYM ? td_sym_vec_new(attrs & TD_SYM_W_MASK, n) : td_vec_new(type, n);
+    if (v && !TD_IS_ERR(v)) v->len = n;
+    return v;
+}
+
+/* Copy n elements from the device into a new host vector. */
+static td_t* fetch_vec(ex_t* x, const void* dptr, int8_t type, uint8_t attrs, int64_t n) {
+    td_t* v = vec_like(type, attrs, n);
+    if (!v || TD_IS_ERR(v)) return v ? v : TD_ERR_PTR(TD_ERR_OOM);
+    size_t bytes = (size_t)n * td_sym_elem_size(type, attrs);
+    int st = tdb_d2h(&x->c, td_data(v), dptr, bytes);
+    if (st) { td_release(v); return TD_ERR_PTR(st); }
+    return v;
+}
+
+/* ---- values ------------------------------------------------------------------------------- */
+static td_t* exec_value(ex_t* x, td_op_t* op, val_t* out);
+
+/* Device columns of a whole table, in column order. */
+static int table_dev_cols(ex_t* x, td_t* t, tdg_col* cols, int max) {
+    int64_t nc = td_table_ncols(t);
+    if (nc > max) return -TD_ERR_NYI;
+    for (int64_t j = 0; j < nc; j++) {
+        tdb_devcol d;
+        int st = tdb_col_device(&x->c, td_table_get_col_idx(t, j), 0, &d);
+        if (st) return -st;
+        memset(&cols[j], 0, sizeof(tdg_col));
+        cols[j].data = d.dptr; cols[j].type = d.type; cols[j].attrs = d.attrs;
+    }
+    return (int)nc;
+}
+
+#define MAX_TCOLS 256
+
+/* Compact a lazy table or vector on the device and bring it to the host. */
+static td_t* materialize(ex_t* x, val_t* v) {
+    if (!v->lazy) { td_t* o = v->obj; td_retain(o); return o; }
+    td_t* src = v->obj;
+    int is_tbl = src->type == TD_TABLE;
+    int64_t n = is_tbl ? td_table_nrows(src) : src->len;
+    const tdg_expr* pred = v->has_pred ? &v->pred : NULL;
+    void* ws = tdb_dev_alloc(&x->c, tdg_select_ws_bytes(n));
+    int64_t* dcount = tdb_dev_alloc(&x->c, 8);
+    if (!ws || !dcount) return TD_ERR_PTR(TD_ERR_OOM);
+    int st = CALL(tdg_select_count(n, pred, v->dsel, ws, dcount, x->c.stream));
+    if (st) return TD_ERR_PTR(st);
+    int64_t m = 0;
+    st = tdb_d2h(&x->c, &m, dcount, 8);
+    if (st) return TD_ERR_PTR(st);
+    tdg_col cols[MAX_TCOLS];
+    void* dst[MAX_TCOLS];
+    int nc;
+    if (is_tbl) {
+        nc = table_dev_cols(x, src, cols, MAX_TCOLS);
+        if (nc < 0) return TD_ERR_PTR(-nc);
+    } else {
+        tdb_devcol d;
+        st = tdb_col_device(&x->c, src, 0, &d);
+        if (st) return TD_ERR_PTR(st);
+        memset(&cols[0], 0, sizeof(tdg_col));
+        cols[0].data = d.dptr; cols[0].type = d.type; cols[0].attrs = d.attrs;
+        nc = 1;
+    }
+    for (int j = 0; j < nc; j++) {
+        dst[j] = tdb_dev_alloc(&x->c, (size_t)(m ? m : 1) * td_sym_elem_size(cols[j].type, cols[j].attrs));
+        if (!dst[j]) return TD_ERR_PTR(TD_ERR_OOM);
+    }
+    st = CALL(tdg_select_gather(n, pred, v->dsel, ws, nc, cols, dst, x->c.stream));
+    if (st) return TD_ERR_PTR(st);
+    if (!is_tbl) return fetch_vec(x, dst[0], cols[0].type, cols[0].attrs, m);
+    td_t* out = td_table_new(nc);
+    if (!out || TD_IS_ERR(out)) return out;
+    for (int j = 0; j < nc; j++) {
+        td_t* col = fetch_vec(x, dst[j], cols[j].type, cols[j].attrs, m);
+        if (TD_IS_ERR(col)) { td_release(out); return col; }
+        out = td_table_add_col(out, td_table_col_name(src, j), col);
+        td_release(col);
+        if (TD_IS_ERR(out)) return out;
+    }
+    return out;
+}
+
+/* ---- group-by --------------------------------------------------------------------------- */
+
+/* One key or aggregate input of a group-by, resolved to a device column. */
+typedef struct {
+    tdg_col  col;
+    int64_t  name;      /* output base name: column symbol, or -1 for expressions */
+    int      filtered;  /* came through td_filter(vector, pred) */
+    td_op_t* pred_op;
+    td_t*    src;       /* host column (for output type), may be NULL for expressions */
+    int8_t   type;
+    uint8_t  attrs;
+    int      has_stats;
+    int64_t  kmin, kmax;
+} gin_t;
+
+/* Join output as a group-by input: where each named column comes from. */
+typedef struct {
+    td_t* left;
+    td_t* right;
+    td_op_ext_t* jext;
+} jsrc_t;
+
+static int col_of_join(ex_t* x, jsrc_t* js, int64_t sym, td_t** col, int* side) {
+    td_t* c = td_table_get_col(js->left, sym);
+    if (c) { *col = c; *side = 0; return TD_OK; }
+    for (int k = 0; k < js->jext->join.n_join_keys; k++) {
+        td_op_ext_t* rk = tdb_find_ext(x->g, js->jext->join.right_keys[k]->id);
+        if (rk && rk->base.opcode == OP_SCAN && rk->sym == sym) return TD_ERR_SCHEMA;
+    }
+    c = td_table_get_col(js->right, sym);
+    if (!c) return TD_ERR_SCHEMA;
+    *col = c; *side = 1;
+    return TD_OK;
+}
+
+static int resolve_gin(ex_t* x, td_op_t* op, td_t* tbl, jsrc_t* js, int want_stats, gin_t* gi) {
+    memset(gi, 0, sizeof(*gi));
+    gi->name = -1;
+    td_op_t* o = op;
+    while (o && (o->opcode == OP_ALIAS || o->opcode == OP_MATERIALIZE)) o = o->inputs[0];
+    if (o && o->opcode == OP_FILTER && o->inputs[0] &&
+        (o->inputs[0]->opcode == OP_SCAN || o->inputs[0]->opcode == OP_ALIAS)) {
+        gi->filtered = 1;
+        gi->pred_op = o->inputs[1];
+        o = o->inputs[0];
+        while (o && o->opcode == OP_ALIAS) o = o->inputs[0];
+    }
+    if (!o) return TD_ERR_NYI;
+    if (o->opcode == OP_SCAN) {
+        td_op_ext_t* ext = tdb_find_ext(x->g, o->id);
+        if (!ext) return TD_ERR_NYI;
+        td_t* col = NULL;
+        int side = 0;
+        if (js) {
+            int st = col_of_join(x, js, ext->sym, &col, &side);
+            if (st) return st;
+        } else {
+            td_t* t = scan_table_of(x, ext, tbl);
+            col = t ? td_table_get_col(t, ext->sym) : NULL;
+            if (!col) return TD_ERR_SCHEMA;
+            if (col->len != td_table_nrows(tbl)) return TD_ERR_LENGTH;
+        }
+        tdb_devcol d;
+        int st = tdb_col_device(&x->c, col, want_stats, &d);
+        if (st) return st;
+        gi->col.data = d.dptr; gi->col.type = d.type; gi->col.attrs = d.attrs; gi->col.side = (uint8_t)side;
+        gi->name = ext->sym;
+        gi->src = col;
+        gi->type = col->type;
+        gi->attrs = col->attrs;
+        gi->has_stats = d.has_stats;
+        gi->kmin = d.kmin; gi->kmax = d.kmax;
+        return TD_OK;
+    }
+    if (js) return TD_ERR_NYI;     /* expressions over a join output are not lowered */
+    /* expression input: evaluate on the device into a temporary column */
+    tdg_expr e;
+    int st = compile_expr(x, tbl, o, &e);
+    if (st) return st;
+    int kind = e.ins[e.out].kind;
+    int64_t n = td_table_nrows(tbl);
+    void* d = tdb_dev_alloc(&x->c, (size_t)(n ? n : 1) * 8);
+    if (!d) return TD_ERR_OOM;
+    st = CALL(tdg_eval(&e, n, d, kind, x->c.stream));
+    if (st) return st;
+    gi->col.data = d; gi->col.type = kind ? TD_F64 : TD_I64;
+    gi->type = gi->col.type;
+    if (want_stats && !kind) {
+        int64_t* mm = tdb_dev_alloc(&x->c, 16);
+        int64_t h[2];
+        if (!mm) return TD_ERR_OOM;
+        st = CALL(tdg_minmax(gi->col, n, mm, x->c.stream));
+        if (!st) st = tdb_d2h(&x->c, h, mm, 16);
+        if (st) return st;
+        gi->has_stats = 1; gi->kmin = h[0]; gi->kmax = h[1];
+    }
+    return TD_OK;
+}
+
+static int64_t agg_name(uint16_t op, int64_t base, int a) {
+    const char* sfx = op == OP_SUM ? "_sum" : op == OP_COUNT ? "_count" : op == OP_AVG ? "_mean"
+                    : op == OP_MIN ? "_min" : op == OP_MAX ? "_max" : "";
+    char buf[300];
+    int n;
+    td_t* s = base >= 0 ? td_sym_str(base) : NULL;
+    if (s && td_str_len(s) + strlen(sfx) < sizeof(buf)) {
+        n = (int)td_str_len(s);
+        memcpy(buf, td_str_ptr(s), (size_t)n);
+        memcpy(buf + n, sfx, strlen(sfx));
+        n += (int)strlen(sfx);
+    } else {
+        n = snprintf(buf, sizeof(buf), "_e%d%s", a, sfx);
+    }
+    return td_sym_intern(buf, (size_t)n);
+}
+
+typedef struct {
+    const tdg_join_desc* jd;
+    const tdg_join_plan* jp;
+    void*                jws;
+} jrun_t;
+
+/* Group-by over `tbl` rows (or over a join's output when js/jr are given). */
+static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pred_in,
+                       const uint64_t* dsel, jsrc_t* js, jrun_t* jr) {
+    int nk = ext->n_keys, na = ext->n_aggs;
+    if (nk > TDG_MAX_KEYS || na > TDG_MAX_AGGS) return TD_ERR_PTR(TD_ERR_NYI);
+    gin_t keys[TDG_MAX_KEYS], ins[TDG_MAX_AGGS];
+    td_op_t* pred_op = NULL;
+    int st;
+    for (int k = 0; k < nk; k++) {
+        st = resolve_gin(x, ext->keys[k], tbl, js, 1, &keys[k]);
+        if (st) return TD_ERR_PTR(st);
+        if (keys[k].filtered) {
+            if (pred_op && pred_op != keys[k].pred_op) return TD_ERR_PTR(TD_ERR_NYI);
+            pred_op = keys[k].pred_op;
+        }
+    }
+    for (int a = 0; a < na; a++) {
+        memset(&ins[a], 0, sizeof(gin_t));
+        ins[a].name = -1;
+        td_op_t* in = ext->agg_ins[a];
+        if (ext->agg_ops[a] == OP_COUNT && in && in->opcode == OP_CONST) continue;
+        st = resolve_gin(x, in, tbl, js, 0, &ins[a]);
+        if (st == TD_ERR_NYI && ext->agg_ops[a] == OP_COUNT) { st = TD_OK; continue; }
+        if (st) return TD_ERR_PTR(st);
+        if (ins[a].filtered) {
+            if (pred_op && pred_op != ins[a].pred_op) return TD_ERR_PTR(TD_ERR_NYI);
+            pred_op = ins[a].pred_op;
+        }
+    }
+    /* selection: caller's lazy filter AND the README-style shared predicate */
+    tdg_expr pred;
+    memset(&pred, 0, sizeof(pred));
+    if (pred_in) pred = *pred_in;
+    if (pred_op) {
+        if (js) return TD_ERR_PTR(TD_ERR_NYI);
+        tdg_expr p2;
+        st = compile_expr(x, tbl, pred_op, &p2);
+        if (st) return TD_ERR_PTR(st);
+        st = expr_and(&pred, &p2);
+        if (st) return TD_ERR_PTR(st);
+    }
+    const tdg_expr* pp = pred.n_ins ? &pred : NULL;
+
+    tdg_group_desc d;
+    memset(&d, 0, sizeof(d));
+    d.nrows = js ? 0 : td_table_nrows(tbl);
+    d.n_keys = nk;
+    d.n_aggs = na;
+    d.have_range = 1;
+    int jtype = jr ? jr->jd->join_type : 0;
+    for (int k = 0; k < nk; k++) {
+        d.keys[k] = keys[k].col;
+        if (!keys[k].has_stats) { d.have_range = 0; continue; }
+        d.key_min[k] = keys[k].kmin;
+        d.key_max[k] = keys[k].kmax;
+        /* outer joins zero-fill the unmatched side: 0 must be a valid key */
+        int nullable = (jtype >= 1 && keys[k].col.side == 1) || (jtype == 2 && keys[k].col.side == 0);
+        if (nullable) {
+            if (d.key_min[k] > 0) d.key_min[k] = 0;
+            if (d.key_max[k] < 0) d.key_max[k] = 0;
+        }
+    }
+    for (int a = 0; a < na; a++) {
+        d.aggs[a].op = ext->agg_ops[a];
+        d.aggs[a].in = ins[a].col;
+        if (d.aggs[a].op != OP_COUNT && !ins[a].col.data) return TD_ERR_PTR(TD_ERR_NYI);
+    }
+    int64_t rows_bound = js ? (jr->jd->n_left + jr->jd->n_right) : d.nrows;
+    if (js) d.nrows = rows_bound;
+    tdg_group_plan plan;
+    st = tdg_group_plan_make(&d, 0, &plan);
+    if (st) return TD_ERR_PTR(st);
+    void* ws = tdb_dev_alloc(&x->c, plan.ws_bytes);
+    tdg_group_out out;
+    memset(&out, 0, sizeof(out));
+    out.d_n_groups = tdb_dev_alloc(&x->c, 8);
+    if (!ws || !out.d_n_groups) return TD_ERR_PTR(TD_ERR_OOM);
+    for (int k = 0; k < nk; k++) {
+        out.keys[k] = tdb_dev_alloc(&x->c, (size_t)plan.max_groups * td_sym_elem_size(keys[k].type, keys[k].attrs));
+        if (!out.keys[k]) return TD_ERR_PTR(TD_ERR_OOM);
+    }
+    for (int a = 0; a < na; a++) {
+        out.aggs[a] = tdb_dev_alloc(&x->c, (size_t)plan.max_groups * 8);
+        if (!out.aggs[a]) return TD_ERR_PTR(TD_ERR_OOM);
+    }
+    if ((st = tdb_check_cancel())) return TD_ERR_PTR(st);
+    if (jr) {
+        st = CALL(tdg_join_group_run(jr->jd, jr->jp, jr->jws, pp, dsel, &d, &plan, ws, &out, x->c.stream));
+        tdb_note_methods(plan.method, jr->jp->method, 1);
+    } else {
+        st = CALL(tdg_group_run(&d, pp, dsel, &plan, ws, &out, x->c.stream));
+        tdb_note_methods(plan.method, 0, pp != NULL);
+    }
+    if (st) return TD_ERR_PTR(st);
+    int64_t ng = 0;
+    st = tdb_d2h(&x->c, &ng, out.d_n_groups, 8);
+    if (st) return TD_ERR_PTR(st);
+
+    td_t* res = td_table_new(nk + na);
+    if (!res || TD_IS_ERR(res)) return res;
+    for (int k = 0; k < nk; k++) {
+        td_t* col = fetch_vec(x, out.keys[k], keys[k].type, keys[k].attrs, ng);
+        if (TD_IS_ERR(col)) { td_release(res); return col; }
+        int64_t nm = keys[k].name >= 0 ? keys[k].name : (int64_t)k;
+        res = td_table_add_col(res, nm, col);
+        td_release(col);
+        if (TD_IS_ERR(res)) return res;
+    }
+    for (int a = 0; a < na; a++) {
+        uint16_t op = ext->agg_ops[a];
+        int is_f = ins[a].col.data && ins[a].col.type == TD_F64;
+        int8_t ot = op == OP_AVG ? TD_F64 : op == OP_COUNT ? TD_I64
+                  : op == OP_SUM ? (is_f ? TD_F64 : TD_I64)
+                  : (ins[a].type ? ins[a].type : TD_I64);
+        td_t* col;
+        if (td_sym_elem_size(ot, ins[a].attrs) == 8 || op == OP_AVG || op == OP_COUNT || op == OP_SUM) {
+            int8_t vt = (ot == TD_F64 || op == OP_AVG) ? TD_F64 : (td_sym_elem_size(ot, ins[a].attrs) == 8 ? ot : TD_I64);
+            col = fetch_vec(x, out.aggs[a], vt, vt == TD_SYM ? ins[a].attrs : 0, ng);
+        } else {
+            /* MIN/MAX of a narrow integer column: narrow the int64 results */
+            td_t* wide = fetch_vec(x, out.aggs[a], TD_I64, 0, ng);
+            if (TD_IS_ERR(wide)) { td_release(res); return wide; }
+            col = vec_like(ot, ins[a].attrs, ng);
+            if (!TD_IS_ERR(col)) {
+                const int64_t* w = (const int64_t*)td_data(wide);
+                for (int64_t i = 0; i < ng; i++) {
+                    if (ot == TD_SYM) td_write_sym(td_data(col), i, (uint64_t)w[i], TD_SYM, ins[a].attrs);
+                    else switch (td_elem_size(ot)) {
+                        case 4: ((int32_t*)td_data(col))[i] = (int32_t)w[i]; break;
+                        case 2: ((int16_t*)td_data(col))[i] = (int16_t)w[i]; break;
+                        default: ((uint8_t*)td_data(col))[i] = (uint8_t)w[i]; break;
+                    }
+                }
+            }
+            td_release(wide);
+        }
+        if (TD_IS_ERR(col)) { td_release(res); return col; }
+        res = td_table_add_col(res, agg_name(op, ins[a].name, a), col);
+        td_release(col);
+        if (TD_IS_ERR(res)) return res;
+    }
+    return res;
+}
+
+/* ---- join ---------------------------------------------------------------------------------- */
+typedef struct {
+    tdg_join_desc d;
+    tdg_join_plan p;
+    void* ws;
+    td_t* left;      /* host tables (retained by the caller's val_t) */
+    td_t* right;
+} jbuilt_t;
+
+/* Right side with a pending filter: compact it on the device first. */
+static td_t* dense_side(ex_t* x, val_t* v) {
+    if (!v->lazy) { td_retain(v->obj); return v->obj; }
+    return materialize(x, v);
+}
+
+static int prepare_join(ex_t* x, td_op_ext_t* ext, val_t* lv, td_t* right, jbuilt_t* jb) {
+    memset(jb, 0, sizeof(*jb));
+    td_t* left = lv->obj;
+    if (!left || left->type != TD_TABLE || !right || right->type != TD_TABLE) return TD_ERR_TYPE;
+    int nk = ext->join.n_join_keys;
+    if (nk < 1 || nk > TDG_MAX_KEYS) return TD_ERR_NYI;
+    jb->left = left; jb->right = right;
+    tdg_join_desc* d = &jb->d;
+    d->n_left = td_table_nrows(left);
+    d->n_right = td_table_nrows(right);
+    if (d->n_left > INT32_MAX || d->n_right > INT32_MAX) return TD_ERR_NYI;
+    d->n_keys = nk;
+    d->join_type = ext->join.join_type;
+    for (int k = 0; k < nk; k++) {
+        td_op_ext_t* lk = tdb_find_ext(x->g, ext->join.left_keys[k]->id);
+        td_op_ext_t* rk = tdb_find_ext(x->g, ext->join.right_keys[k]->id);
+        td_t* lc = (lk && lk->base.opcode == OP_SCAN) ? td_table_get_col(left, lk->sym) : NULL;
+        td_t* rc = NULL;
+        if (rk && rk->base.opcode == OP_SCAN) rc = td_table_get_col(right, rk->sym);
+        else if (rk && rk->base.opcode == OP_CONST && rk->literal && td_is_vec(rk->literal)) rc = rk->literal;
+        if (!lc || !rc) return TD_ERR_SCHEMA;
+        tdb_devcol dl, dr;
+        int st = tdb_col_device(&x->c, lc, 0, &dl);
+        if (!st) st = tdb_col_device(&x->c, rc, nk == 1, &dr);
+        if (st) return st;
+        d->lkeys[k] = (tdg_col){ dl.dptr, dl.type, dl.attrs, 0, {0} };
+        d->rkeys[k] = (tdg_col){ dr.dptr, dr.type, dr.attrs, 1, {0} };
+        if (nk == 1 && dr.has_stats && dr.len > 0) {
+            d->have_range = 1;
+            d->rkey_min = dr.kmin;
+            d->rkey_max = dr.kmax;
+        }
+    }
+    int st = tdg_join_plan_make(d, &jb->p);
+    if (st) return st;
+    jb->ws = tdb_dev_alloc(&x->c, jb->p.ws_bytes);
+    if (!jb->ws) return TD_ERR_OOM;
+    if ((st = tdb_check_cancel())) return st;
+    return CALL(tdg_join_build(d, &jb->p, jb->ws, x->c.stream));
+}
+
+static int is_right_key(ex_t* x, td_op_ext_t* ext, int64_t name) {
+    for (int k = 0; k < ext->join.n_join_keys; k++) {
+        td_op_ext_t* rk = tdb_find_ext(x->g, ext->join.right_keys[k]->id);
+        if (rk && rk->base.opcode == OP_SCAN && rk->sym == name) return 1;
+    }
+    return 0;
+}
+
+static td_t* join_materialize(ex_t* x, td_op_ext_t* ext, val_t* lv, jbuilt_t* jb) {
+    const tdg_expr* lp = lv->has_pred ? &lv->pred : NULL;
+    int64_t* dcount = tdb_dev_alloc(&x->c, 8);
+    if (!dcount) return TD_ERR_PTR(TD_ERR_OOM);
+    int st = CALL(tdg_join_count(&jb->d, &jb->p, jb->ws, lp, lv->dsel, dcount, x->c.stream));
+    if (st) return TD_ERR_PTR(st);
+    int64_t m = 0;
+    st = tdb_d2h(&x->c, &m, dcount, 8);
+    if (st) return TD_ERR_PTR(st);
+    tdg_col lsrc[MAX_TCOLS], rsrc[MAX_TCOLS];
+    void *ldst[MAX_TCOLS], *rdst[MAX_TCOLS];
+    int64_t rname[MAX_TCOLS];
+    int nl = table_dev_cols(x, jb->left, lsrc, 16);
+    if (nl < 0) return TD_ERR_PTR(-nl);
+    int nr = 0;
+    for (int64_t j = 0; j < td_table_ncols(jb->right); j++) {
+        int64_t nm = td_table_col_name(jb->right, j);
+        if (is_right_key(x, ext, nm)) continue;
+        if (nr >= 16) return TD_ERR_PTR(TD_ERR_NYI);
+        tdb_devcol dd;
+        st = tdb_col_device(&x->c, td_table_get_col_idx(jb->right, j), 0, &dd);
+        if (st) return TD_ERR_PTR(st);
+        rsrc[nr] = (tdg_col){ dd.dptr, dd.type, dd.attrs, 1, {0} };
+        rname[nr++] = nm;
+    }
+    size_t cnt = (size_t)(m ? m : 1);
+    for (int j = 0; j < nl; j++)
+        if (!(ldst[j] = tdb_dev_alloc(&x->c, cnt * td_sym_elem_size(lsrc[j].type, lsrc[j].attrs))))
+            return TD_ERR_PTR(TD_ERR_OOM);
+    for (int j = 0; j < nr; j++)
+        if (!(rdst[j] = tdb_dev_alloc(&x->c, cnt * td_sym_elem_size(rsrc[j].type, rsrc[j].attrs))))
+            return TD_ERR_PTR(TD_ERR_OOM);
+    st = CALL(tdg_join_emit(&jb->d, &jb->p, jb->ws, lp, lv->dsel, nl, lsrc, ldst, nr, rsrc, rdst, x->c.stream));
+    if (st) return TD_ERR_PTR(st);
+    tdb_note_methods(0, jb->p.method, 0);
+    td_t* res = td_table_new(nl + nr);
+    if (!res || TD_IS_ERR(res)) return res;
+    for (int j = 0; j < nl + nr; j++) {
+        const tdg_col* sc = j < nl ? &lsrc[j] : &rsrc[j - nl];
+        void* dp = j < nl ? ldst[j] : rdst[j - nl];
+        td_t* col = fetch_vec(x, dp, sc->type, sc->attrs, m);
+        if (TD_IS_ERR(col)) { td_release(res); return col; }
+        int64_t nm = j < nl ? td_table_col_name(jb->left, j) : rname[j - nl];
+        res = td_table_add_col(res, nm, col);
+        td_release(col);
+        if (TD_IS_ERR(res)) return res;
+    }
+    return res;
+}
+
+/* ---- scalar reductions ------------------------------------------------------------------------ */
+static td_t* reduce(ex_t* x, uint16_t opc, val_t* v) {
+    td_t* o = v->obj;
+    if (td_is_atom(o)) {
+        if (opc == OP_COUNT) return td_i64(1);
+        td_retain(o);
+        return o;
+    }
+    if (o->type == TD_TABLE) {
+        /* COUNT of a table counts its (selected) rows */
+        if (opc != OP_COUNT) return TD_ERR_PTR(TD_ERR_TYPE);
+        if (!v->lazy) return td_i64(td_table_nrows(o));
+        int64_t n = td_table_nrows(o);
+        void* ws = tdb_dev_alloc(&x->c, tdg_select_ws_bytes(n));
+        int64_t* dc = tdb_dev_alloc(&x->c, 8);
+        if (!ws || !dc) return TD_ERR_PTR(TD_ERR_OOM);
+        int st = CALL(tdg_select_count(n, v->has_pred ? &v->pred : NULL, v->dsel, ws, dc, x->c.stream));
+        int64_t m = 0;
+        if (!st) st = tdb_d2h(&x->c, &m, dc, 8);
+        return st ? TD_ERR_PTR(st) : td_i64(m);
+    }
+    if (!v->lazy && opc == OP_COUNT) return td_i64(o->len);
+    if (o->type == TD_BOOL || o->type == TD_SEL || o->type == TD_LIST) {
+        if (opc == OP_COUNT) return td_i64(o->len);
+    }
+    /* one-slot group-by over the vector's (selected) rows */
+    tdb_devcol dc;
+    int st = tdb_col_device(&x->c, o, 0, &dc);
+    if (st) return TD_ERR_PTR(st);
+    tdg_group_desc d;
+    memset(&d, 0, sizeof(d));
+    d.nrows = o->len;
+    d.n_aggs = 2;
+    d.aggs[0].op = opc == OP_AVG ? OP_SUM : opc;
+    d.aggs[0].in = (tdg_col){ dc.dptr, dc.type, dc.attrs, 0, {0} };
+    d.aggs[1].op = OP_COUNT;
+    d.have_range = 1;
+    tdg_group_plan plan;
+    st = tdg_group_plan_make(&d, 1, &plan);
+    if (st) return TD_ERR_PTR(st);
+    void* ws = tdb_dev_alloc(&x->c, plan.ws_bytes);
+    tdg_group_out out;
+    memset(&out, 0, sizeof(out));
+    out.d_n_groups = tdb_dev_alloc(&x->c, 8);
+    out.aggs[0] = tdb_dev_alloc(&x->c, 8 * (size_t)plan.max_groups);
+    out.aggs[1] = tdb_dev_alloc(&x->c, 8 * (size_t)plan.max_groups);
+    if (!ws || !out.d_n_groups || !out.aggs[0] || !out.aggs[1]) return TD_ERR_PTR(TD_ERR_OOM);
+    st = CALL(tdg_group_run(&d, v->has_pred ? &v->pred : NULL, v->dsel, &plan, ws, &out, x->c.stream));
+    if (st) return TD_ERR_PTR(st);
+    int64_t ng = 0;
+    uint64_t val = 0;
+    int64_t cnt = 0;
+    st = tdb_d2h(&x->c, &ng, out.d_n_groups, 8);
+    if (!st && ng > 0) st = tdb_d2h(&x->c, &val, out.aggs[0], 8);
+    if (!st && ng > 0) st = tdb_d2h(&x->c, &cnt, out.aggs[1], 8);
+    if (st) return TD_ERR_PTR(st);
+    int isf = dc.type == TD_F64;
+    double f; int64_t i;
+    memcpy(&f, &val, 8);
+    i = (int64_t)val;
+    switch (opc) {
+        case OP_COUNT: return td_i64(cnt);
+        case OP_SUM:   return isf ? td_f64(ng ? f : 0.0) : td_i64(ng ? i : 0);
+        case OP_MIN: case OP_MAX:
+            return isf ? td_f64(cnt ? f : 0.0) : td_i64(cnt ? i : 0);
+        case OP_AVG:
+            if (!cnt) return td_f64(0.0);
+            return td_f64(isf ? f / (double)cnt : (double)i / (double)cnt);
+    }
+    return TD_ERR_PTR(TD_ERR_NYI);
+}
+
+/* ---- the walk -------------------------------------------------------------------------------------- */
+static int is_elementwise(uint16_t o) {
+    return (o >= OP_NEG && o <= OP_CAST && o != OP_SQRT && o != OP_LOG && o != OP_EXP &&
+            o != OP_CEIL && o != OP_FLOOR && o != OP_ISNULL) ||
+           (o >= OP_ADD && o <= OP_MAX2);
+}
+
+static td_op_ext_t* single_join(td_graph_t* g) {
+    td_op_ext_t* found = NULL;
+    for (uint32_t i = 0; i < g->ext_count; i++) {
+        td_op_ext_t* e = g->ext_nodes[i];
+        if (e && g->nodes[e->base.id].opcode == OP_JOIN) {
+            if (found) return NULL;
+            found = e;
+        }
+    }
+    return found;
+}
+
+static td_t* exec_group_node(ex_t* x, td_op_t* op) {
+    td_op_ext_t* ext = tdb_find_ext(x->g, op->id);
+    if (!ext) return TD_ERR_PTR(TD_ERR_NYI);
+    td_graph_t* g = x->g;
+    if (!g->table) {
+        td_op_ext_t* jext = single_join(g);
+        if (!jext) return TD_ERR_PTR(TD_ERR_SCHEMA);
+        /* fused filter -> join -> group: the join is probed, never materialized */
+        val_t lv = vnone(), rv = vnone();
+        td_t* r = exec_value(x, jext->base.inputs[0], &lv);
+        if (TD_IS_ERR(r)) return r;
+        r = exec_value(x, jext->base.inputs[1], &rv);
+        if (TD_IS_ERR(r)) { vfree(&lv); return r; }
+        td_t* right = dense_side(x, &rv);
+        td_t* res;
+        if (TD_IS_ERR(right)) {
+            res = right;
+        } else {
+            jbuilt_t jb;
+            int st = prepare_join(x, jext, &lv, right, &jb);
+            if (st) {
+                res = TD_ERR_PTR(st);
+            } else {
+                jsrc_t js = { lv.obj, right, jext };
+                jrun_t jr = { &jb.d, &jb.p, jb.ws };
+                res = run_group(x, ext, NULL, lv.has_pred ? &lv.pred : NULL, lv.dsel, &js, &jr);
+            }
+            td_release(right);
+        }
+        vfree(&lv);
+        vfree(&rv);
+        return res;
+    }
+    /* the caller's TD_SEL (if any) restricts the rows */
+    const uint64_t* dsel = NULL;
+    if (g->selection && g->selection->type == TD_SEL && g->selection->len == td_table_nrows(g->table)) {
+        size_t bytes = (size_t)((g->selection->len + 63) / 64) * 8;
+        void* d = tdb_dev_alloc(&x->c, bytes ? bytes : 8);
+        if (!d) return TD_ERR_PTR(TD_ERR_OOM);
+        int st = tdb_h2d(&x->c, d, td_sel_bits(g->selection), bytes);
+        if (st) return TD_ERR_PTR(st);
+        dsel = d;
+    }
+    return run_group(x, ext, g->table, NULL, dsel, NULL, NULL);
+}
+
+/* Evaluate op; sets *out (retained value) and returns its obj or an error. */
+static td_t* exec_value(ex_t* x, td_op_t* op, val_t* out) {
+    *out = vnone();
+    if (!op) return TD_ERR_PTR(TD_ERR_NYI);
+    int st = tdb_check_cancel();
+    if (st) return TD_ERR_PTR(st);
+    td_graph_t* g = x->g;
+    switch (op->opcode) {
+        case OP_SCAN: {
+            td_op_ext_t* ext = tdb_find_ext(g, op->id);
+            if (!ext) return TD_ERR_PTR(TD_ERR_NYI);
+            td_t* t = scan_table_of(x, ext, g->table);
+            td_t* col = t ? td_table_get_col(t, ext->sym) : NULL;
+            if (!col) return TD_ERR_PTR(TD_ERR_SCHEMA);
+            td_retain(col);
+            out->obj = col;
+            return col;
+        }
+        case OP_CONST: {
+            td_op_ext_t* ext = tdb_find_ext(g, op->id);
+            if (!ext || !ext->literal) return TD_ERR_PTR(TD_ERR_NYI);
+            td_retain(ext->literal);
+            out->obj = ext->literal;
+            return out->obj;
+        }
+        case OP_ALIAS: case OP_MATERIALIZE:
+            return exec_value(x, op->inputs[0], out);
+        case OP_FILTER: {
+            td_op_t* child = op->inputs[0];
+            if (child && child->opcode == OP_GROUP) {
+                /* HAVING: the predicate reads the group-by result */
+                td_t* grp = exec_group_node(x, child);
+                if (TD_IS_ERR(grp)) return grp;
+                tdg_expr p;
+                st = compile_expr(x, grp, op->inputs[1], &p);
+                if (st) { td_release(grp); return TD_ERR_PTR(st); }
+                out->obj = grp;
+                out->lazy = 1;
+                out->has_pred = 1;
+                out->pred = p;
+                return grp;
+            }
+            val_t in;
+            td_t* r = exec_value(x, child, &in);
+            if (TD_IS_ERR(r)) return r;
+            td_t* rows_tbl = in.obj->type == TD_TABLE ? in.obj : g->table;
+            if (!rows_tbl) { vfree(&in); return TD_ERR_PTR(TD_ERR_SCHEMA); }
+            if (in.obj->type != TD_TABLE && in.obj->len != td_table_nrows(rows_tbl)) {
+                vfree(&in);
+                return TD_ERR_PTR(TD_ERR_LENGTH);
+            }
+            tdg_expr p;
+            st = compile_expr(x, rows_tbl, op->inputs[1], &p);
+            if (!st) {
+                if (!in.has_pred) { memset(&in.pred, 0, sizeof(in.pred)); }
+                st = expr_and(&in.pred, &p);
+            }
+            if (st) { vfree(&in); return TD_ERR_PTR(st); }
+            in.lazy = 1;
+            in.has_pred = 1;
+            *out = in;
+            return out->obj;
+        }
+        case OP_GROUP: {
+            td_t* r = exec_group_node(x, op);
+            if (TD_IS_ERR(r)) return r;
+            out->obj = r;
+            return r;
+        }
+        case OP_JOIN: {
+            val_t lv, rv;
+            td_t* r = exec_value(x, op->inputs[0], &lv);
+            if (TD_IS_ERR(r)) return r;
+            r = exec_value(x, op->inputs[1], &rv);
+            if (TD_IS_ERR(r)) { vfree(&lv); return r; }
+            td_op_ext_t* ext = tdb_find_ext(g, op->id);
+            td_t* right = ext ? dense_side(x, &rv) : TD_ERR_PTR(TD_ERR_NYI);
+            td_t* res = right;
+            if (!TD_IS_ERR(right)) {
+                jbuilt_t jb;
+                st = prepare_join(x, ext, &lv, right, &jb);
+                res = st ? TD_ERR_PTR(st) : join_materialize(x, ext, &lv, &jb);
+                td_release(right);
+            }
+            vfree(&lv);
+            vfree(&rv);
+            if (TD_IS_ERR(res)) return res;
+            out->obj = res;
+            return res;
+        }
+        case OP_COUNT: case OP_SUM: case OP_MIN: case OP_MAX: case OP_AVG: {
+            val_t in;
+            td_t* r = exec_value(x, op->inputs[0], &in);
+            if (TD_IS_ERR(r)) return r;
+            td_t* res = reduce(x, op->opcode, &in);
+            vfree(&in);
+            if (TD_IS_ERR(res)) return res;
+            out->obj = res;
+            return res;
+        }
+        default:
+            break;
+    }
+    if (is_elementwise(op->opcode)) {
+        if (!g->table) return TD_ERR_PTR(TD_ERR_SCHEMA);
+        tdg_expr e;
+        st = compile_expr(x, g->table, op, &e);
+        if (st) return TD_ERR_PTR(st);
+        int64_t n = td_table_nrows(g->table);
+        int kind = e.ins[e.out].kind;
+        int is_bool = op->out_type == TD_BOOL || (op->opcode >= OP_EQ && op->opcode <= OP_OR) || op->opcode == OP_NOT;
+        int out_kind = is_bool ? 2 : kind;
+        void* d = tdb_dev_alloc(&x->c, (size_t)(n ? n : 1) * 8);
+        if (!d) return TD_ERR_PTR(TD_ERR_OOM);
+        st = CALL(tdg_eval(&e, n, d, out_kind, x->c.stream));
+        if (st) return TD_ERR_PTR(st);
+        td_t* v = fetch_vec(x, d, is_bool ? TD_BOOL : (kind ? TD_F64 : TD_I64), 0, n);
+        if (TD_IS_ERR(v)) return v;
+        out->obj = v;
+        return v;
+    }
+    return TD_ERR_PTR(TD_ERR_NYI);
+}
+
+td_t* tdb_exec(td_graph_t* g, td_op_t* root) {
+    ex_t x;
+    memset(&x, 0, sizeof(x));
+    x.g = g;
+    tdb_reset_methods();
+    int st = tdb_ctx_begin(&x.c);
+    if (st) return TD_ERR_PTR(st);
+    val_t v;
+    td_t* r = exec_value(&x, root, &v);
+    td_t* res;
+    if (TD_IS_ERR(r)) {
+        res = r;
+    } else {
+        res = materialize(&x, &v);
+        vfree(&v);
+    }
+    tdb_ctx_end(&x.c);
+    if (g->selection) { td_release(g->selection); g->selection = NULL; }
+    return res;
+}
+
+td_t* td_execute(td_graph_t* g, td_op_t* root) {
+    if (!g || !root) return TD_ERR_PTR(TD_ERR_NYI);
+    atomic_store(&tdb_cancel_flag, 0);
+    return tdb_exec(g, root);
+}

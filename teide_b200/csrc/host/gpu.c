@@ -1,0 +1,442 @@
+/*
+ * Device residency for td_t columns: the device arena, host<->device copies,
+ * resident (pinned) tables with per-column statistics, and the per-call
+ * execution context.
+ *
+ * Teide keeps columns in its host buddy heap only (src/mem/heap.c).  Here a
+ * column can additionally have a device mirror:
+ *   - resident mirrors (td_gpu_pin) live until unpinned, or until the host
+ *     block is freed or mutated through the td_* API (td_cow / td_vec_set /
+ *     td_vec_append / td_vec_set_null all call tdb_mirror_forget);
+ *   - transient mirrors are uploaded by one td_execute call and released when
+ *     it returns.
+ * Resident integer columns carry min/max statistics computed once at upload;
+ * the group-by and join planners use them to choose direct arrays/maps.
+ *
+ * Device memory comes from a caching arena over cudaMalloc (freed blocks are
+ * kept for reuse; td_gpu_trim returns them).  td_gpu_set_mem_limit caps the
+ * bytes held, which is how out-of-memory handling is tested without
+ * exhausting a real GPU.
+ */
+
+#include "internal.h"
+#include <cuda_runtime_api.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+_Atomic(int) tdb_cancel_flag;
+
+static pthread_mutex_t mu = PTHREAD_MUTEX_INITIALIZER;
+static int gpu_probe = -1;        /* -1 unknown, else device count */
+static int gpu_ready;
+
+/* ---- device arena -------------------------------------------------------------- */
+typedef struct { void* p; size_t sz; } dblk;
+static dblk* freel; static int n_free, cap_free;
+static dblk* live;  static int n_live, cap_live;
+static size_t live_bytes, peak_bytes, cached_bytes, mem_limit;
+
+static size_t round_sz(size_t n) {
+    if (n < 512) return 512;
+    if (n < ((size_t)2 << 20)) { size_t p = 512; while (p < n) p <<= 1; return p; }
+    return (n + ((size_t)2 << 20) - 1) & ~(((size_t)2 << 20) - 1);
+}
+
+static int push(dblk** a, int* n, int* cap, void* p, size_t sz) {
+    if (*n == *cap) {
+        int nc = *cap ? *cap * 2 : 64;
+        dblk* na = realloc(*a, (size_t)nc * sizeof(dblk));
+        if (!na) return 0;
+        *a = na; *cap = nc;
+    }
+    (*a)[(*n)++] = (dblk){p, sz};
+    return 1;
+}
+
+static void release_cached_locked(void) {
+    for (int i = 0; i < n_free; i++) cudaFree(freel[i].p);
+    n_free = 0;
+    cached_bytes = 0;
+}
+
+static void* arena_alloc(size_t bytes) {
+    size_t sz = round_sz(bytes ? bytes : 1);
+    pthread_mutex_lock(&mu);
+    if (mem_limit && live_bytes + sz > mem_limit) { pthread_mutex_unlock(&mu); return NULL; }
+    int best = -1;
+    for (int i = 0; i < n_free; i++)
+        if (freel[i].sz >= sz && freel[i].sz <= sz + sz / 4 + ((size_t)2 << 20) &&
+            (best < 0 || freel[i].sz < freel[best].sz)) best = i;
+    void* p = NULL;
+    if (best >= 0) {
+        p = freel[best].p;
+        sz = freel[best].sz;
+        cached_bytes -= sz;
+        freel[best] = freel[--n_free];
+    } else if (cudaMalloc(&p, sz) != cudaSuccess) {
+        cudaGetLastError();
+        release_cached_locked();
+        if (cudaMalloc(&p, sz) != cudaSuccess) { cudaGetLastError(); p = NULL; }
+    }
+    if (p && !push(&live, &n_live, &cap_live, p, sz)) { cudaFree(p); p = NULL; }
+    if (p) {
+        live_bytes += sz;
+        if (live_bytes > peak_bytes) peak_bytes = live_bytes;
+    }
+    pthread_mutex_unlock(&mu);
+    return p;
+}
+
+static void arena_free(void* p) {
+    if (!p) return;
+    pthread_mutex_lock(&mu);
+    for (int i = 0; i < n_live; i++) {
+        if (live[i].p == p) {
+            size_t sz = live[i].sz;
+            live[i] = live[--n_live];
+            live_bytes -= sz;
+            if (push(&freel, &n_free, &cap_free, p, sz)) cached_bytes += sz;
+            else cudaFree(p);
+            break;
+        }
+    }
+    pthread_mutex_unlock(&mu);
+}
+
+void td_gpu_trim(void) {
+    pthread_mutex_lock(&mu);
+    if (gpu_ready) release_cached_locked();
+    pthread_mutex_unlock(&mu);
+}
+
+void td_gpu_set_mem_limit(size_t bytes) {
+    pthread_mutex_lock(&mu);
+    mem_limit = bytes;
+    pthread_mutex_unlock(&mu);
+}
+
+void* tdb_dev_alloc_persistent(size_t bytes) { return arena_alloc(bytes); }
+void  tdb_dev_free_persistent(void* p) { arena_free(p); }
+
+/* ---- device presence ---------------------------------------------------------------- */
+int tdb_gpu_available(void) {
+    pthread_mutex_lock(&mu);
+    if (gpu_probe < 0) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess) { cudaGetLastError(); n = 0; }
+        gpu_probe = n;
+    }
+    int n = gpu_probe;
+    pthread_mutex_unlock(&mu);
+    return n > 0;
+}
+
+int td_gpu_device_count(void) {
+    tdb_gpu_available();
+    return gpu_probe < 0 ? 0 : gpu_probe;
+}
+
+int tdb_gpu_ensure(void) {
+    if (!tdb_gpu_available()) return TD_ERR_IO;
+    pthread_mutex_lock(&mu);
+    if (!gpu_ready) {
+        const char* env = getenv("TD_GPU_DEVICE");
+        int dev = env ? atoi(env) : -1;
+        if (dev >= 0) cudaSetDevice(dev);
+        if (cudaFree(0) != cudaSuccess) { cudaGetLastError(); pthread_mutex_unlock(&mu); return TD_ERR_IO; }
+        gpu_ready = 1;
+    }
+    pthread_mutex_unlock(&mu);
+    return TD_OK;
+}
+
+int tdb_check_cancel(void) { return atomic_load(&tdb_cancel_flag) ? TD_ERR_CANCEL : TD_OK; }
+
+/* ---- resident mirrors ------------------------------------------------------------------ */
+typedef struct {
+    td_t*      host;
+    uint64_t   serial;
+    tdb_devcol dc;
+    size_t     bytes;
+} mirror_t;
+
+static mirror_t* mirrors; static int n_mir, cap_mir;
+
+static int find_mirror_locked(td_t* v) {
+    uint64_t s = tdb_block_serial(v);
+    for (int i = 0; i < n_mir; i++) if (mirrors[i].host == v && mirrors[i].serial == s) return i;
+    return -1;
+}
+
+static void drop_mirror_locked(int i) {
+    void* p = mirrors[i].dc.dptr;
+    mirrors[i] = mirrors[--n_mir];
+    pthread_mutex_unlock(&mu);
+    arena_free(p);
+    pthread_mutex_lock(&mu);
+}
+
+void tdb_mirror_forget(td_t* v) {
+    if (!v || TD_IS_ERR(v) || !n_mir) return;
+    pthread_mutex_lock(&mu);
+    for (int i = n_mir - 1; i >= 0; i--) if (mirrors[i].host == v) drop_mirror_locked(i);
+    pthread_mutex_unlock(&mu);
+}
+
+void tdb_gpu_on_free(td_t* v, tdb_block_prefix* p) {
+    tdb_mirror_forget(v);
+    if (atomic_load(&p->pinned)) {
+        cudaHostUnregister(p->raw);
+        cudaGetLastError();
+        atomic_store(&p->pinned, 0);
+    }
+}
+
+static size_t col_bytes(td_t* col) {
+    return (size_t)col->len * td_sym_elem_size(col->type, col->attrs);
+}
+
+/* Page-lock the used part of a large host block once, so uploads from it
+ * run as DMA at link speed instead of through a staging buffer. */
+static void pin_host(td_t* col) {
+    if (!tdb_is_heap_block(col) || getenv("TD_GPU_NO_HOST_PIN")) return;
+    tdb_block_prefix* p = tdb_prefix(col);
+    if (p->kind != TDB_BLK_MMAP || atomic_load(&p->pinned)) return;
+    size_t used = sizeof(tdb_block_prefix) + 32 + col_bytes(col);
+    used = (used + 4095) & ~(size_t)4095;
+    if (used > p->raw_size) used = p->raw_size;
+    if (cudaHostRegister(p->raw, used, cudaHostRegisterPortable) == cudaSuccess)
+        atomic_store(&p->pinned, used);
+    else
+        cudaGetLastError();
+}
+
+static int upload(tdb_ctx* c, td_t* col, tdb_devcol* out, int persistent) {
+    size_t bytes = col_bytes(col);
+    void* d = persistent ? arena_alloc(bytes) : tdb_dev_alloc(c, bytes);
+    if (!d) return TD_ERR_OOM;
+    if (bytes) {
+        pin_host(col);
+        if (cudaMemcpyAsync(d, td_data(col), bytes, cudaMemcpyHostToDevice, (cudaStream_t)c->stream) != cudaSuccess) {
+            cudaGetLastError();
+            if (persistent) arena_free(d);
+            return TD_ERR_IO;
+        }
+        c->h2d_bytes += bytes;
+    }
+    memset(out, 0, sizeof(*out));
+    out->dptr = d;
+    out->len = col->len;
+    out->type = col->type;
+    out->attrs = col->attrs;
+    return TD_OK;
+}
+
+static int is_int_type(int8_t t) {
+    return t == TD_BOOL || t == TD_U8 || t == TD_CHAR || t == TD_I16 || t == TD_I32 || t == TD_I64 ||
+           t == TD_DATE || t == TD_TIME || t == TD_TIMESTAMP || t == TD_SYM;
+}
+
+static int compute_stats(tdb_ctx* c, tdb_devcol* dc) {
+    if (!is_int_type(dc->type)) return TD_OK;
+    int64_t* d = tdb_dev_alloc(c, 16);
+    if (!d) return TD_ERR_OOM;
+    tdg_col col = { dc->dptr, dc->type, dc->attrs, 0, {0} };
+    int st = tdg_minmax(col, dc->len, d, c->stream);
+    if (st) return st;
+    int64_t mm[2];
+    st = tdb_d2h(c, mm, d, 16);
+    if (st) return st;
+    dc->kmin = mm[0];
+    dc->kmax = mm[1];
+    dc->has_stats = 1;
+    return TD_OK;
+}
+
+/* ---- execution context ------------------------------------------------------------------- */
+typedef struct { td_t* host; uint64_t serial; tdb_devcol dc; } tmirror_t;
+static _Thread_local void* tls_stream;
+static _Thread_local tmirror_t* tls_tm;
+static _Thread_local int tls_ntm, tls_captm;
+
+int tdb_ctx_begin(tdb_ctx* c) {
+    memset(c, 0, sizeof(*c));
+    int st = tdb_gpu_ensure();
+    if (st) return st;
+    if (!tls_stream) {
+        cudaStream_t s;
+        if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) { cudaGetLastError(); return TD_ERR_IO; }
+        tls_stream = s;
+    }
+    c->stream = tls_stream;
+    tls_ntm = 0;
+    return TD_OK;
+}
+
+void* tdb_dev_alloc(tdb_ctx* c, size_t bytes) {
+    void* p = arena_alloc(bytes);
+    if (!p) return NULL;
+    if (c->n_tmp == c->cap_tmp) {
+        int nc = c->cap_tmp ? c->cap_tmp * 2 : 32;
+        void** nt = realloc(c->tmp, (size_t)nc * sizeof(void*));
+        if (!nt) { arena_free(p); return NULL; }
+        c->tmp = nt; c->cap_tmp = nc;
+    }
+    c->tmp[c->n_tmp++] = p;
+    return p;
+}
+
+int tdb_ctx_sync(tdb_ctx* c) {
+    if (cudaStreamSynchronize((cudaStream_t)c->stream) != cudaSuccess) { cudaGetLastError(); return TD_ERR_IO; }
+    return TD_OK;
+}
+
+static td_gpu_stats_t last_stats;
+static _Atomic(uint64_t) kernel_calls;
+void tdb_note_kernel(void) { atomic_fetch_add(&kernel_calls, 1); }
+void tdb_note_methods(int group, int join, int fused) {
+    if (group) last_stats.last_group_method = group;
+    if (join) last_stats.last_join_method = join;
+    if (fused) last_stats.last_fused = fused;
+}
+
+void tdb_ctx_end(tdb_ctx* c) {
+    if (c->stream) cudaStreamSynchronize((cudaStream_t)c->stream);
+    for (int i = 0; i < c->n_tmp; i++) arena_free(c->tmp[i]);
+    free(c->tmp);
+    c->tmp = NULL;
+    c->n_tmp = c->cap_tmp = 0;
+    tls_ntm = 0;
+    pthread_mutex_lock(&mu);
+    last_stats.h2d_bytes = c->h2d_bytes;
+    last_stats.d2h_bytes = c->d2h_bytes;
+    last_stats.kernel_calls = atomic_exchange(&kernel_calls, 0);
+    last_stats.dev_bytes_live = live_bytes;
+    last_stats.dev_bytes_peak = peak_bytes;
+    pthread_mutex_unlock(&mu);
+}
+
+void td_gpu_last_stats(td_gpu_stats_t* out) {
+    if (!out) return;
+    pthread_mutex_lock(&mu);
+    *out = last_stats;
+    pthread_mutex_unlock(&mu);
+}
+
+void tdb_reset_methods(void) {
+    pthread_mutex_lock(&mu);
+    last_stats.last_group_method = last_stats.last_join_method = last_stats.last_fused = 0;
+    pthread_mutex_unlock(&mu);
+}
+
+int tdb_d2h(tdb_ctx* c, void* host, const void* dev, size_t bytes) {
+    if (!bytes) return TD_OK;
+    if (cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)c->stream) != cudaSuccess ||
+        cudaStreamSynchronize((cudaStream_t)c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return TD_ERR_IO;
+    }
+    c->d2h_bytes += bytes;
+    return TD_OK;
+}
+
+int tdb_h2d(tdb_ctx* c, void* dev, const void* host, size_t bytes) {
+    if (!bytes) return TD_OK;
+    if (cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, (cudaStream_t)c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return TD_ERR_IO;
+    }
+    c->h2d_bytes += bytes;
+    return TD_OK;
+}
+
+int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
+    if (!col || TD_IS_ERR(col) || col->type <= 0 || col->type == TD_TABLE || col->type == TD_LIST ||
+        col->type == TD_SEL)
+        return TD_ERR_TYPE;
+    if (col->attrs & TD_ATTR_SLICE) return TD_ERR_NYI;
+    uint64_t serial = tdb_block_serial(col);
+    pthread_mutex_lock(&mu);
+    int i = find_mirror_locked(col);
+    if (i >= 0 && mirrors[i].dc.len == col->len) {
+        *out = mirrors[i].dc;
+        pthread_mutex_unlock(&mu);
+        return TD_OK;
+    }
+    pthread_mutex_unlock(&mu);
+    for (int k = 0; k < tls_ntm; k++) {
+        if (tls_tm[k].host == col && tls_tm[k].serial == serial && tls_tm[k].dc.len == col->len) {
+            if (want_stats && !tls_tm[k].dc.has_stats) {
+                int st = compute_stats(c, &tls_tm[k].dc);
+                if (st) return st;
+            }
+            *out = tls_tm[k].dc;
+            return TD_OK;
+        }
+    }
+    if (tls_ntm == tls_captm) {
+        int nc = tls_captm ? tls_captm * 2 : 16;
+        tmirror_t* nt = realloc(tls_tm, (size_t)nc * sizeof(tmirror_t));
+        if (!nt) return TD_ERR_OOM;
+        tls_tm = nt; tls_captm = nc;
+    }
+    tmirror_t* t = &tls_tm[tls_ntm];
+    t->host = col;
+    t->serial = serial;
+    int st = upload(c, col, &t->dc, 0);
+    if (st) return st;
+    if (want_stats) {
+        st = compute_stats(c, &t->dc);
+        if (st) return st;
+    }
+    tls_ntm++;
+    *out = t->dc;
+    return TD_OK;
+}
+
+td_err_t td_gpu_pin(td_t* tbl) {
+    if (!tbl || TD_IS_ERR(tbl)) return TD_ERR_TYPE;
+    tdb_ctx c;
+    int st = tdb_ctx_begin(&c);
+    if (st) return (td_err_t)st;
+    int64_t nc = tbl->type == TD_TABLE ? td_table_ncols(tbl) : 1;
+    for (int64_t j = 0; j < nc && !st; j++) {
+        td_t* col = tbl->type == TD_TABLE ? td_table_get_col_idx(tbl, j) : tbl;
+        if (!col || col->type <= 0 || col->type == TD_TABLE || col->type == TD_LIST) continue;
+        pthread_mutex_lock(&mu);
+        int have = find_mirror_locked(col) >= 0;
+        pthread_mutex_unlock(&mu);
+        if (have) continue;
+        tdb_devcol dc;
+        st = upload(&c, col, &dc, 1);
+        if (st) break;
+        st = compute_stats(&c, &dc);
+        if (st) { arena_free(dc.dptr); break; }
+        pthread_mutex_lock(&mu);
+        if (n_mir == cap_mir) {
+            int ncap = cap_mir ? cap_mir * 2 : 64;
+            mirror_t* nm = realloc(mirrors, (size_t)ncap * sizeof(mirror_t));
+            if (!nm) { pthread_mutex_unlock(&mu); arena_free(dc.dptr); st = TD_ERR_OOM; break; }
+            mirrors = nm; cap_mir = ncap;
+        }
+        mirrors[n_mir++] = (mirror_t){ col, tdb_block_serial(col), dc, col_bytes(col) };
+        pthread_mutex_unlock(&mu);
+    }
+    tdb_ctx_end(&c);
+    if (st) td_gpu_unpin(tbl);
+    return (td_err_t)st;
+}
+
+void td_gpu_unpin(td_t* tbl) {
+    if (!tbl || TD_IS_ERR(tbl)) return;
+    if (tbl->type != TD_TABLE) { tdb_mirror_forget(tbl); return; }
+    for (int64_t j = 0; j < td_table_ncols(tbl); j++) tdb_mirror_forget(td_table_get_col_idx(tbl, j));
+}
+
+/* ---- execution control ------------------------------------------------------------------- */
+td_err_t td_pool_init(uint32_t n_workers) { (void)n_workers; return TD_OK; }
+void td_pool_destroy(void) {}
+void td_cancel(void) { atomic_store(&tdb_cancel_flag, 1); }
+
+uint32_t td_thread_count(void) { return 1; }

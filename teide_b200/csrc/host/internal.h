@@ -1,0 +1,92 @@
+/*
+ * Internal declarations shared by the host-side C17 sources of
+ * libteide_b200.so.  Nothing here is part of the public ABI.
+ */
+#ifndef TDB_INTERNAL_H
+#define TDB_INTERNAL_H
+
+#include "teide/td.h"
+#include "teide/td_b200.h"
+#include "tdg.h"
+#include <stdatomic.h>
+
+/* ---- heap ------------------------------------------------------------------
+ * Every block carries a 64-byte hidden prefix in front of its td_t header.
+ * Blocks of 2 MB and more come from mmap (pages committed on first touch)
+ * and are page-locked on their first upload to the GPU, so host->device
+ * copies of large columns run at PCIe/C2C link speed. */
+typedef struct tdb_block_prefix {
+    uint32_t magic;
+    uint32_t kind;          /* TDB_BLK_MALLOC or TDB_BLK_MMAP */
+    void*    raw;           /* start of the OS allocation */
+    size_t   raw_size;      /* bytes of the OS allocation */
+    _Atomic(size_t) pinned; /* bytes page-locked with cudaHostRegister */
+    uint64_t serial;        /* allocation serial: device mirrors key on it */
+    uint8_t  pad[16];
+} tdb_block_prefix;
+
+#define TDB_BLK_MAGIC 0x7D6B1C0Au
+#define TDB_BLK_MALLOC 1u
+#define TDB_BLK_MMAP   2u
+
+static inline tdb_block_prefix* tdb_prefix(td_t* v) {
+    return (tdb_block_prefix*)((char*)v - sizeof(tdb_block_prefix));
+}
+
+void     tdb_retain_owned_refs(td_t* v);
+int      tdb_is_heap_block(td_t* v);
+uint64_t tdb_block_serial(td_t* v);
+
+/* ---- atoms / vectors -------------------------------------------------------- */
+int64_t tdb_vec_capacity(td_t* v);
+int     tdb_atom_numeric(td_t* a, double* f, int64_t* i, int* is_f64);
+
+/* ---- graph ------------------------------------------------------------------ */
+td_op_ext_t* tdb_find_ext(td_graph_t* g, uint32_t id);
+
+/* ---- GPU residency (gpu.c) ---------------------------------------------------- */
+typedef struct tdb_devcol {
+    void*    dptr;      /* device copy of the element data */
+    int64_t  len;
+    int8_t   type;
+    uint8_t  attrs;
+    int      has_stats; /* min/max valid */
+    int64_t  kmin, kmax;
+} tdb_devcol;
+
+/* execution context of one td_execute call */
+typedef struct tdb_ctx {
+    void*    stream;            /* cudaStream_t */
+    int      device;
+    /* transient device buffers freed at the end of the call */
+    void**   tmp;
+    int      n_tmp, cap_tmp;
+    /* host->device bytes uploaded in this call (for statistics) */
+    uint64_t h2d_bytes, d2h_bytes;
+} tdb_ctx;
+
+int      tdb_gpu_ensure(void);                 /* 0 ok, else td_err_t */
+int      tdb_gpu_available(void);              /* 1 if a CUDA device exists */
+void*    tdb_dev_alloc(tdb_ctx* c, size_t bytes);   /* transient, freed by ctx_end */
+void*    tdb_dev_alloc_persistent(size_t bytes);
+void     tdb_dev_free_persistent(void* p);
+int      tdb_ctx_begin(tdb_ctx* c);
+void     tdb_ctx_end(tdb_ctx* c);
+int      tdb_ctx_sync(tdb_ctx* c);               /* 0 ok, else td_err_t */
+/* device view of a host column, copied into *out; uploads it unless it is
+ * resident.  want_stats asks for min/max of an integer column. */
+int      tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out);
+void     tdb_note_kernel(void);
+void     tdb_note_methods(int group, int join, int fused);
+void     tdb_reset_methods(void);
+int      tdb_d2h(tdb_ctx* c, void* host, const void* dev, size_t bytes);
+int      tdb_h2d(tdb_ctx* c, void* dev, const void* host, size_t bytes);
+void     tdb_mirror_forget(td_t* v);             /* host block freed or mutated */
+int      tdb_check_cancel(void);
+
+extern _Atomic(int) tdb_cancel_flag;
+
+/* ---- executor ------------------------------------------------------------------ */
+td_t* tdb_exec(td_graph_t* g, td_op_t* root);
+
+#endif

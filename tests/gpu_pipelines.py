@@ -1,0 +1,94 @@
+"""DAG builders for the filter -> (join ->) group pipelines, shared by the GPU
+parity tests, the smoke test and the benchmark.  Each runs through the
+td.h API (td_execute) of whatever library the Td binding wraps."""
+import numpy as np
+
+from teide_b200.td import OP_COUNT
+
+
+def const(g, k):
+    return g.f64(k) if isinstance(k, float) else g.i64(k)
+
+
+def readme_group(td, tbl, pred, keys, aggs):
+    """One graph: group keys and aggregate inputs are td_filter(scan, pred)
+    vectors sharing one predicate (README.md's filter + group + sum)."""
+    g = td.graph(tbl)
+    try:
+        c, op, k = pred
+        p = g.op(op, g.scan(c), const(g, k))
+        ks = [g.filter(g.scan(name), p) for name in keys]
+        ins = [g.filter(g.scan(name), p) for _, name in aggs]
+        r = g.execute(g.group(ks, [a for a, _ in aggs], ins), optimize=True)
+    finally:
+        g.free()
+    out = td.table_dict(r)
+    td.release(r)
+    return out
+
+
+def two_graph_group(td, tbl, pred, keys, aggs):
+    """Filter graph -> compacted table -> group graph."""
+    g = td.graph(tbl)
+    try:
+        c, op, k = pred
+        t2 = g.execute(g.filter(g.const_table(tbl), g.op(op, g.scan(c), const(g, k))))
+    finally:
+        g.free()
+    g = td.graph(t2)
+    try:
+        r = g.execute(g.group([g.scan(n) for n in keys], [a for a, _ in aggs],
+                              [g.scan(n) for _, n in aggs]))
+    finally:
+        g.free()
+    out = td.table_dict(r)
+    td.release(r)
+    td.release(t2)
+    return out
+
+
+def fused_join_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_type=0):
+    """One graph bound to no table: group over join(filter(probe), build)."""
+    g = td.graph(None)
+    try:
+        c, op, k = pred
+        left = g.filter(g.const_table(probe_t), g.op(op, g.scan(c), const(g, k)))
+        g.join(left, [g.scan(lkey)], g.const_table(build_t), [g.scan(rkey)], join_type)
+        grp = g.group([g.scan(n) for n in keys], [a for a, _ in aggs], [g.scan(n) for _, n in aggs])
+        r = g.execute(grp)
+    finally:
+        g.free()
+    out = td.table_dict(r)
+    td.release(r)
+    return out
+
+
+def join_then_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_type=0):
+    """Two calls: materialized join, then a group graph over its result."""
+    g = td.graph(probe_t)
+    try:
+        c, op, k = pred
+        left = g.filter(g.const_table(probe_t), g.op(op, g.scan(c), const(g, k)))
+        jr = g.execute(g.join(left, [g.scan(lkey)], g.const_table(build_t), [g.scan(rkey)], join_type))
+    finally:
+        g.free()
+    joined = td.table_dict(jr)
+    g = td.graph(jr)
+    try:
+        r = g.execute(g.group([g.scan(n) for n in keys], [a for a, _ in aggs],
+                              [g.scan(n) for _, n in aggs]))
+    finally:
+        g.free()
+    out = td.table_dict(r)
+    td.release(r)
+    td.release(jr)
+    return out, joined
+
+
+def f64_tolerance_ok(got, want, abs_sum, rel=1e-12):
+    """|got - want| <= rel * max(|want|, sum |x|) elementwise."""
+    scale = np.maximum(np.abs(want), abs_sum)
+    return bool(np.all(np.abs(got - want) <= rel * np.maximum(scale, 1e-300)))
+
+
+CONFIG3_AGGS = [(None, "price"), (OP_COUNT, "price")]

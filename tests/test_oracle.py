@@ -1,0 +1,140 @@
+"""Pins the numpy oracle (oracle/oracle.py) to Teide itself.
+
+1. Against the committed golden fixtures, which hold Teide's own outputs
+   (generated by tests/golden/make_golden.py from the compiled reference).
+2. Against Teide's unit-test known answers.
+3. Against the compiled reference run live on fresh seeded inputs (skipped
+   where oracle/_ref/libteide_ref.so is not built).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+from teide_b200 import workloads
+from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
+
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def load(name):
+    with np.load(os.path.join(GOLD, name + ".npz")) as z:
+        return {k: z[k] for k in z.files}
+
+
+def pick(z, prefix):
+    return {k[len(prefix):]: v for k, v in z.items() if k.startswith(prefix)}
+
+
+def assert_group_equal(got, want, keys, ftol=1e-12):
+    got = oracle.canonical(got, by=keys)
+    want = oracle.canonical(want, by=keys)
+    assert list(got) == list(want), (list(got), list(want))
+    for k in want:
+        g, w = np.asarray(got[k]), np.asarray(want[k])
+        assert g.shape == w.shape, k
+        if w.dtype.kind == "f":
+            scale = np.maximum(np.abs(w), 1.0)
+            assert np.all(np.abs(g - w) <= ftol * scale), k
+        else:
+            assert np.array_equal(g, w), k
+
+
+def test_oracle_config1_golden():
+    z = load("config1_small")
+    cin = pick(z, "in_")
+    m = oracle.conj(cin, [("flag", "eq", 0)])
+    got = oracle.group({"region": cin["region"]}, [(OP_SUM, "amount", cin["amount"])], m)
+    assert_group_equal(got, pick(z, "out_"), ["region"])
+
+
+def test_oracle_config2_golden():
+    z = load("config2_small")
+    c = pick(z, "in_")
+    m = oracle.conj(c, [("v1", "gt", 0)])
+    got = oracle.group({"key": c["key"]}, [(OP_COUNT, "v1", None), (OP_SUM, "v1", c["v1"]),
+                                           (OP_MIN, "v1", c["v1"]), (OP_MAX, "v1", c["v1"]),
+                                           (OP_AVG, "v2", c["v2"])], m)
+    assert_group_equal(got, pick(z, "out_"), ["key"])
+
+
+def test_oracle_config3_golden():
+    z = load("config3_small")
+    b, p = pick(z, "b_"), pick(z, "p_")
+    m = oracle.conj(p, [("qty", "gt", 10)])
+    j = oracle.join(p, b, ["fk"], ["pk"], 0, m)
+    assert oracle.canonical(j).keys() == pick(z, "join_").keys()
+    for k, v in oracle.canonical(j).items():
+        assert np.array_equal(v, pick(z, "join_")[k]), k
+    got = oracle.group({"cat": j["cat"]}, [(OP_SUM, "price", j["price"]), (OP_COUNT, "price", None)])
+    assert_group_equal(got, pick(z, "out_"), ["cat"])
+
+
+@pytest.mark.parametrize("jt", [0, 1, 2])
+def test_oracle_outer_join_golden(jt):
+    z = load("join_outer_small")
+    left, right = pick(z, "l_"), pick(z, "r_")
+    got = oracle.canonical(oracle.join(left, right, ["id"], ["id"], jt))
+    want = pick(z, f"j{jt}_")
+    assert list(got) == list(want)
+    for k in want:
+        assert np.array_equal(got[k], want[k]), k
+
+
+def test_oracle_known_answers():
+    id1 = np.array([1, 1, 2, 2, 3, 3, 1, 2, 3, 1])
+    v1 = np.array([10, 20, 30, 40, 50, 60, 70, 80, 90, 100])
+    cols = {"v1": v1}
+    for op, n in {"eq": 1, "ne": 9, "lt": 4, "le": 5, "gt": 5, "ge": 6}.items():
+        assert oracle.conj(cols, [("v1", op, 50)]).sum() == n
+    g = oracle.group({"id1": id1}, [(OP_SUM, "v1", v1)])
+    assert dict(zip(g["id1"], g["v1_sum"])) == {1: 200, 2: 150, 3: 200}
+    i = np.arange(100_000)
+    li, ri = oracle.join_pairs([i % 50000], [i % 50000])
+    assert len(li) == 200_000 and (i * 10)[ri].sum() == 99_999_000_000
+    li, ri = oracle.join_pairs([i[:80000]], [i[:80000] + 40000], 2)
+    assert len(li) == 120_000
+    li, ri = oracle.join_pairs([np.full(100_000, 42)], [i], 0)
+    assert len(li) == 100_000 and ((i * 7)[ri] == 294).all()
+
+
+def test_oracle_integer_sum_wraps():
+    big = np.array([2**62, 2**62, 2**62, -5], np.int64)
+    g = oracle.group({"k": np.zeros(4, np.int64)}, [(OP_SUM, "v", big)])
+    with np.errstate(over="ignore"):
+        assert g["v_sum"][0] == np.int64(2**62) * 3 - 5
+
+
+# ---- live comparison with the compiled reference -----------------------------------
+
+def _ref_group(ref, cols, pred, keys, aggs):
+    import sys
+    sys.path.insert(0, GOLD)
+    from make_golden import ref_filter_group
+    return ref_filter_group(ref, cols, pred, keys, aggs)
+
+
+@pytest.mark.parametrize("seed", [7, 8])
+def test_oracle_vs_reference_filter_group(ref, seed):
+    c = workloads.config2(n=60_000, seed=seed, nkeys=1 << 14)
+    aggs = [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")]
+    want = _ref_group(ref, c, ("v1", "gt", 0), ["key"], aggs)
+    m = oracle.conj(c, [("v1", "gt", 0)])
+    got = oracle.group({"key": c["key"]}, [(a, nm, None if a == OP_COUNT else c[nm]) for a, nm in aggs], m)
+    assert_group_equal(got, want, ["key"])
+
+
+def test_oracle_vs_reference_filter_join_group(ref):
+    import sys
+    sys.path.insert(0, GOLD)
+    from make_golden import ref_filter_join_group
+    b, p = workloads.config3(n_build=20_000, n_probe=80_000, seed=9)
+    want, joined = ref_filter_join_group(ref, b, p, ("qty", "gt", 10), "fk", "pk", ["cat"],
+                                         [(OP_SUM, "price"), (OP_COUNT, "price")])
+    m = oracle.conj(p, [("qty", "gt", 10)])
+    j = oracle.join(p, b, ["fk"], ["pk"], 0, m)
+    for k, v in oracle.canonical(j).items():
+        assert np.array_equal(v, joined[k]), k
+    got = oracle.group({"cat": j["cat"]}, [(OP_SUM, "price", j["price"]), (OP_COUNT, "price", None)])
+    assert_group_equal(got, want, ["cat"])
