@@ -83,7 +83,7 @@ class Clocks:
         for line in self.proc.stdout:
             parts = [x.strip() for x in line.split(",")]
             if len(parts) == 7:
-                self.rows.append(parts)
+                self.rows.append((time.monotonic(), parts))
 
     def __exit__(self, *exc):
         if self.proc:
@@ -93,15 +93,20 @@ class Clocks:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
 
-    def summary(self):
-        if not self.rows:
+    def summary(self, t0, t1):
+        """Samples taken while [t0, t1] ran (the sampler ticks every 200 ms,
+        so a short timed region also takes the ticks just around it)."""
+        near = [r for t, r in self.rows if t0 - 0.25 <= t <= t1 + 0.25]
+        if not near and self.rows:
+            near = [r for _, r in sorted(self.rows, key=lambda x: abs(x[0] - (t0 + t1) / 2))[:3]]
+        if not near:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        sm = [float(r[0]) for r in near if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in near if r[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[3 + i] == "Active"})
+        reasons = sorted({names[i] for r in near for i in range(4) if r[3 + i] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(near)}
 
 
 # ---- workloads through the td.h API ------------------------------------------------
@@ -126,11 +131,12 @@ def run_query(td, workload, tabs):
     from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
     if workload == "join_group":
         return fused_join_group(td, tabs["build"], tabs["probe"], ("qty", "gt", 10), "fk", "pk", ["cat"],
-                                [(OP_SUM, "price"), (OP_COUNT, "price")])
+                                [(OP_SUM, "price"), (OP_COUNT, "price")], as_dict=False)
     if workload == "group_radix":
         return readme_group(td, tabs["t"], ("v1", "gt", 0), ["key"],
-                            [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")])
-    return readme_group(td, tabs["t"], ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+                            [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")],
+                            as_dict=False)
+    return readme_group(td, tabs["t"], ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")], as_dict=False)
 
 
 def stats_of(td):
@@ -264,20 +270,24 @@ def main():
         st = L.td_gpu_pin(t)
         if st:
             raise RuntimeError(f"td_gpu_pin failed: {st}")
+    clk = Clocks(local).__enter__()
     for _ in range(args.warmup):
         run_query(td, args.workload, tabs)
     barrier()
     l0 = L.tdg_launch_count()
     main_ms, build_ms = [], []
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        ev0.record()
-        for _ in range(args.steps):
-            run_query(td, args.workload, tabs)
-            main_ms.append(L.tdg_last_main_ms())
-            build_ms.append(L.tdg_last_build_ms())
-        ev1.record()
-        torch.cuda.synchronize()
+    tc0 = time.monotonic()
+    ev0.record()
+    for _ in range(args.steps):
+        run_query(td, args.workload, tabs)
+        main_ms.append(L.tdg_last_main_ms())
+        build_ms.append(L.tdg_last_build_ms())
+    ev1.record()
+    torch.cuda.synchronize()
+    tc1 = time.monotonic()
+    time.sleep(0.3)
+    clk.__exit__(None, None, None)
     elapsed = ev0.elapsed_time(ev1) / 1e3
     launches = L.tdg_launch_count() - l0
     s_res = stats_of(td)
@@ -322,7 +332,7 @@ def main():
         "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": int(s_e2e.h2d),
                 "d2h_bytes_per_step": int(s_e2e.d2h), "steps": e2e_steps},
         "gpu_launches": int(launches),
-        "clocks": clk.summary(),
+        "clocks": clk.summary(tc0, tc1),
         "resident_h2d_bytes_per_step": int(s_res.h2d),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
@@ -336,7 +346,7 @@ def main():
             n += 1
         dt = (time.perf_counter() - t0) / n
         line["cpu_baseline"] = {"value": rows_s / dt, "unit": "rows/s", "cores": os.cpu_count(),
-                                "kind": "reference", "sample": desc + f", median of {n} runs"}
+                                "kind": "reference", "sample": desc + f", mean of {n} runs"}
     if rank == 0:
         print(json.dumps(line))
     if dist:

@@ -222,10 +222,14 @@ tdg_status tdg_join_emit(const tdg_join_desc* d, const tdg_join_plan* plan, void
                          int32_t n_rcols, const tdg_col* rsrc, void* const* rdst,
                          void* stream);
 
-/* Fused probe + group-by: every joined row (probe rows passing lpred/lsel)
- * is aggregated directly, with no join output materialized.  Key and
- * aggregate columns of `g` name their side (tdg_col.side).  g->nrows is
- * ignored.  Replaces exec_join followed by exec_group on its result. */
+/* Fused build + probe + group-by: every joined row (probe rows passing
+ * lpred/lsel) is aggregated directly, with no join output materialized.  Key
+ * and aggregate columns of `g` name their side (tdg_col.side); g->nrows is an
+ * upper bound on joined rows.  This call builds the join table itself (do not
+ * call tdg_join_build first): when the build keys are dense and unique and
+ * the group-by is a direct array fed by probe-side values, the table stores
+ * each key's group slot and the probe reads nothing else from the build
+ * side.  Replaces exec_join followed by exec_group on its result. */
 tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_plan* jplan, void* jws,
                               const tdg_expr* lpred, const uint64_t* lsel,
                               const tdg_group_desc* g, const tdg_group_plan* gplan, void* gws,

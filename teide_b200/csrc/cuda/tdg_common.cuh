@@ -203,6 +203,8 @@ struct Pred {
     int32_t n;
     Term t[kMaxTerms];
     const uint64_t* sel;   // optional TD_SEL bit array
+    int32_t w8;            // every term column is 8 bytes wide (kind 0 or 1)
+    int32_t pad;
 };
 
 template <typename T>
@@ -217,8 +219,20 @@ __device__ __forceinline__ bool cmp(int32_t op, T x, T y) {
     }
 }
 
+// 8-byte columns (I64, F64, TIMESTAMP, SYM W64) read without a type switch:
+// the raw word is an integer unless the column is F64.
+__device__ __forceinline__ int64_t ld_i8(const tdg_col& c, int64_t r) {
+    const long long x = ld_stream((const long long*)c.data + r);
+    return c.type == T_F64 ? (int64_t)__longlong_as_double(x) : (int64_t)x;
+}
+__device__ __forceinline__ double ld_f8(const tdg_col& c, int64_t r) {
+    const long long x = ld_stream((const long long*)c.data + r);
+    return c.type == T_F64 ? __longlong_as_double(x) : (double)x;
+}
+
 // PK: 0 = none, 1 = conjunction, 2 = interpreter.  `prog` is only read for PK 2.
-template <int PK>
+// W8: every column the predicate reads is 8 bytes wide.
+template <int PK, bool W8 = false>
 __device__ __forceinline__ bool row_pass(const Pred& p, const tdg_expr& prog, int64_t r) {
     bool ok = true;
     if (p.sel) ok = (__ldg(p.sel + (r >> 6)) >> (r & 63)) & 1;
@@ -227,8 +241,11 @@ __device__ __forceinline__ bool row_pass(const Pred& p, const tdg_expr& prog, in
         for (int i = 0; i < kMaxTerms; i++) {
             if (i < p.n) {
                 const Term& t = p.t[i];
-                bool b = t.f ? cmp(t.op, ld_f(t.col, r), __longlong_as_double(t.k))
-                             : cmp(t.op, ld_i(t.col, r), t.k);
+                bool b;
+                if (W8) b = t.f ? cmp(t.op, ld_f8(t.col, r), __longlong_as_double(t.k))
+                                : cmp(t.op, ld_i8(t.col, r), t.k);
+                else    b = t.f ? cmp(t.op, ld_f(t.col, r), __longlong_as_double(t.k))
+                                : cmp(t.op, ld_i(t.col, r), t.k);
                 ok = ok && b;
             }
         }

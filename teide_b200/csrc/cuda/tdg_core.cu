@@ -102,8 +102,15 @@ Pred make_pred(const tdg_expr* prog, const uint64_t* sel, int* pk) {
     Pred p;
     memset(&p, 0, sizeof(p));
     p.sel = sel;
+    p.w8 = 1;
     if (!prog || prog->n_ins <= 0) { *pk = 0; return p; }
-    if (collect_terms(prog, prog->out, &p)) { p.kind = 1; *pk = 1; return p; }
+    if (collect_terms(prog, prog->out, &p)) {
+        for (int i = 0; i < p.n; i++) p.w8 = p.w8 && elem_size(p.t[i].col.type, p.t[i].col.attrs) == 8;
+        p.kind = 1;
+        *pk = 1;
+        return p;
+    }
+    p.w8 = 0;
     memset(p.t, 0, sizeof(p.t));
     p.n = 0;
     p.kind = 2;

@@ -5,46 +5,75 @@
 // (exec.c:5948-6404) and otherwise a 256-way radix-partitioned hash table
 // built in three phases (exec.c:6406-6667).  Here:
 //
-//   direct array (TDG_GROUP_DIRECT) -- slot = sum_k (key_k - min_k) * stride_k.
-//     When the accumulators fit in 48 KB they are privatized per CTA in
-//     shared memory and merged into global memory once per CTA; larger
-//     arrays (up to 2^26 slots) are updated in place with global atomics,
-//     whose hot lines stay in L2.
-//   hash table (TDG_GROUP_HASH) -- open addressing in HBM (tdg_hash.cuh),
-//     one pass, no partitioning.
+//   direct array (TDG_GROUP_DIRECT) -- slot = sum_k (key_k - min_k) * stride_k,
+//     up to 2^26 slots.
+//   hash table (TDG_GROUP_HASH) -- open addressing in HBM (tdg_hash.cuh), one
+//     pass, no partitioning: the hot part of the table stays in the 126 MB L2.
 //
-// Both keep the same accumulator layout -- count[S] plus one 8-byte array
-// per non-COUNT aggregate -- and share one emit pass that writes the groups
-// whose count is non-zero in slot order (ascending key order for the direct
-// array, like Teide's DA emit at exec.c:6330-6391).
+// Accumulators live in three places:
+//   MODE 0  every slot privatized per CTA in shared memory (32-bit counts,
+//           8-byte accumulators), merged into the global records once per CTA;
+//   MODE 1  direct array in global memory;
+//   MODE 2  hash table in global memory.
+// Global accumulators are slot-major records [count, acc_0, acc_1, ...] so
+// one row's updates touch at most two 32-byte sectors.  In MODES 1 and 2 a
+// sampling pass finds the slots that take a large share of the rows (Zipf
+// heads) and every CTA caches those "hot" slots in shared memory; only cold
+// slots are updated with global atomics, so a key that holds 11% of the rows
+// no longer serializes on one L2 address.
 //
-// Arithmetic matches the CPU loops: integer SUM wraps, AVG = sum / count in
-// double (exec.c:4430-4432, emit_agg_columns 4632-4773), MIN/MAX of F64 skip
-// NaN.  F64 SUM is accumulated with atomics, so its summation order differs
-// from the CPU's per-worker order; results agree to ~1e-15 relative.
+// Every aggregate reads its input once per row; the emit pass writes the
+// groups whose count is non-zero in slot order (ascending key order for the
+// direct array, like Teide's DA emit at exec.c:6330-6391).  Arithmetic
+// follows the CPU loops: integer SUM wraps, AVG = sum / count in double
+// (exec.c:4430-4432, emit_agg_columns 4632-4773), MIN/MAX of F64 skip NaN.
+// F64 SUM uses atomics, so its summation order differs from the CPU's
+// per-worker order (results agree to ~1e-15 relative).
 #include "tdg_hash.cuh"
 #include <string.h>
 
 namespace tdg {
 
-constexpr int kItems = 4;
+// Minimum resident CTAs per SM the streaming kernels are compiled for
+// (bounds their registers): 6 keeps every hot variant spill-free.
+#ifndef TDG_MINB
+#define TDG_MINB 6
+#endif
+#ifndef TDG_ITEMS
+#define TDG_ITEMS 4
+#endif
+constexpr int kItems = TDG_ITEMS;
 constexpr int kEmitChunk = kThreads * 32;
-constexpr size_t kSmemAccMax = 48 * 1024;
+constexpr size_t kSmemMax = 48 * 1024;
 constexpr int64_t kDirectMaxSlots = (int64_t)1 << 26;
+constexpr int kHotMap = 2048;                 // shared hot-slot map entries (power of 2)
+constexpr int kHotMapBits = 11;
+constexpr int kHotMax = 1024;                 // at most this many hot slots
+constexpr int64_t kSampleRows = (int64_t)1 << 18;
+constexpr int64_t kSampleCap = (int64_t)1 << 19;
+constexpr uint32_t kHotMin = 8;               // sampled hits that make a slot hot
+constexpr int64_t kSampleMinRows = (int64_t)1 << 22;
+
+enum : int32_t { K_COUNT = 0, K_SUM_I, K_SUM_F, K_MIN_I, K_MAX_I, K_MIN_F, K_MAX_F };
 
 struct GroupK {
     int32_t nk, na, method, n_acc;
+    int32_t W;                    // 8-byte words per global slot record
+    int32_t hot_cap;              // hot slots a CTA caches (0: no cache)
     tdg_col key[TDG_MAX_KEYS];
     int64_t kmin[TDG_MAX_KEYS], krange[TDG_MAX_KEYS], stride[TDG_MAX_KEYS];
     int32_t op[TDG_MAX_AGGS];
-    int32_t f[TDG_MAX_AGGS];      // aggregate input is F64
+    int32_t kind[TDG_MAX_AGGS];   // K_*
     int32_t ai[TDG_MAX_AGGS];     // accumulator index, -1 for COUNT
     tdg_col in[TDG_MAX_AGGS];
     int64_t S;
-    unsigned long long* cnt;
-    unsigned long long* acc;      // n_acc * S
+    unsigned long long* rec;      // S * W words
     HtRef ht;
-    int32_t* err;
+    int32_t* err;                 // [0] error code, [1] duplicate build key (payload join)
+    int64_t* sample_keys;
+    uint32_t* sample_cnt;
+    int64_t* hot;                 // hot slot list
+    int32_t* hot_n;
 };
 
 struct OutK {
@@ -53,48 +82,56 @@ struct OutK {
     void* aggs[TDG_MAX_AGGS];
 };
 
+__device__ __forceinline__ unsigned long long* grec(const GroupK& G, int64_t s) { return G.rec + s * G.W; }
+
+__host__ __device__ __forceinline__ unsigned long long acc_init_kind(int kind) {
+    return (kind == K_MIN_I || kind == K_MIN_F) ? (unsigned long long)INT64_MAX
+         : (kind == K_MAX_I || kind == K_MAX_F) ? (unsigned long long)INT64_MIN : 0ULL;
+}
+
 // ---- typed multi-row loads --------------------------------------------------
-// Loads N rows of one column (row < 0 or masked off gives 0).  The type switch
-// runs once per column, so the N loads issue back to back.  Probe-side
-// columns stream (evict-first); build-side columns are gathered at random and
-// use the read-only path so they stay cached.
-template <int N>
+// N rows of one column (row < 0 or masked off gives 0).  The type switch runs
+// once per column, so the N loads issue back to back; with W8 every column is
+// 8 bytes and there is no switch at all.  Probe-side columns stream
+// (evict-first); build-side columns are gathered at random and use the
+// read-only path so they stay cached.
+template <bool W8, int N>
 __device__ __forceinline__ void ld_items_i(const tdg_col& c, const int64_t (&r)[N], const bool (&m)[N],
                                            int64_t (&v)[N]) {
-#define TDG_LD(T)                                                                        \
-    {                                                                                    \
-        const T* p = (const T*)c.data;                                                   \
-        _Pragma("unroll") for (int i = 0; i < N; i++)                                    \
-            v[i] = (m[i] && r[i] >= 0) ? (int64_t)(c.side ? __ldg(p + r[i]) : ld_stream(p + r[i])) : 0; \
+#define TDG_LD(T, CONV)                                                                                   \
+    {                                                                                                     \
+        const T* p = (const T*)c.data;                                                                    \
+        _Pragma("unroll") for (int i = 0; i < N; i++)                                                    \
+            v[i] = (m[i] && r[i] >= 0) ? (int64_t)CONV(c.side ? __ldg(p + r[i]) : ld_stream(p + r[i])) : 0; \
+    }
+#define TDG_ID(x) (x)
+    if (W8) {
+        if (c.type == T_F64) TDG_LD(double, TDG_ID) else TDG_LD(long long, TDG_ID)
+        return;
     }
     switch (c.type) {
-        case T_I64: case T_TIMESTAMP: TDG_LD(long long) break;
-        case T_I32: case T_DATE: case T_TIME: TDG_LD(int) break;
-        case T_I16: TDG_LD(short) break;
-        case T_BOOL: case T_U8: case T_CHAR: TDG_LD(unsigned char) break;
+        case T_I64: case T_TIMESTAMP: TDG_LD(long long, TDG_ID) break;
+        case T_I32: case T_DATE: case T_TIME: TDG_LD(int, TDG_ID) break;
+        case T_I16: TDG_LD(short, TDG_ID) break;
+        case T_BOOL: case T_U8: case T_CHAR: TDG_LD(unsigned char, TDG_ID) break;
         case T_SYM:
             switch (c.attrs & 3) {
-                case 0: TDG_LD(unsigned char) break;
-                case 1: TDG_LD(unsigned short) break;
-                case 2: TDG_LD(unsigned int) break;
-                default: TDG_LD(long long) break;
+                case 0: TDG_LD(unsigned char, TDG_ID) break;
+                case 1: TDG_LD(unsigned short, TDG_ID) break;
+                case 2: TDG_LD(unsigned int, TDG_ID) break;
+                default: TDG_LD(long long, TDG_ID) break;
             }
             break;
-        case T_F64: {
-            const double* p = (const double*)c.data;
-#pragma unroll
-            for (int i = 0; i < N; i++)
-                v[i] = (m[i] && r[i] >= 0) ? (int64_t)(c.side ? __ldg(p + r[i]) : ld_stream(p + r[i])) : 0;
-            break;
-        }
+        case T_F64: TDG_LD(double, TDG_ID) break;
         default:
 #pragma unroll
             for (int i = 0; i < N; i++) v[i] = 0;
     }
+#undef TDG_ID
 #undef TDG_LD
 }
 
-template <int N>
+template <bool W8, int N>
 __device__ __forceinline__ void ld_items_f(const tdg_col& c, const int64_t (&r)[N], const bool (&m)[N],
                                            double (&v)[N]) {
     if (c.type == T_F64) {
@@ -104,44 +141,43 @@ __device__ __forceinline__ void ld_items_f(const tdg_col& c, const int64_t (&r)[
             v[i] = (m[i] && r[i] >= 0) ? (c.side ? __ldg(p + r[i]) : ld_stream(p + r[i])) : 0.0;
     } else {
         int64_t t[N];
-        ld_items_i<N>(c, r, m, t);
+        ld_items_i<W8, N>(c, r, m, t);
 #pragma unroll
         for (int i = 0; i < N; i++) v[i] = (double)t[i];
     }
 }
 
-__device__ __forceinline__ unsigned long long acc_init(int op) {
-    return op == A_MIN ? (unsigned long long)INT64_MAX : op == A_MAX ? (unsigned long long)INT64_MIN : 0ULL;
-}
-
-template <bool GLOBAL>
-__device__ __forceinline__ void upd_i(unsigned long long* a, int op, int64_t v) {
-    if (op == A_MIN) {
-        if (!GLOBAL || v < *(volatile long long*)a) atomicMin((long long*)a, (long long)v);
-    } else if (op == A_MAX) {
-        if (!GLOBAL || v > *(volatile long long*)a) atomicMax((long long*)a, (long long)v);
-    } else {
-        atomicAdd(a, (unsigned long long)v);
+// One accumulator update (shared or global memory).  The returned old value
+// is never used, so global updates compile to fire-and-forget reductions.
+__device__ __forceinline__ void upd(unsigned long long* a, int kind, int64_t iv, double fv) {
+    switch (kind) {
+        case K_SUM_I: atomicAdd(a, (unsigned long long)iv); break;
+        case K_SUM_F: atomicAdd((double*)a, fv); break;
+        case K_MIN_I: atomicMin((long long*)a, (long long)iv); break;
+        case K_MAX_I: atomicMax((long long*)a, (long long)iv); break;
+        case K_MIN_F: if (fv == fv) atomicMin((long long*)a, f2ord(fv)); break;
+        case K_MAX_F: if (fv == fv) atomicMax((long long*)a, f2ord(fv)); break;
+        default: break;
     }
 }
 
-template <bool GLOBAL>
-__device__ __forceinline__ void upd_f(unsigned long long* a, int op, double v) {
-    if (op == A_MIN || op == A_MAX) {
-        if (v != v) return;                       // NaN never becomes a MIN/MAX
-        const long long o = f2ord(v);
-        if (op == A_MIN) {
-            if (!GLOBAL || o < *(volatile long long*)a) atomicMin((long long*)a, o);
-        } else {
-            if (!GLOBAL || o > *(volatile long long*)a) atomicMax((long long*)a, o);
-        }
-    } else {
-        atomicAdd((double*)a, v);
+// Merge one accumulator value (already in accumulator form) into another.
+__device__ __forceinline__ void merge(unsigned long long* a, int kind, unsigned long long v) {
+    switch (kind) {
+        case K_SUM_I: atomicAdd(a, v); break;
+        case K_SUM_F: atomicAdd((double*)a, __longlong_as_double((long long)v)); break;
+        case K_MIN_I: case K_MIN_F:
+            if ((long long)v != INT64_MAX) atomicMin((long long*)a, (long long)v);
+            break;
+        case K_MAX_I: case K_MAX_F:
+            if ((long long)v != INT64_MIN) atomicMax((long long*)a, (long long)v);
+            break;
+        default: break;
     }
 }
 
 // Slot of each (probe row, build row) pair; -1 when masked off or on error.
-template <int MODE, int N>
+template <int MODE, bool W8, int N>
 __device__ __forceinline__ void slots_of(const GroupK& G, const int64_t (&rp)[N], const int64_t (&rb)[N],
                                          const bool (&m)[N], int64_t (&slot)[N]) {
     if (MODE != 2) {
@@ -150,7 +186,7 @@ __device__ __forceinline__ void slots_of(const GroupK& G, const int64_t (&rp)[N]
         for (int i = 0; i < N; i++) { slot[i] = 0; ok[i] = m[i]; }
         for (int k = 0; k < G.nk; k++) {
             int64_t v[N];
-            ld_items_i<N>(G.key[k], G.key[k].side ? rb : rp, m, v);
+            ld_items_i<W8, N>(G.key[k], G.key[k].side ? rb : rp, m, v);
 #pragma unroll
             for (int i = 0; i < N; i++) {
                 const int64_t d = v[i] - G.kmin[k];
@@ -176,58 +212,155 @@ __device__ __forceinline__ void slots_of(const GroupK& G, const int64_t (&rp)[N]
     }
 }
 
-template <int MODE, int N>
-__device__ __forceinline__ void accumulate(const GroupK& G, unsigned long long* cnt, unsigned long long* acc,
-                                           int64_t S, const int64_t (&rp)[N], const int64_t (&rb)[N],
-                                           const bool (&m)[N]) {
-    constexpr bool GL = MODE != 0;
-    int64_t slot[N];
-    slots_of<MODE, N>(G, rp, rb, m, slot);
+// ---- shared-memory accumulators -----------------------------------------------------
+// MODE 0: cnt[S] (32-bit) then acc[n_acc][S].
+// MODES 1/2: a map from hot slot to cache index, then cnt[hot_cap] and
+// acc[n_acc][hot_cap].
+struct SmemView {
+    uint32_t* cnt;
+    unsigned long long* acc;
+    int64_t cap;        // entries per array
+    int32_t* map_key;   // hot slot, -1 empty
+    int16_t* map_idx;
+    int n_hot;
+};
+
+__host__ __device__ inline size_t smem_full_bytes(int64_t S, int n_acc) {
+    return (((size_t)S * 4 + 7) & ~(size_t)7) + (size_t)S * 8 * n_acc;
+}
+__host__ __device__ inline size_t smem_hot_bytes(int hot_cap, int n_acc) {
+    return (size_t)kHotMap * 4 + (size_t)kHotMap * 2 + (((size_t)hot_cap * 4 + 7) & ~(size_t)7) +
+           (size_t)hot_cap * 8 * n_acc;
+}
+
+__device__ __forceinline__ int hot_find(const SmemView& V, int64_t slot) {
+    uint32_t h = ((uint32_t)slot * 2654435761u) >> (32 - kHotMapBits);
+    for (int p = 0; p < kHotMap; p++) {
+        const int32_t k = V.map_key[h];
+        if (k == (int32_t)slot) return V.map_idx[h];
+        if (k == -1) return -1;
+        h = (h + 1) & (kHotMap - 1);
+    }
+    return -1;
+}
+
+template <int MODE>
+__device__ SmemView smem_setup(const GroupK& G, unsigned long long* sm) {
+    SmemView V;
+    V.cnt = nullptr;
+    V.acc = nullptr;
+    V.cap = 0;
+    V.map_key = nullptr;
+    V.map_idx = nullptr;
+    V.n_hot = 0;
+    if (MODE == 0) {
+        V.cap = G.S;
+        V.cnt = (uint32_t*)sm;
+        V.acc = sm + ((G.S * 4 + 7) >> 3);
+    } else {
+        V.cap = G.hot_cap;
+        if (!G.hot_cap) return V;
+        V.map_key = (int32_t*)sm;
+        V.map_idx = (int16_t*)(V.map_key + kHotMap);
+        V.cnt = (uint32_t*)(V.map_idx + kHotMap);
+        V.acc = (unsigned long long*)((char*)V.cnt + (((size_t)G.hot_cap * 4 + 7) & ~(size_t)7));
+        const int nh = *G.hot_n;
+        V.n_hot = nh < G.hot_cap ? nh : G.hot_cap;
+        for (int i = threadIdx.x; i < kHotMap; i += blockDim.x) V.map_key[i] = -1;
+        __syncthreads();
+        for (int h = threadIdx.x; h < V.n_hot; h += blockDim.x) {
+            const int32_t slot = (int32_t)G.hot[h];
+            uint32_t p = ((uint32_t)slot * 2654435761u) >> (32 - kHotMapBits);
+            for (int t = 0; t < kHotMap; t++) {
+                if (atomicCAS(&V.map_key[p], -1, slot) == -1) { V.map_idx[p] = (int16_t)h; break; }
+                p = (p + 1) & (kHotMap - 1);
+            }
+        }
+    }
+    const int64_t n = MODE == 0 ? G.S : V.n_hot;
+    for (int64_t s = threadIdx.x; s < n; s += blockDim.x) V.cnt[s] = 0;
+    for (int a = 0; a < G.na; a++) {
+        if (G.ai[a] < 0) continue;
+        const unsigned long long init = acc_init_kind(G.kind[a]);
+        for (int64_t s = threadIdx.x; s < n; s += blockDim.x) V.acc[(int64_t)G.ai[a] * V.cap + s] = init;
+    }
+    __syncthreads();
+    return V;
+}
+
+template <int MODE>
+__device__ void smem_flush(const GroupK& G, const SmemView& V) {
+    __syncthreads();
+    const int64_t n = MODE == 0 ? G.S : V.n_hot;
+    for (int64_t s = threadIdx.x; s < n; s += blockDim.x) {
+        const uint32_t c = V.cnt[s];
+        if (!c) continue;
+        const int64_t slot = MODE == 0 ? s : G.hot[s];
+        unsigned long long* r = grec(G, slot);
+        atomicAdd(r, (unsigned long long)c);
+        for (int a = 0; a < G.na; a++)
+            if (G.ai[a] >= 0) merge(r + 1 + G.ai[a], G.kind[a], V.acc[(int64_t)G.ai[a] * V.cap + s]);
+    }
+}
+
+// Aggregate N rows whose slots are known (slot < 0 or !m[i]: skipped).
+template <int MODE, bool W8, int N>
+__device__ __forceinline__ void accumulate_at(const GroupK& G, const SmemView& V, const int64_t (&rp)[N],
+                                              const int64_t (&rb)[N], const int64_t (&slot)[N], const bool (&m)[N]) {
     bool ok[N];
+    int hidx[N];
 #pragma unroll
     for (int i = 0; i < N; i++) {
         ok[i] = m[i] && slot[i] >= 0;
-        if (ok[i]) atomicAdd(&cnt[slot[i]], 1ULL);
+        hidx[i] = -1;
+        if (MODE == 0) hidx[i] = ok[i] ? (int)slot[i] : -1;
+        else if (V.n_hot && ok[i]) hidx[i] = hot_find(V, slot[i]);
+        if (ok[i]) {
+            if (hidx[i] >= 0) atomicAdd(&V.cnt[hidx[i]], 1u);
+            else atomicAdd(grec(G, slot[i]), 1ULL);
+        }
     }
     for (int a = 0; a < G.na; a++) {
-        const int op = G.op[a];
-        if (op == A_COUNT) continue;
-        unsigned long long* base = acc + (int64_t)G.ai[a] * S;
+        const int kind = G.kind[a];
+        if (kind == K_COUNT) continue;
+        const int ai = G.ai[a];
         const tdg_col& c = G.in[a];
         const int64_t (&rr)[N] = c.side ? rb : rp;
-        if (G.f[a]) {
-            double v[N];
-            ld_items_f<N>(c, rr, ok, v);
+        int64_t iv[N];
+        double fv[N];
+        if (kind == K_SUM_F || kind == K_MIN_F || kind == K_MAX_F) {
+            ld_items_f<W8, N>(c, rr, ok, fv);
 #pragma unroll
-            for (int i = 0; i < N; i++) if (ok[i]) upd_f<GL>(base + slot[i], op, v[i]);
+            for (int i = 0; i < N; i++) iv[i] = 0;
         } else {
-            int64_t v[N];
-            ld_items_i<N>(c, rr, ok, v);
+            ld_items_i<W8, N>(c, rr, ok, iv);
 #pragma unroll
-            for (int i = 0; i < N; i++) if (ok[i]) upd_i<GL>(base + slot[i], op, v[i]);
+            for (int i = 0; i < N; i++) fv[i] = 0;
+        }
+#pragma unroll
+        for (int i = 0; i < N; i++) {
+            if (!ok[i]) continue;
+            if (hidx[i] >= 0) upd(V.acc + (int64_t)ai * V.cap + hidx[i], kind, iv[i], fv[i]);
+            else upd(grec(G, slot[i]) + 1 + ai, kind, iv[i], fv[i]);
         }
     }
 }
 
-// MODE 0: direct array in shared memory; 1: direct array in global memory;
-// 2: hash table.  JOIN: probe rows are joined through J first and every
+template <int MODE, bool W8, int N>
+__device__ __forceinline__ void accumulate(const GroupK& G, const SmemView& V, const int64_t (&rp)[N],
+                                           const int64_t (&rb)[N], const bool (&m)[N]) {
+    int64_t slot[N];
+    slots_of<MODE, W8, N>(G, rp, rb, m, slot);
+    accumulate_at<MODE, W8, N>(G, V, rp, rb, slot, m);
+}
+
+// The main kernel.  JOIN: probe rows are joined through J first and every
 // (probe, build) match is one input row of the group-by.
-template <int PK, int MODE, bool JOIN>
-__global__ void __launch_bounds__(kThreads) k_group(const GroupK G, const Pred P, const tdg_expr prog,
+template <int PK, int MODE, bool JOIN, bool W8>
+__global__ void __launch_bounds__(kThreads, TDG_MINB) k_group(const GroupK G, const Pred P, const tdg_expr prog,
                                                     const JoinK J, int64_t n) {
     extern __shared__ unsigned long long sm[];
-    const int64_t S = G.S;
-    unsigned long long* cnt = MODE == 0 ? sm : G.cnt;
-    unsigned long long* acc = MODE == 0 ? sm + S : G.acc;
-    if (MODE == 0) {
-        for (int64_t s = threadIdx.x; s < S; s += blockDim.x) cnt[s] = 0;
-        for (int a = 0; a < G.na; a++) {
-            if (G.ai[a] < 0) continue;
-            const unsigned long long init = acc_init(G.op[a]);
-            for (int64_t s = threadIdx.x; s < S; s += blockDim.x) acc[(int64_t)G.ai[a] * S + s] = init;
-        }
-        __syncthreads();
-    }
+    const SmemView V = smem_setup<MODE>(G, sm);
     const int64_t tile = (int64_t)kThreads * kItems;
     for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
         int64_t rp[kItems], rb[kItems];
@@ -236,7 +369,7 @@ __global__ void __launch_bounds__(kThreads) k_group(const GroupK G, const Pred P
         for (int i = 0; i < kItems; i++) {
             rp[i] = base + i * kThreads + threadIdx.x;
             rb[i] = -1;
-            m[i] = rp[i] < n && row_pass<PK>(P, prog, rp[i]);
+            m[i] = rp[i] < n && row_pass<PK, W8>(P, prog, rp[i]);
         }
         if (JOIN) {
 #pragma unroll
@@ -246,7 +379,7 @@ __global__ void __launch_bounds__(kThreads) k_group(const GroupK G, const Pred P
                 if (J.matched && rb[i] >= 0) J.matched[rb[i]] = 1;
             }
         }
-        accumulate<MODE, kItems>(G, cnt, acc, S, rp, rb, m);
+        accumulate<MODE, W8, kItems>(G, V, rp, rb, m);
         if (JOIN) {
             // further matches of duplicate build keys
             for (int i = 0; i < kItems; i++) {
@@ -256,62 +389,158 @@ __global__ void __launch_bounds__(kThreads) k_group(const GroupK G, const Pred P
                     int64_t p1[1] = {rp[i]}, b1[1] = {nb};
                     bool m1[1] = {true};
                     if (J.matched) J.matched[nb] = 1;
-                    accumulate<MODE, 1>(G, cnt, acc, S, p1, b1, m1);
+                    accumulate<MODE, W8, 1>(G, V, p1, b1, m1);
                     nb = __ldg(&J.next[nb]);
                 }
             }
         }
     }
-    if (MODE == 0) {
-        __syncthreads();
-        for (int64_t s = threadIdx.x; s < S; s += blockDim.x) {
-            const unsigned long long c = cnt[s];
-            if (!c) continue;
-            atomicAdd(&G.cnt[s], c);
-            for (int a = 0; a < G.na; a++) {
-                const int op = G.op[a];
-                if (op == A_COUNT) continue;
-                const int64_t o = (int64_t)G.ai[a] * S + s;
-                const unsigned long long v = acc[o];
-                if (op == A_MIN) atomicMin((long long*)&G.acc[o], (long long)v);
-                else if (op == A_MAX) atomicMax((long long*)&G.acc[o], (long long)v);
-                else if (G.f[a]) atomicAdd((double*)&G.acc[o], __longlong_as_double((long long)v));
-                else atomicAdd(&G.acc[o], v);
-            }
+    if (MODE == 0 || V.n_hot) smem_flush<MODE>(G, V);
+}
+
+// ---- hot-slot sampling (MODES 1 and 2) ---------------------------------------------
+// Rows at a fixed stride go through the same selection, join and slot
+// computation as the main kernel; their slots are counted in a small hash
+// table, and slots seen at least kHotMin times become the hot list.
+template <int PK, int MODE, bool JOIN>
+__global__ void __launch_bounds__(kThreads) k_sample(const GroupK G, const Pred P, const tdg_expr prog,
+                                                     const JoinK J, int64_t n, int64_t step, int64_t m_rows) {
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m_rows; j += (int64_t)gridDim.x * blockDim.x) {
+        int64_t rp[1] = {j * step}, rb[1] = {-1}, slot[1];
+        bool m[1] = {rp[0] < n && row_pass<PK>(P, prog, rp[0])};
+        if (JOIN && m[0]) {
+            rb[0] = join_first(J, rp[0]);
+            if (J.join_type == 0) m[0] = rb[0] >= 0;
+        }
+        slots_of<MODE, false, 1>(G, rp, rb, m, slot);
+        if (!m[0] || slot[0] < 0) continue;
+        uint64_t h = mix64((uint64_t)slot[0]) & (uint64_t)(kSampleCap - 1);
+        for (int64_t t = 0; t < kSampleCap; t++) {
+            const unsigned long long prev = atomicCAS((unsigned long long*)&G.sample_keys[h], ~0ULL,
+                                                      (unsigned long long)slot[0]);
+            if (prev == ~0ULL || prev == (unsigned long long)slot[0]) { atomicAdd(&G.sample_cnt[h], 1u); break; }
+            h = (h + 1) & (uint64_t)(kSampleCap - 1);
         }
     }
 }
 
+__global__ void __launch_bounds__(kThreads) k_select_hot(const GroupK G) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < kSampleCap; e += (int64_t)gridDim.x * blockDim.x) {
+        if (G.sample_keys[e] == -1 || G.sample_cnt[e] < kHotMin) continue;
+        const int i = atomicAdd(G.hot_n, 1);
+        if (i < kHotMax) G.hot[i] = G.sample_keys[e];
+    }
+}
+
+// ---- payload join -> group ---------------------------------------------------------
+// When the build side has unique, dense integer join keys and the group-by
+// is a direct array whose aggregate inputs all come from the probe side, the
+// build pass stores in map[key - kmin] the build row's share of the group
+// slot (sum over build-side group keys of (key - min) * stride), or EMPTY.
+// The probe then needs one small random read per row -- a 2-byte entry when
+// the slots fit in 16 bits, so a 10M-row build side is a 20 MB map that stays
+// in L2 -- instead of the head[] lookup plus the build-column gather.
+template <typename PT> struct Empty;
+template <> struct Empty<uint16_t> { static constexpr uint16_t v = 0xFFFF; };
+template <> struct Empty<uint32_t> { static constexpr uint32_t v = 0xFFFFFFFFu; };
+
+template <typename PT>
+__global__ void __launch_bounds__(kThreads) k_payload_build(const GroupK G, const JoinK J, PT* map,
+                                                            int64_t n_right, int32_t* dup) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_right;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = ld_i(J.rkeys[0], r) - J.kmin;
+        if (k < 0 || k >= J.n_slots) { set_err(G.err, E_DOMAIN); continue; }
+        int64_t s = 0;
+        bool ok = true;
+        for (int kk = 0; kk < G.nk; kk++) {
+            if (!G.key[kk].side) continue;
+            const int64_t d = ld_i(G.key[kk], r) - G.kmin[kk];
+            ok = ok && d >= 0 && d < G.krange[kk];
+            s += d * G.stride[kk];
+        }
+        if (!ok) { set_err(G.err, E_DOMAIN); continue; }
+        const PT old = atomicCAS(map + k, Empty<PT>::v, (PT)s);
+        if (old != Empty<PT>::v) atomicExch(dup, 1);
+    }
+}
+
+template <int PK, bool SMEM, typename PT, bool W8>
+__global__ void __launch_bounds__(kThreads, TDG_MINB) k_payload_probe(const GroupK G, const Pred P, const tdg_expr prog,
+                                                            const tdg_col lkey, int64_t kmin, int64_t n_map,
+                                                            const PT* __restrict__ map, int64_t n) {
+    extern __shared__ unsigned long long sm[];
+    constexpr int MODE = SMEM ? 0 : 1;
+    const SmemView V = smem_setup<MODE>(G, sm);
+    const int64_t tile = (int64_t)kThreads * kItems;
+    for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
+        int64_t rp[kItems], rb[kItems], kv[kItems], slot[kItems];
+        bool m[kItems];
+#pragma unroll
+        for (int i = 0; i < kItems; i++) {
+            rp[i] = base + i * kThreads + threadIdx.x;
+            rb[i] = -1;
+            m[i] = rp[i] < n && row_pass<PK, W8>(P, prog, rp[i]);
+        }
+        ld_items_i<W8, kItems>(lkey, rp, m, kv);
+#pragma unroll
+        for (int i = 0; i < kItems; i++) {
+            const int64_t k = kv[i] - kmin;
+            const bool in = m[i] && k >= 0 && k < n_map;
+            const PT pl = in ? __ldg(map + k) : Empty<PT>::v;
+            m[i] = pl != Empty<PT>::v;
+            slot[i] = m[i] ? (int64_t)pl : -1;
+        }
+        for (int kk = 0; kk < G.nk; kk++) {       // probe-side share of the slot
+            if (G.key[kk].side) continue;
+            int64_t v[kItems];
+            ld_items_i<W8, kItems>(G.key[kk], rp, m, v);
+#pragma unroll
+            for (int i = 0; i < kItems; i++) {
+                const int64_t d = v[i] - G.kmin[kk];
+                if (m[i] && (d < 0 || d >= G.krange[kk])) { set_err(G.err, E_DOMAIN); m[i] = false; }
+                slot[i] += d * G.stride[kk];
+            }
+        }
+        accumulate_at<MODE, W8, kItems>(G, V, rp, rb, slot, m);
+    }
+    if (MODE == 0 || V.n_hot) smem_flush<MODE>(G, V);
+}
+
 // Full outer join: build rows that no probe row matched enter the group-by
-// with zero-filled probe-side values.
+// with zero-filled probe-side values (global accumulators, no cache).
 template <int MODE>
-__global__ void __launch_bounds__(kThreads) k_group_unmatched(const GroupK G, const JoinK J, int64_t n_right) {
+__global__ void __launch_bounds__(kThreads) k_group_unmatched(GroupK G, const JoinK J, int64_t n_right) {
+    G.hot_cap = 0;
+    SmemView V;
+    memset(&V, 0, sizeof(V));
     for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < n_right;
          b += (int64_t)gridDim.x * blockDim.x) {
         if (J.matched[b]) continue;
         int64_t p1[1] = {-1}, b1[1] = {b};
         bool m1[1] = {true};
-        accumulate<MODE == 0 ? 1 : MODE, 1>(G, G.cnt, G.acc, G.S, p1, b1, m1);
+        accumulate<MODE, false, 1>(G, V, p1, b1, m1);
     }
 }
 
 __global__ void k_group_init(const GroupK G) {
     for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < G.S; s += (int64_t)gridDim.x * blockDim.x) {
-        G.cnt[s] = 0;
+        unsigned long long* r = grec(G, s);
+        r[0] = 0;
         for (int a = 0; a < G.na; a++)
-            if (G.ai[a] >= 0) G.acc[(int64_t)G.ai[a] * G.S + s] = acc_init(G.op[a]);
+            if (G.ai[a] >= 0) r[1 + G.ai[a]] = acc_init_kind(G.kind[a]);
         if (G.method == TDG_GROUP_HASH) G.ht.state[s] = 0;
     }
 }
 
 // ---- emit ------------------------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) k_emit_count(const unsigned long long* cnt, int64_t S, int64_t* counts) {
+__global__ void __launch_bounds__(kThreads) k_emit_count(const GroupK G, int64_t* counts) {
     __shared__ int red[32];
     const int64_t base = (int64_t)blockIdx.x * kEmitChunk;
     int c = 0;
     for (int i = 0; i < kEmitChunk / kThreads; i++) {
         const int64_t s = base + i * kThreads + threadIdx.x;
-        c += (s < S && cnt[s] != 0) ? 1 : 0;
+        c += (s < G.S && grec(G, s)[0] != 0) ? 1 : 0;
     }
     int tot;
     block_excl_scan(c, &tot, red);
@@ -334,7 +563,8 @@ __global__ void __launch_bounds__(kThreads) k_emit(const GroupK G, const OutK O,
     const int64_t S = G.S;
     for (int i = 0; i < kEmitChunk / kThreads; i++) {
         const int64_t s = base + i * kThreads + threadIdx.x;
-        const unsigned long long c = s < S ? G.cnt[s] : 0;
+        const unsigned long long* r = s < S ? grec(G, s) : nullptr;
+        const unsigned long long c = r ? r[0] : 0;
         int tot;
         const int pre = block_excl_scan(c ? 1 : 0, &tot, red);
         if (c) {
@@ -346,22 +576,22 @@ __global__ void __launch_bounds__(kThreads) k_emit(const GroupK G, const OutK O,
                 put_key(O.keys[k], O.kesz[k], o, v);
             }
             for (int a = 0; a < G.na; a++) {
-                const int op = G.op[a];
-                uint64_t r;
-                if (op == A_COUNT) {
-                    r = c;
+                const int kind = G.kind[a];
+                uint64_t res;
+                if (kind == K_COUNT) {
+                    res = c;
                 } else {
-                    const unsigned long long v = G.acc[(int64_t)G.ai[a] * S + s];
-                    if (op == A_AVG) {
-                        const double sum = G.f[a] ? __longlong_as_double((long long)v) : (double)(long long)v;
-                        r = (uint64_t)__double_as_longlong(sum / (double)c);
-                    } else if ((op == A_MIN || op == A_MAX) && G.f[a]) {
-                        r = (uint64_t)__double_as_longlong(ord2f((long long)v));
+                    const unsigned long long v = r[1 + G.ai[a]];
+                    if (G.op[a] == A_AVG) {
+                        const double sum = kind == K_SUM_F ? __longlong_as_double((long long)v) : (double)(long long)v;
+                        res = (uint64_t)__double_as_longlong(sum / (double)c);
+                    } else if (kind == K_MIN_F || kind == K_MAX_F) {
+                        res = (uint64_t)__double_as_longlong(ord2f((long long)v));
                     } else {
-                        r = v;
+                        res = v;
                     }
                 }
-                ((uint64_t*)O.aggs[a])[o] = r;
+                ((uint64_t*)O.aggs[a])[o] = res;
             }
         }
         out += tot;
@@ -369,24 +599,46 @@ __global__ void __launch_bounds__(kThreads) k_emit(const GroupK G, const OutK O,
     }
 }
 
-__global__ void k_scan_counts_g(int64_t* counts, int64_t m, int64_t* d_total);
+__global__ void __launch_bounds__(1024) k_scan_counts_g(int64_t* counts, int64_t m, int64_t* d_total) {
+    __shared__ long long part[1024];
+    const int64_t per = (m + blockDim.x - 1) / blockDim.x;
+    const int64_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
+    long long sum = 0;
+    for (int64_t i = b; i < e; i++) sum += counts[i];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        long long v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    long long run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    for (int64_t i = b; i < e; i++) { long long c = counts[i]; counts[i] = run; run += c; }
+    if (threadIdx.x == blockDim.x - 1 && d_total) *d_total = part[blockDim.x - 1];
+}
 
-// ---- workspace layout -----------------------------------------------------------------
+// ---- host side: layout, plan, launch ----------------------------------------------------
 struct Layout {
-    size_t err, cnt, acc, state, keys, emit, total;
+    size_t err, rec, state, keys, emit, sample_keys, sample_cnt, hot, hot_n, total;
 };
 
 static size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static Layout layout_of(int64_t S, int n_acc, int nk, int method) {
+static int words_of(int n_acc) { return 1 + n_acc == 3 ? 4 : 1 + n_acc; }
+
+static Layout layout_of(int64_t S, int n_acc, int nk, int method, bool sampled) {
     Layout L;
     size_t o = 0;
     L.err = o; o += 256;
-    L.cnt = o; o += al((size_t)S * 8);
-    L.acc = o; o += al((size_t)S * 8 * n_acc);
+    L.rec = o; o += al((size_t)S * 8 * words_of(n_acc));
     L.state = o; o += method == TDG_GROUP_HASH ? al((size_t)S * 4) : 0;
     L.keys = o; o += method == TDG_GROUP_HASH ? al((size_t)S * 8 * nk) : 0;
     L.emit = o; o += al((size_t)((S + kEmitChunk - 1) / kEmitChunk + 1) * 8);
+    L.sample_keys = o; o += sampled ? al((size_t)kSampleCap * 8) : 0;
+    L.sample_cnt = o; o += sampled ? al((size_t)kSampleCap * 4) : 0;
+    L.hot = o; o += sampled ? al((size_t)kHotMax * 8) : 0;
+    L.hot_n = o; o += sampled ? 256 : 0;
     L.total = o;
     return L;
 }
@@ -416,6 +668,11 @@ static tdg_status validate(const tdg_group_desc* d) {
     return E_OK;
 }
 
+// The hot-slot cache pays off for large inputs aggregated in global memory.
+static bool wants_sampling(int method, bool smem, int64_t S, int64_t nrows) {
+    return !smem && nrows >= kSampleMinRows && S < ((int64_t)1 << 31) && (method == TDG_GROUP_DIRECT || method == TDG_GROUP_HASH);
+}
+
 static tdg_status plan_group(const tdg_group_desc* d, int64_t nrows_bound, int64_t hint, tdg_group_plan* p) {
     tdg_status st = validate(d);
     if (st) return st;
@@ -439,7 +696,7 @@ static tdg_status plan_group(const tdg_group_desc* d, int64_t nrows_bound, int64
     if (direct) {
         p->method = TDG_GROUP_DIRECT;
         p->n_slots = slots;
-        p->smem = (size_t)slots * 8 * (1 + n_acc) <= kSmemAccMax ? 1 : 0;
+        p->smem = smem_full_bytes(slots, n_acc) <= kSmemMax ? 1 : 0;
     } else {
         int64_t bound = nrows_bound > 0 ? nrows_bound : 1;
         if (hint > 0 && hint < bound) bound = hint;
@@ -458,24 +715,36 @@ static tdg_status plan_group(const tdg_group_desc* d, int64_t nrows_bound, int64
         p->n_slots = next_pow2(bound * 2 > 1024 ? bound * 2 : 1024);
     }
     p->max_groups = p->n_slots;
-    p->ws_bytes = layout_of(p->n_slots, n_acc, d->n_keys, p->method).total;
+    const bool sampled = wants_sampling(p->method, p->smem != 0, p->n_slots, nrows_bound);
+    p->ws_bytes = layout_of(p->n_slots, n_acc, d->n_keys, p->method, sampled).total;
     return E_OK;
 }
 
-static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws) {
+static int kind_of(const tdg_agg& a) {
+    const bool f = a.in.type == T_F64;
+    switch (a.op) {
+        case A_COUNT: return K_COUNT;
+        case A_MIN: return f ? K_MIN_F : K_MIN_I;
+        case A_MAX: return f ? K_MAX_F : K_MAX_I;
+        default: return f ? K_SUM_F : K_SUM_I;     // SUM, AVG
+    }
+}
+
+static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws, int64_t nrows_bound) {
     GroupK G;
     memset(&G, 0, sizeof(G));
     const int n_acc = count_acc(d);
-    const Layout L = layout_of(p->n_slots, n_acc, d->n_keys, p->method);
+    const bool sampled = wants_sampling(p->method, p->smem != 0, p->n_slots, nrows_bound);
+    const Layout L = layout_of(p->n_slots, n_acc, d->n_keys, p->method, sampled);
     char* w = (char*)ws;
     G.nk = d->n_keys;
     G.na = d->n_aggs;
     G.method = p->method;
     G.n_acc = n_acc;
+    G.W = words_of(n_acc);
     G.S = p->n_slots;
     G.err = (int32_t*)(w + L.err);
-    G.cnt = (unsigned long long*)(w + L.cnt);
-    G.acc = (unsigned long long*)(w + L.acc);
+    G.rec = (unsigned long long*)(w + L.rec);
     int64_t stride = 1;
     for (int k = d->n_keys - 1; k >= 0; k--) {
         G.key[k] = d->keys[k];
@@ -490,7 +759,7 @@ static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws
     for (int a = 0; a < d->n_aggs; a++) {
         G.op[a] = d->aggs[a].op;
         G.in[a] = d->aggs[a].in;
-        G.f[a] = d->aggs[a].in.type == T_F64;
+        G.kind[a] = kind_of(d->aggs[a]);
         G.ai[a] = G.op[a] == A_COUNT ? -1 : ai++;
     }
     if (p->method == TDG_GROUP_HASH) {
@@ -500,23 +769,35 @@ static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws
         G.ht.nk = d->n_keys;
         G.ht.err = G.err;
     }
+    if (sampled) {
+        G.sample_keys = (int64_t*)(w + L.sample_keys);
+        G.sample_cnt = (uint32_t*)(w + L.sample_cnt);
+        G.hot = (int64_t*)(w + L.hot);
+        G.hot_n = (int32_t*)(w + L.hot_n);
+        int cap = (int)((kSmemMax - (size_t)kHotMap * 6 - 8) / (4 + 8 * (size_t)n_acc));
+        G.hot_cap = cap < kHotMax ? cap : kHotMax;
+    }
     return G;
 }
 
-static tdg_status prepare(const GroupK& G, const tdg_group_plan* p, cudaStream_t s) {
+static tdg_status prepare(const GroupK& G, cudaStream_t s) {
     cudaMemsetAsync(G.err, 0, 256, s);
     const int g = grid_for((const void*)k_group_init, kThreads, 0, G.S);
     (note_launch(), k_group_init<<<g, kThreads, 0, s>>>(G));
-    (void)p;
+    if (G.hot_cap) {
+        cudaMemsetAsync(G.sample_keys, 0xFF, (size_t)kSampleCap * 8, s);
+        cudaMemsetAsync(G.sample_cnt, 0, (size_t)kSampleCap * 4, s);
+        cudaMemsetAsync(G.hot_n, 0, 4, s);
+    }
     return launch_status();
 }
 
 static tdg_status finish(const GroupK& G, const tdg_group_desc* d, void* ws, const tdg_group_out* out,
                          cudaStream_t s) {
-    const Layout L = layout_of(G.S, G.n_acc, G.nk, G.method);
+    const Layout L = layout_of(G.S, G.n_acc, G.nk, G.method, G.hot_cap != 0);
     int64_t* counts = (int64_t*)((char*)ws + L.emit);
     const int64_t chunks = (G.S + kEmitChunk - 1) / kEmitChunk;
-    (note_launch(), k_emit_count<<<(unsigned)chunks, kThreads, 0, s>>>(G.cnt, G.S, counts));
+    (note_launch(), k_emit_count<<<(unsigned)chunks, kThreads, 0, s>>>(G, counts));
     (note_launch(), k_scan_counts_g<<<1, 1024, 0, s>>>(counts, chunks, out->d_n_groups));
     OutK O;
     memset(&O, 0, sizeof(O));
@@ -534,54 +815,146 @@ static tdg_status finish(const GroupK& G, const tdg_group_desc* d, void* ws, con
     return err;
 }
 
-template <int PK, int MODE, bool JOIN>
+static bool group_w8(const GroupK& G, const Pred& P, const JoinK* J) {
+    if (!P.w8) return false;
+    for (int k = 0; k < G.nk; k++) if (elem_size(G.key[k].type, G.key[k].attrs) != 8) return false;
+    for (int a = 0; a < G.na; a++)
+        if (G.kind[a] != K_COUNT && elem_size(G.in[a].type, G.in[a].attrs) != 8) return false;
+    if (J) for (int k = 0; k < J->nk; k++) if (elem_size(J->lkeys[k].type, J->lkeys[k].attrs) != 8) return false;
+    return true;
+}
+
+template <int PK, int MODE, bool JOIN, bool W8>
 static tdg_status launch_main(const GroupK& G, const Pred& P, const tdg_expr& prog, const JoinK& J, int64_t n,
                               cudaStream_t s) {
-    const size_t smem = MODE == 0 ? (size_t)G.S * 8 * (1 + G.n_acc) : 0;
-    const void* fn = (const void*)k_group<PK, MODE, JOIN>;
+    const size_t smem = MODE == 0 ? smem_full_bytes(G.S, G.n_acc) : (G.hot_cap ? smem_hot_bytes(G.hot_cap, G.n_acc) : 0);
+    const void* fn = (const void*)k_group<PK, MODE, JOIN, W8>;
     const int g = grid_for(fn, kThreads, smem, (n + kItems - 1) / kItems);
-    (note_launch(), k_group<PK, MODE, JOIN><<<g, kThreads, smem, s>>>(G, P, prog, J, n));
+    (note_launch(), k_group<PK, MODE, JOIN, W8><<<g, kThreads, smem, s>>>(G, P, prog, J, n));
+    return launch_status();
+}
+
+template <int PK, int MODE, bool JOIN>
+static tdg_status launch_sample(const GroupK& G, const Pred& P, const tdg_expr& prog, const JoinK& J, int64_t n,
+                                cudaStream_t s) {
+    const int64_t m_rows = n < kSampleRows ? n : kSampleRows;
+    const int64_t step = n / m_rows;
+    const int g = grid_for((const void*)k_sample<PK, MODE, JOIN>, kThreads, 0, m_rows);
+    (note_launch(), k_sample<PK, MODE, JOIN><<<g, kThreads, 0, s>>>(G, P, prog, J, n, step, m_rows));
+    const int g2 = grid_for((const void*)k_select_hot, kThreads, 0, kSampleCap);
+    (note_launch(), k_select_hot<<<g2, kThreads, 0, s>>>(G));
     return launch_status();
 }
 
 template <bool JOIN>
 static tdg_status dispatch(int pk, const GroupK& G, bool smem, const Pred& P, const tdg_expr& prog,
-                           const JoinK& J, int64_t n, cudaStream_t s) {
+                           const JoinK& J, int64_t n, cudaStream_t s, EventTimer& tm) {
     const int mode = G.method == TDG_GROUP_HASH ? 2 : (smem ? 0 : 1);
-#define TDG_CASE(PKV, MV) if (pk == PKV && mode == MV) return launch_main<PKV, MV, JOIN>(G, P, prog, J, n, s);
-    TDG_CASE(0, 0) TDG_CASE(0, 1) TDG_CASE(0, 2)
-    TDG_CASE(1, 0) TDG_CASE(1, 1) TDG_CASE(1, 2)
-    TDG_CASE(2, 0) TDG_CASE(2, 1) TDG_CASE(2, 2)
+    tdg_status st = E_OK;
+    if (G.hot_cap && n > 0) {
+#define TDG_SMP(PKV, MV) if (pk == PKV && mode == MV) st = launch_sample<PKV, MV, JOIN>(G, P, prog, J, n, s);
+        TDG_SMP(0, 1) TDG_SMP(0, 2) TDG_SMP(1, 1) TDG_SMP(1, 2) TDG_SMP(2, 1) TDG_SMP(2, 2)
+#undef TDG_SMP
+        if (st) return st;
+    }
+    const bool w8 = pk != 2 && group_w8(G, P, JOIN ? &J : nullptr);
+    tm.start(s);
+#define TDG_CASE(PKV, MV, W) \
+    if (pk == PKV && mode == MV && w8 == W) { st = launch_main<PKV, MV, JOIN, W>(G, P, prog, J, n, s); tm.stop(s); return st; }
+    TDG_CASE(0, 0, true) TDG_CASE(0, 1, true) TDG_CASE(0, 2, true)
+    TDG_CASE(0, 0, false) TDG_CASE(0, 1, false) TDG_CASE(0, 2, false)
+    TDG_CASE(1, 0, true) TDG_CASE(1, 1, true) TDG_CASE(1, 2, true)
+    TDG_CASE(1, 0, false) TDG_CASE(1, 1, false) TDG_CASE(1, 2, false)
+    TDG_CASE(2, 0, false) TDG_CASE(2, 1, false) TDG_CASE(2, 2, false)
 #undef TDG_CASE
+    tm.stop(s);
     return E_NYI;
 }
 
-__global__ void __launch_bounds__(1024) k_scan_counts_g(int64_t* counts, int64_t m, int64_t* d_total) {
-    __shared__ long long part[1024];
-    const int64_t per = (m + blockDim.x - 1) / blockDim.x;
-    const int64_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
-    long long sum = 0;
-    for (int64_t i = b; i < e; i++) sum += counts[i];
-    part[threadIdx.x] = sum;
-    __syncthreads();
-    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-        long long v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
-        __syncthreads();
-        part[threadIdx.x] += v;
-        __syncthreads();
+// ---- shared with tdg_join.cu ------------------------------------------------------
+
+// Payload join -> group (see k_payload_build).  Sets *used when it ran; when
+// the shape does not qualify, or the build side turns out to hold duplicate
+// keys, it returns with *used == false and the caller takes the general path.
+tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, void* ws,
+                             const tdg_expr* pred, const uint64_t* sel, const JoinK* J, int64_t n_left,
+                             int64_t n_right, const tdg_group_out* out, cudaStream_t s, bool* used) {
+    *used = false;
+    if (J->method != TDG_JOIN_DIRECT || J->join_type != 0 || p->method != TDG_GROUP_DIRECT) return E_OK;
+    if (J->rkeys[0].type == T_F64 || p->n_slots >= 0xFFFFFFFFLL) return E_OK;
+    for (int a = 0; a < d->n_aggs; a++)
+        if (d->aggs[a].op != A_COUNT && d->aggs[a].in.side != 0) return E_OK;
+    GroupK G = make_gk(d, p, ws, d->nrows);
+    G.hot_cap = 0;
+    tdg_status st = prepare(G, s);
+    if (st) return st;
+    const bool narrow = p->n_slots < 0xFFFF;
+    void* map = J->head;
+    cudaMemsetAsync(map, 0xFF, (size_t)J->n_slots * (narrow ? 2 : 4), s);
+    EventTimer tb;
+    tb.start(s);
+    if (n_right > 0) {
+        if (narrow) {
+            const int g = grid_for((const void*)k_payload_build<uint16_t>, kThreads, 0, n_right);
+            (note_launch(), k_payload_build<uint16_t><<<g, kThreads, 0, s>>>(G, *J, (uint16_t*)map, n_right, G.err + 1));
+        } else {
+            const int g = grid_for((const void*)k_payload_build<uint32_t>, kThreads, 0, n_right);
+            (note_launch(), k_payload_build<uint32_t><<<g, kThreads, 0, s>>>(G, *J, (uint32_t*)map, n_right, G.err + 1));
+        }
     }
-    long long run = threadIdx.x ? part[threadIdx.x - 1] : 0;
-    for (int64_t i = b; i < e; i++) { long long c = counts[i]; counts[i] = run; run += c; }
-    if (threadIdx.x == blockDim.x - 1 && d_total) *d_total = part[blockDim.x - 1];
+    tb.stop(s);
+    int32_t flags[2] = {0, 0};
+    st = launch_status();
+    if (!st && cudaMemcpyAsync(flags, G.err, sizeof(flags), cudaMemcpyDeviceToHost, s) != cudaSuccess) st = E_IO;
+    if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = E_IO;
+    const float bms = tb.ms();
+    if (st) return st;
+    if (flags[0]) return flags[0];
+    if (flags[1]) return E_OK;                      // duplicate build keys: general path
+    if (tb.on) set_last_build_ms(bms);
+    *used = true;
+    int pk;
+    Pred P = make_pred(pred, sel, &pk);
+    static tdg_expr empty;
+    const tdg_expr& prog = pred ? *pred : empty;
+    const bool sm = p->smem != 0;
+    const bool w8 = pk != 2 && group_w8(G, P, J);
+    const size_t smem = sm ? smem_full_bytes(G.S, G.n_acc) : 0;
+    EventTimer tm;
+    tm.start(s);
+#define TDG_PL(PKV, SMV, PT, W)                                                                         \
+    if (pk == PKV && sm == SMV && narrow == (sizeof(PT) == 2) && w8 == W) {                             \
+        const int g = grid_for((const void*)k_payload_probe<PKV, SMV, PT, W>, kThreads, smem,            \
+                               (n_left + kItems - 1) / kItems);                                          \
+        (note_launch(), k_payload_probe<PKV, SMV, PT, W><<<g, kThreads, smem, s>>>(                      \
+            G, P, prog, J->lkeys[0], J->kmin, J->n_slots, (const PT*)map, n_left));                      \
+    }
+    TDG_PL(0, true, uint16_t, true) TDG_PL(0, false, uint16_t, true)
+    TDG_PL(0, true, uint32_t, true) TDG_PL(0, false, uint32_t, true)
+    TDG_PL(1, true, uint16_t, true) TDG_PL(1, false, uint16_t, true)
+    TDG_PL(1, true, uint32_t, true) TDG_PL(1, false, uint32_t, true)
+    TDG_PL(0, true, uint16_t, false) TDG_PL(0, false, uint16_t, false)
+    TDG_PL(0, true, uint32_t, false) TDG_PL(0, false, uint32_t, false)
+    TDG_PL(1, true, uint16_t, false) TDG_PL(1, false, uint16_t, false)
+    TDG_PL(1, true, uint32_t, false) TDG_PL(1, false, uint32_t, false)
+    TDG_PL(2, true, uint16_t, false) TDG_PL(2, false, uint16_t, false)
+    TDG_PL(2, true, uint32_t, false) TDG_PL(2, false, uint32_t, false)
+#undef TDG_PL
+    tm.stop(s);
+    st = launch_status();
+    if (st) { tm.ms(); return st; }
+    st = finish(G, d, ws, out, s);
+    const float ms = tm.ms();
+    if (tm.on) set_last_main_ms(ms);
+    return st;
 }
 
-// ---- shared with tdg_join.cu ------------------------------------------------------
 tdg_status group_run_joined(const tdg_group_desc* d, const tdg_group_plan* p, void* ws,
                             const tdg_expr* pred, const uint64_t* sel, const JoinK* J, int64_t n_left,
                             int64_t n_right, const tdg_group_out* out, cudaStream_t s) {
     if (p->method != TDG_GROUP_DIRECT && p->method != TDG_GROUP_HASH) return E_RANGE;
-    GroupK G = make_gk(d, p, ws);
-    tdg_status st = prepare(G, p, s);
+    GroupK G = make_gk(d, p, ws, d->nrows);
+    tdg_status st = prepare(G, s);
     if (st) return st;
     int pk;
     Pred P = make_pred(pred, sel, &pk);
@@ -589,9 +962,7 @@ tdg_status group_run_joined(const tdg_group_desc* d, const tdg_group_plan* p, vo
     const tdg_expr& prog = pred ? *pred : empty;
     EventTimer tm;
     if (J) {
-        tm.start(s);
-        st = dispatch<true>(pk, G, p->smem != 0, P, prog, *J, n_left, s);
-        tm.stop(s);
+        st = dispatch<true>(pk, G, p->smem != 0, P, prog, *J, n_left, s, tm);
         if (!st && J->join_type == 2 && n_right > 0) {
             const int mode = G.method == TDG_GROUP_HASH ? 2 : 1;
             const int g = grid_for((const void*)k_group_unmatched<1>, kThreads, 0, n_right);
@@ -602,9 +973,7 @@ tdg_status group_run_joined(const tdg_group_desc* d, const tdg_group_plan* p, vo
     } else {
         JoinK none;
         memset(&none, 0, sizeof(none));
-        tm.start(s);
-        st = dispatch<false>(pk, G, p->smem != 0, P, prog, none, d->nrows, s);
-        tm.stop(s);
+        st = dispatch<false>(pk, G, p->smem != 0, P, prog, none, d->nrows, s, tm);
     }
     if (st) { tm.ms(); return st; }
     st = finish(G, d, ws, out, s);       // synchronizes the stream

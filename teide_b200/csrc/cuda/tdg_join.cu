@@ -21,6 +21,9 @@ namespace tdg {
 tdg_status group_run_joined(const tdg_group_desc* d, const tdg_group_plan* p, void* ws,
                             const tdg_expr* pred, const uint64_t* sel, const JoinK* J, int64_t n_left,
                             int64_t n_right, const tdg_group_out* out, cudaStream_t s);
+tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, void* ws,
+                             const tdg_expr* pred, const uint64_t* sel, const JoinK* J, int64_t n_left,
+                             int64_t n_right, const tdg_group_out* out, cudaStream_t s, bool* used);
 
 constexpr int kJChunk = kThreads * 16;
 constexpr int kMaxJCols = 16;
@@ -324,7 +327,7 @@ extern "C" tdg_status tdg_join_count(const tdg_join_desc* d, const tdg_join_plan
     }
     (note_launch(), k_scan_counts_g<<<1, 1024, 0, s>>>(counts, chunks, counts + chunks));
     if (d->join_type == 2 && d->n_right > 0)
-        (note_launch(), k_unmatched_count<<<1, 1024, 0, s>>>(J.matched, d->n_right, counts + chunks + 1));
+        (note_launch(), k_unmatched_count<<<1, kThreads, 0, s>>>(J.matched, d->n_right, counts + chunks + 1));
     (note_launch(), k_join_total<<<1, 1, 0, s>>>(counts, chunks, d_count));
     tdg_status st = launch_status();
     if (st) return st;
@@ -373,7 +376,7 @@ extern "C" tdg_status tdg_join_emit(const tdg_join_desc* d, const tdg_join_plan*
         if (cudaMemcpyAsync(&probe_total, counts + chunks, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess) return E_IO;
         if (cudaStreamSynchronize(s) != cudaSuccess) return E_IO;
         const uint8_t* matched = (const uint8_t*)((char*)ws + L.matched);
-        (note_launch(), k_unmatched_emit<<<1, 1024, 0, s>>>(matched, d->n_right, probe_total, C));
+        (note_launch(), k_unmatched_emit<<<1, kThreads, 0, s>>>(matched, d->n_right, probe_total, C));
     }
     return launch_status();
 }
@@ -383,8 +386,16 @@ extern "C" tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_
                                          const tdg_group_desc* g, const tdg_group_plan* gp, void* gws,
                                          const tdg_group_out* out, void* stream) {
     if (!d || !jp || !jws || !g || !gp || !gws || !out) return E_TYPE;
+    tdg_status st = check_desc(d);
+    if (st) return st;
     cudaStream_t s = (cudaStream_t)stream;
     JoinK J = make_jk(d, jp, jws);
+    cudaMemsetAsync(J.ht.err, 0, 256, s);
+    bool used = false;
+    st = group_run_payload(g, gp, gws, lpred, lsel, &J, d->n_left, d->n_right, out, s, &used);
+    if (st || used) return st;
+    st = tdg_join_build(d, jp, jws, stream);
+    if (st) return st;
     if (d->join_type == 2 && d->n_right > 0) cudaMemsetAsync(J.matched, 0, (size_t)d->n_right, s);
     return group_run_joined(g, gp, gws, lpred, lsel, &J, d->n_left, d->n_right, out, s);
 }

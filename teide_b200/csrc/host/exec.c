@@ -262,8 +262,10 @@ static td_t* fetch_vec(ex_t* x, const void* dptr, int8_t type, uint8_t attrs, in
     td_t* v = vec_like(type, attrs, n);
     if (!v || TD_IS_ERR(v)) return v ? v : TD_ERR_PTR(TD_ERR_OOM);
     size_t bytes = (size_t)n * td_sym_elem_size(type, attrs);
+    if (bytes >= ((size_t)8 << 20)) tdb_pin_host(v);     /* DMA straight into the result */
     int st = tdb_d2h(&x->c, td_data(v), dptr, bytes);
     if (st) { td_release(v); return TD_ERR_PTR(st); }
+    tdb_adopt_mirror(&x->c, v, (void*)dptr);
     return v;
 }
 
@@ -615,7 +617,9 @@ static td_t* dense_side(ex_t* x, val_t* v) {
     return materialize(x, v);
 }
 
-static int prepare_join(ex_t* x, td_op_ext_t* ext, val_t* lv, td_t* right, jbuilt_t* jb) {
+/* Plan the join and allocate its scratch; build the table unless the caller
+ * hands it to tdg_join_group_run, which builds it itself. */
+static int prepare_join(ex_t* x, td_op_ext_t* ext, val_t* lv, td_t* right, jbuilt_t* jb, int build) {
     memset(jb, 0, sizeof(*jb));
     td_t* left = lv->obj;
     if (!left || left->type != TD_TABLE || !right || right->type != TD_TABLE) return TD_ERR_TYPE;
@@ -653,7 +657,7 @@ static int prepare_join(ex_t* x, td_op_ext_t* ext, val_t* lv, td_t* right, jbuil
     jb->ws = tdb_dev_alloc(&x->c, jb->p.ws_bytes);
     if (!jb->ws) return TD_ERR_OOM;
     if ((st = tdb_check_cancel())) return st;
-    return CALL(tdg_join_build(d, &jb->p, jb->ws, x->c.stream));
+    return build ? CALL(tdg_join_build(d, &jb->p, jb->ws, x->c.stream)) : TD_OK;
 }
 
 static int is_right_key(ex_t* x, td_op_ext_t* ext, int64_t name) {
@@ -824,7 +828,7 @@ static td_t* exec_group_node(ex_t* x, td_op_t* op) {
             res = right;
         } else {
             jbuilt_t jb;
-            int st = prepare_join(x, jext, &lv, right, &jb);
+            int st = prepare_join(x, jext, &lv, right, &jb, 0);
             if (st) {
                 res = TD_ERR_PTR(st);
             } else {
@@ -931,7 +935,7 @@ static td_t* exec_value(ex_t* x, td_op_t* op, val_t* out) {
             td_t* res = right;
             if (!TD_IS_ERR(right)) {
                 jbuilt_t jb;
-                st = prepare_join(x, ext, &lv, right, &jb);
+                st = prepare_join(x, ext, &lv, right, &jb, 1);
                 res = st ? TD_ERR_PTR(st) : join_materialize(x, ext, &lv, &jb);
                 td_release(right);
             }

@@ -185,32 +185,33 @@ void tdb_mirror_forget(td_t* v) {
 }
 
 void tdb_gpu_on_free(td_t* v, tdb_block_prefix* p) {
+    (void)p;
     tdb_mirror_forget(v);
-    if (atomic_load(&p->pinned)) {
-        cudaHostUnregister(p->raw);
-        cudaGetLastError();
-        atomic_store(&p->pinned, 0);
-    }
+}
+
+/* A large host block leaves the heap's cache for good: drop its page lock. */
+void tdb_gpu_unpin_raw(void* raw) {
+    cudaHostUnregister(raw);
+    cudaGetLastError();
 }
 
 static size_t col_bytes(td_t* col) {
     return (size_t)col->len * td_sym_elem_size(col->type, col->attrs);
 }
 
-/* Page-lock the used part of a large host block once, so uploads from it
- * run as DMA at link speed instead of through a staging buffer. */
-static void pin_host(td_t* col) {
+/* Page-lock a large host block once (the whole block: the heap reuses it for
+ * any vector of the same size class), so copies to and from it run as DMA at
+ * link speed instead of through a staging buffer. */
+void tdb_pin_host(td_t* col) {
     if (!tdb_is_heap_block(col) || getenv("TD_GPU_NO_HOST_PIN")) return;
     tdb_block_prefix* p = tdb_prefix(col);
     if (p->kind != TDB_BLK_MMAP || atomic_load(&p->pinned)) return;
-    size_t used = sizeof(tdb_block_prefix) + 32 + col_bytes(col);
-    used = (used + 4095) & ~(size_t)4095;
-    if (used > p->raw_size) used = p->raw_size;
-    if (cudaHostRegister(p->raw, used, cudaHostRegisterPortable) == cudaSuccess)
-        atomic_store(&p->pinned, used);
+    if (cudaHostRegister(p->raw, p->raw_size, cudaHostRegisterPortable) == cudaSuccess)
+        atomic_store(&p->pinned, p->raw_size);
     else
         cudaGetLastError();
 }
+#define pin_host tdb_pin_host
 
 static int upload(tdb_ctx* c, td_t* col, tdb_devcol* out, int persistent) {
     size_t bytes = col_bytes(col);
@@ -362,6 +363,14 @@ int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
     if (i >= 0 && mirrors[i].dc.len == col->len) {
         *out = mirrors[i].dc;
         pthread_mutex_unlock(&mu);
+        if (want_stats && !out->has_stats && is_int_type(out->type)) {
+            int st = compute_stats(c, out);
+            if (st) return st;
+            pthread_mutex_lock(&mu);
+            i = find_mirror_locked(col);
+            if (i >= 0) mirrors[i].dc = *out;
+            pthread_mutex_unlock(&mu);
+        }
         return TD_OK;
     }
     pthread_mutex_unlock(&mu);
@@ -393,6 +402,30 @@ int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
     tls_ntm++;
     *out = t->dc;
     return TD_OK;
+}
+
+/* Keep a device buffer this call produced as the resident mirror of the host
+ * vector it was copied to: a later query over the result reads it from HBM.
+ * The buffer leaves the call's transient list; it is freed with the host
+ * vector (td_free) or by td_gpu_unpin. */
+void tdb_adopt_mirror(tdb_ctx* c, td_t* host, void* dptr) {
+    if (!host || TD_IS_ERR(host) || !dptr || getenv("TD_GPU_NO_RESULT_MIRROR")) return;
+    int k = -1;
+    for (int i = 0; i < c->n_tmp; i++) if (c->tmp[i] == dptr) { k = i; break; }
+    if (k < 0) return;
+    pthread_mutex_lock(&mu);
+    if (n_mir == cap_mir) {
+        int ncap = cap_mir ? cap_mir * 2 : 64;
+        mirror_t* nm = realloc(mirrors, (size_t)ncap * sizeof(mirror_t));
+        if (!nm) { pthread_mutex_unlock(&mu); return; }
+        mirrors = nm; cap_mir = ncap;
+    }
+    tdb_devcol dc;
+    memset(&dc, 0, sizeof(dc));
+    dc.dptr = dptr; dc.len = host->len; dc.type = host->type; dc.attrs = host->attrs;
+    mirrors[n_mir++] = (mirror_t){ host, tdb_block_serial(host), dc, col_bytes(host) };
+    pthread_mutex_unlock(&mu);
+    c->tmp[k] = c->tmp[--c->n_tmp];
 }
 
 td_err_t td_gpu_pin(td_t* tbl) {

@@ -17,6 +17,7 @@
  */
 
 #include "internal.h"
+#include <pthread.h>
 #include <stdlib.h>
 #include <string.h>
 #include <sys/mman.h>
@@ -27,6 +28,55 @@ static _Atomic(size_t) st_alloc, st_free, st_bytes, st_peak, st_direct, st_direc
 static _Atomic(uint64_t) st_serial;
 
 void tdb_gpu_on_free(td_t* v, tdb_block_prefix* p);   /* gpu.c */
+void tdb_gpu_unpin_raw(void* raw);                    /* gpu.c */
+
+/* Freed mmap blocks are kept (up to TDB_CACHE_MAX bytes) and handed out again
+ * for the same block size: their pages are already committed and, once a
+ * block has been page-locked for a transfer, it stays page-locked, so
+ * query results reuse fast DMA destinations instead of faulting in fresh
+ * pages every time. */
+#define TDB_CACHE_MAX ((size_t)16 << 30)
+#define TDB_CACHE_SLOTS 256
+static pthread_mutex_t cache_mu = PTHREAD_MUTEX_INITIALIZER;
+static void* cache_raw[TDB_CACHE_SLOTS];
+static size_t cache_size[TDB_CACHE_SLOTS];
+static size_t cache_pinned[TDB_CACHE_SLOTS];
+static int cache_n;
+static size_t cache_bytes;
+
+static void* cache_take(size_t raw_size, size_t* pinned) {
+    void* r = NULL;
+    pthread_mutex_lock(&cache_mu);
+    for (int i = 0; i < cache_n; i++) {
+        if (cache_size[i] == raw_size) {
+            r = cache_raw[i];
+            *pinned = cache_pinned[i];
+            cache_bytes -= raw_size;
+            cache_n--;
+            cache_raw[i] = cache_raw[cache_n];
+            cache_size[i] = cache_size[cache_n];
+            cache_pinned[i] = cache_pinned[cache_n];
+            break;
+        }
+    }
+    pthread_mutex_unlock(&cache_mu);
+    return r;
+}
+
+static int cache_put(void* raw, size_t raw_size, size_t pinned) {
+    int ok = 0;
+    pthread_mutex_lock(&cache_mu);
+    if (cache_n < TDB_CACHE_SLOTS && cache_bytes + raw_size <= TDB_CACHE_MAX) {
+        cache_raw[cache_n] = raw;
+        cache_size[cache_n] = raw_size;
+        cache_pinned[cache_n] = pinned;
+        cache_n++;
+        cache_bytes += raw_size;
+        ok = 1;
+    }
+    pthread_mutex_unlock(&cache_mu);
+    return ok;
+}
 
 static uint8_t ceil_log2(size_t x) {
     uint8_t k = 0;
@@ -65,10 +115,14 @@ td_t* td_alloc(size_t data_size) {
     size_t raw_size = block + sizeof(tdb_block_prefix);
     void* raw;
     uint32_t kind;
+    size_t pinned = 0;
     if (block >= TDB_MMAP_MIN) {
         raw_size = (raw_size + 4095) & ~(size_t)4095;
-        raw = mmap(NULL, raw_size, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
-        if (raw == MAP_FAILED) return NULL;
+        raw = cache_take(raw_size, &pinned);
+        if (!raw) {
+            raw = mmap(NULL, raw_size, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+            if (raw == MAP_FAILED) return NULL;
+        }
         kind = TDB_BLK_MMAP;
         atomic_fetch_add(&st_direct, 1);
         atomic_fetch_add(&st_direct_bytes, raw_size);
@@ -83,6 +137,7 @@ td_t* td_alloc(size_t data_size) {
     p->kind = kind;
     p->raw = raw;
     p->raw_size = raw_size;
+    atomic_store(&p->pinned, pinned);
     p->serial = atomic_fetch_add(&st_serial, 1) + 1;
     td_t* v = (td_t*)(p + 1);
     memset(v, 0, 32);
@@ -138,11 +193,9 @@ static void for_each_owned(td_t* v, void (*fn)(td_t*)) {
 
 void tdb_retain_owned_refs(td_t* v) { if (v && !TD_IS_ERR(v)) for_each_owned(v, td_retain); }
 
-void td_free(td_t* v) {
-    if (!v || TD_IS_ERR(v)) return;
-    atomic_store_explicit(&v->rc, 1, memory_order_relaxed);
-    for_each_owned(v, td_release);
-    if (!tdb_is_heap_block(v)) return;          /* not ours: leave it alone */
+/* Return a block's memory: large blocks go back to the cache (still
+ * page-locked) when there is room, else to the OS. */
+static void release_block(td_t* v) {
     tdb_block_prefix* p = tdb_prefix(v);
     tdb_gpu_on_free(v, p);
     size_t block = (size_t)1 << v->order;
@@ -150,12 +203,25 @@ void td_free(td_t* v) {
     atomic_fetch_add(&st_free, 1);
     atomic_fetch_sub(&st_bytes, block);
     if (p->kind == TDB_BLK_MMAP) {
+        void* raw = p->raw;
+        size_t raw_size = p->raw_size, pinned = atomic_load(&p->pinned);
         atomic_fetch_sub(&st_direct, 1);
-        atomic_fetch_sub(&st_direct_bytes, p->raw_size);
-        munmap(p->raw, p->raw_size);
+        atomic_fetch_sub(&st_direct_bytes, raw_size);
+        if (!cache_put(raw, raw_size, pinned)) {
+            if (pinned) tdb_gpu_unpin_raw(raw);
+            munmap(raw, raw_size);
+        }
     } else {
         free(p->raw);
     }
+}
+
+void td_free(td_t* v) {
+    if (!v || TD_IS_ERR(v)) return;
+    atomic_store_explicit(&v->rc, 1, memory_order_relaxed);
+    for_each_owned(v, td_release);
+    if (!tdb_is_heap_block(v)) return;          /* not ours: leave it alone */
+    release_block(v);
 }
 
 td_t* td_alloc_copy(td_t* v) {
@@ -194,15 +260,7 @@ td_t* td_scratch_realloc(td_t* v, size_t new_data_size) {
     atomic_store_explicit(&n->rc, 1, memory_order_relaxed);
     /* ownership of children moves to the new block: free the old one without
      * releasing them */
-    tdb_block_prefix* p = tdb_prefix(v);
-    if (tdb_is_heap_block(v)) {
-        tdb_gpu_on_free(v, p);
-        size_t block = (size_t)1 << v->order;
-        p->magic = 0;
-        atomic_fetch_add(&st_free, 1);
-        atomic_fetch_sub(&st_bytes, block);
-        if (p->kind == TDB_BLK_MMAP) munmap(p->raw, p->raw_size); else free(p->raw);
-    }
+    if (tdb_is_heap_block(v)) release_block(v);
     return n;
 }
 

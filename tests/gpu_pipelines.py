@@ -10,7 +10,15 @@ def const(g, k):
     return g.f64(k) if isinstance(k, float) else g.i64(k)
 
 
-def readme_group(td, tbl, pred, keys, aggs):
+def _result(td, r, as_dict):
+    """The result as {name: numpy array}, or just released (as_dict False:
+    the query's host td_t result is produced and dropped unread)."""
+    out = td.table_dict(r) if as_dict else None
+    td.release(r)
+    return out
+
+
+def readme_group(td, tbl, pred, keys, aggs, as_dict=True):
     """One graph: group keys and aggregate inputs are td_filter(scan, pred)
     vectors sharing one predicate (README.md's filter + group + sum)."""
     g = td.graph(tbl)
@@ -22,9 +30,7 @@ def readme_group(td, tbl, pred, keys, aggs):
         r = g.execute(g.group(ks, [a for a, _ in aggs], ins), optimize=True)
     finally:
         g.free()
-    out = td.table_dict(r)
-    td.release(r)
-    return out
+    return _result(td, r, as_dict)
 
 
 def two_graph_group(td, tbl, pred, keys, aggs):
@@ -47,7 +53,7 @@ def two_graph_group(td, tbl, pred, keys, aggs):
     return out
 
 
-def fused_join_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_type=0):
+def fused_join_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_type=0, as_dict=True):
     """One graph bound to no table: group over join(filter(probe), build)."""
     g = td.graph(None)
     try:
@@ -58,9 +64,7 @@ def fused_join_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_ty
         r = g.execute(grp)
     finally:
         g.free()
-    out = td.table_dict(r)
-    td.release(r)
-    return out
+    return _result(td, r, as_dict)
 
 
 def join_then_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_type=0):
