@@ -192,11 +192,17 @@ __device__ inline uint64_t x_eval(const tdg_expr& e, int64_t row) {
 // kMaxTerms column-vs-constant comparisons); anything else runs through the
 // interpreter.  The launcher analyses the program on the host.
 constexpr int kMaxTerms = 4;
+// A term is evaluated branch-free as (lo <= v && v <= hi) != neg: EQ is
+// [k, k], LT/LE/GT/GE are half-open ranges (strict bounds on doubles move to
+// the adjacent representable value, so NaN still fails), NE is EQ negated.
 struct Term {
     tdg_col col;
-    int32_t op;      // TDG_X_EQ .. TDG_X_GE
+    int32_t op;      // TDG_X_EQ .. TDG_X_GE (for the interpreter fallback)
     int32_t f;       // compare as double
     int64_t k;       // constant bits (int64 or double)
+    int64_t lo, hi;  // inclusive bounds (double bits when f)
+    int32_t neg;
+    int32_t pad;
 };
 struct Pred {
     int32_t kind;    // 0 = every row, 1 = conjunction of terms, 2 = program
@@ -242,11 +248,14 @@ __device__ __forceinline__ bool row_pass(const Pred& p, const tdg_expr& prog, in
             if (i < p.n) {
                 const Term& t = p.t[i];
                 bool b;
-                if (W8) b = t.f ? cmp(t.op, ld_f8(t.col, r), __longlong_as_double(t.k))
-                                : cmp(t.op, ld_i8(t.col, r), t.k);
-                else    b = t.f ? cmp(t.op, ld_f(t.col, r), __longlong_as_double(t.k))
-                                : cmp(t.op, ld_i(t.col, r), t.k);
-                ok = ok && b;
+                if (t.f) {
+                    const double v = W8 ? ld_f8(t.col, r) : ld_f(t.col, r);
+                    b = (v >= __longlong_as_double(t.lo)) & (v <= __longlong_as_double(t.hi));
+                } else {
+                    const int64_t v = W8 ? ld_i8(t.col, r) : ld_i(t.col, r);
+                    b = (v >= t.lo) & (v <= t.hi);
+                }
+                ok = ok && (b != (bool)t.neg);
             }
         }
     } else if (PK == 2) {

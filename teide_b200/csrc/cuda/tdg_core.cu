@@ -9,6 +9,7 @@
 // packs bits with warp ballots, and compaction is a two-pass stable scatter.
 #include "tdg_common.cuh"
 #include <atomic>
+#include <math.h>
 #include <string.h>
 
 namespace tdg {
@@ -95,6 +96,35 @@ static bool collect_terms(const tdg_expr* e, int reg, Pred* p) {
     t.op = op;
     t.f = col->kind == 1;
     t.k = cst->imm;
+    t.neg = op == TDG_X_NE;
+    if (t.f) {
+        double k;
+        memcpy(&k, &cst->imm, 8);
+        double lo = -INFINITY, hi = INFINITY;
+        switch (op) {
+            case TDG_X_EQ: case TDG_X_NE: lo = hi = k; break;
+            case TDG_X_LT: hi = nextafter(k, -INFINITY); break;
+            case TDG_X_LE: hi = k; break;
+            case TDG_X_GT: lo = nextafter(k, INFINITY); break;
+            default: lo = k; break;
+        }
+        if (k != k) { lo = INFINITY; hi = -INFINITY; }   // comparisons with NaN are false
+        if (k != k && op == TDG_X_NE) { lo = INFINITY; hi = -INFINITY; }
+        memcpy(&t.lo, &lo, 8);
+        memcpy(&t.hi, &hi, 8);
+    } else {
+        const int64_t k = cst->imm;
+        int64_t lo = INT64_MIN, hi = INT64_MAX;
+        switch (op) {
+            case TDG_X_EQ: case TDG_X_NE: lo = hi = k; break;
+            case TDG_X_LT: if (k == INT64_MIN) { lo = 1; hi = 0; } else hi = k - 1; break;
+            case TDG_X_LE: hi = k; break;
+            case TDG_X_GT: if (k == INT64_MAX) { lo = 1; hi = 0; } else lo = k + 1; break;
+            default: lo = k; break;
+        }
+        t.lo = lo;
+        t.hi = hi;
+    }
     return true;
 }
 

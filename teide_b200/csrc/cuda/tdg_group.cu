@@ -68,6 +68,7 @@ struct GroupK {
     tdg_col in[TDG_MAX_AGGS];
     int64_t S;
     unsigned long long* rec;      // S * W words
+    unsigned long long finit[TDG_MAX_AGGS + 2];   // initial value of each record word
     HtRef ht;
     int32_t* err;                 // [0] error code, [1] duplicate build key (payload join)
     int64_t* sample_keys;
@@ -147,18 +148,16 @@ __device__ __forceinline__ void ld_items_f(const tdg_col& c, const int64_t (&r)[
     }
 }
 
-// One accumulator update (shared or global memory).  The returned old value
-// is never used, so global updates compile to fire-and-forget reductions.
-__device__ __forceinline__ void upd(unsigned long long* a, int kind, int64_t iv, double fv) {
-    switch (kind) {
-        case K_SUM_I: atomicAdd(a, (unsigned long long)iv); break;
-        case K_SUM_F: atomicAdd((double*)a, fv); break;
-        case K_MIN_I: atomicMin((long long*)a, (long long)iv); break;
-        case K_MAX_I: atomicMax((long long*)a, (long long)iv); break;
-        case K_MIN_F: if (fv == fv) atomicMin((long long*)a, f2ord(fv)); break;
-        case K_MAX_F: if (fv == fv) atomicMax((long long*)a, f2ord(fv)); break;
-        default: break;
-    }
+// Accumulator updates.  Sums are fire-and-forget reductions; a global MIN/MAX
+// first reads the current value and skips the atomic when it cannot change,
+// which after the first rows of a group is almost always.
+template <bool GL>
+__device__ __forceinline__ void upd_min(unsigned long long* a, long long v) {
+    if (!GL || v < *(volatile long long*)a) atomicMin((long long*)a, v);
+}
+template <bool GL>
+__device__ __forceinline__ void upd_max(unsigned long long* a, long long v) {
+    if (!GL || v > *(volatile long long*)a) atomicMax((long long*)a, v);
 }
 
 // Merge one accumulator value (already in accumulator form) into another.
@@ -320,30 +319,59 @@ __device__ __forceinline__ void accumulate_at(const GroupK& G, const SmemView& V
             else atomicAdd(grec(G, slot[i]), 1ULL);
         }
     }
+    // one dispatch per aggregate, then a straight loop over the N rows
+#define TDG_TARGET(i) (hidx[i] >= 0 ? V.acc + (int64_t)ai * V.cap + hidx[i] : grec(G, slot[i]) + 1 + ai)
     for (int a = 0; a < G.na; a++) {
         const int kind = G.kind[a];
         if (kind == K_COUNT) continue;
         const int ai = G.ai[a];
         const tdg_col& c = G.in[a];
         const int64_t (&rr)[N] = c.side ? rb : rp;
-        int64_t iv[N];
-        double fv[N];
         if (kind == K_SUM_F || kind == K_MIN_F || kind == K_MAX_F) {
-            ld_items_f<W8, N>(c, rr, ok, fv);
+            double v[N];
+            ld_items_f<W8, N>(c, rr, ok, v);
+            if (kind == K_SUM_F) {
 #pragma unroll
-            for (int i = 0; i < N; i++) iv[i] = 0;
+                for (int i = 0; i < N; i++) if (ok[i]) atomicAdd((double*)TDG_TARGET(i), v[i]);
+            } else if (kind == K_MIN_F) {
+#pragma unroll
+                for (int i = 0; i < N; i++)
+                    if (ok[i] && v[i] == v[i]) {
+                        if (hidx[i] >= 0) upd_min<false>(TDG_TARGET(i), f2ord(v[i]));
+                        else upd_min<true>(TDG_TARGET(i), f2ord(v[i]));
+                    }
+            } else {
+#pragma unroll
+                for (int i = 0; i < N; i++)
+                    if (ok[i] && v[i] == v[i]) {
+                        if (hidx[i] >= 0) upd_max<false>(TDG_TARGET(i), f2ord(v[i]));
+                        else upd_max<true>(TDG_TARGET(i), f2ord(v[i]));
+                    }
+            }
         } else {
-            ld_items_i<W8, N>(c, rr, ok, iv);
+            int64_t v[N];
+            ld_items_i<W8, N>(c, rr, ok, v);
+            if (kind == K_SUM_I) {
 #pragma unroll
-            for (int i = 0; i < N; i++) fv[i] = 0;
-        }
+                for (int i = 0; i < N; i++) if (ok[i]) atomicAdd(TDG_TARGET(i), (unsigned long long)v[i]);
+            } else if (kind == K_MIN_I) {
 #pragma unroll
-        for (int i = 0; i < N; i++) {
-            if (!ok[i]) continue;
-            if (hidx[i] >= 0) upd(V.acc + (int64_t)ai * V.cap + hidx[i], kind, iv[i], fv[i]);
-            else upd(grec(G, slot[i]) + 1 + ai, kind, iv[i], fv[i]);
+                for (int i = 0; i < N; i++)
+                    if (ok[i]) {
+                        if (hidx[i] >= 0) upd_min<false>(TDG_TARGET(i), v[i]);
+                        else upd_min<true>(TDG_TARGET(i), v[i]);
+                    }
+            } else {
+#pragma unroll
+                for (int i = 0; i < N; i++)
+                    if (ok[i]) {
+                        if (hidx[i] >= 0) upd_max<false>(TDG_TARGET(i), v[i]);
+                        else upd_max<true>(TDG_TARGET(i), v[i]);
+                    }
+            }
         }
     }
+#undef TDG_TARGET
 }
 
 template <int MODE, bool W8, int N>
@@ -523,14 +551,30 @@ __global__ void __launch_bounds__(kThreads) k_group_unmatched(GroupK G, const Jo
     }
 }
 
+// Initial values of the slot records.  Each warp fills 32 whole records as
+// 32*W consecutive words, so every store instruction writes 256 contiguous
+// bytes (no partial-sector read-modify-write in L2).
 __global__ void k_group_init(const GroupK G) {
-    for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < G.S; s += (int64_t)gridDim.x * blockDim.x) {
-        unsigned long long* r = grec(G, s);
-        r[0] = 0;
-        for (int a = 0; a < G.na; a++)
-            if (G.ai[a] >= 0) r[1 + G.ai[a]] = acc_init_kind(G.kind[a]);
-        if (G.method == TDG_GROUP_HASH) G.ht.state[s] = 0;
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int W = G.W;
+    const int step = 32 % W;
+    const int64_t nchunks = (G.S + 31) >> 5;
+    for (int64_t ch = warp; ch < nchunks; ch += nwarps) {
+        const int64_t recs = G.S - ch * 32 < 32 ? G.S - ch * 32 : 32;
+        const int words = (int)(recs * W);
+        unsigned long long* base = G.rec + ch * 32 * W;
+        int f = lane % W;
+        for (int j = lane; j < words; j += 32) {
+            base[j] = G.finit[f];
+            f += step;
+            if (f >= W) f -= W;
+        }
     }
+    if (G.method == TDG_GROUP_HASH)
+        for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < G.S; s += (int64_t)gridDim.x * blockDim.x)
+            G.ht.state[s] = 0;
 }
 
 // ---- emit ------------------------------------------------------------------------
@@ -761,6 +805,7 @@ static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws
         G.in[a] = d->aggs[a].in;
         G.kind[a] = kind_of(d->aggs[a]);
         G.ai[a] = G.op[a] == A_COUNT ? -1 : ai++;
+        if (G.ai[a] >= 0) G.finit[1 + G.ai[a]] = acc_init_kind(G.kind[a]);
     }
     if (p->method == TDG_GROUP_HASH) {
         G.ht.state = (uint32_t*)(w + L.state);
