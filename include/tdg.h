@@ -173,6 +173,25 @@ tdg_status tdg_group_run(const tdg_group_desc* d, const tdg_expr* pred, const ui
                          const tdg_group_plan* plan, void* ws, const tdg_group_out* out,
                          void* stream);
 
+/* Group-by that allocates nothing.  No counterpart in the reference.
+ *
+ * For callers that cannot call cudaMalloc -- an engine embedded in a process
+ * whose device memory belongs to another runtime's caching allocator (a
+ * cudaMalloc there fails or fragments that pool), or a latency-critical path
+ * that cannot take cudaMalloc's implicit device synchronization.  Same inputs,
+ * outputs and results as tdg_group_run, but the scratch comes from an array of
+ * TDG_STATIC_SCRATCH_BYTES compiled into the library, which every GPU that
+ * loads the library holds until the process exits.  `out` must hold
+ * plan.max_groups rows, where tdg_group_plan_make(d, 0, &plan) gives the plan
+ * (and its ws_bytes); a group-by that needs more scratch than the array holds
+ * is refused with TD_ERR_RANGE.  The first call on a device looks up the
+ * array's device address; make it before any stream capture.  Every call
+ * shares the array, and each call re-initializes what it reads, but calls
+ * that overlap on the GPU race: serialize them. */
+#define TDG_STATIC_SCRATCH_BYTES (16u << 20)
+tdg_status tdg_group_run_static(const tdg_group_desc* d, const tdg_expr* pred, const uint64_t* sel_in,
+                                const tdg_group_out* out, void* stream);
+
 /* ---- join ----------------------------------------------------------------------
  * Equi-join of a probe (left) side against a build (right) side on n_keys
  * key columns.  join_type 0 = inner, 1 = left outer, 2 = full outer.

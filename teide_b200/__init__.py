@@ -47,7 +47,7 @@ def load():
     return _td
 
 
-def tdg():
+def device_abi():
     """The binding of the device-path C ABI (include/tdg.h)."""
     from .tdg import Tdg
     return Tdg(load().lib)

@@ -313,4 +313,10 @@ bool timing_on();
 void set_last_main_ms(float ms);
 void set_last_build_ms(float ms);
 
+// While alive, this thread's tdg calls record no timing events.
+struct ThreadTimingOff {
+    ThreadTimingOff();
+    ~ThreadTimingOff();
+};
+
 }  // namespace tdg

@@ -48,8 +48,12 @@ static std::atomic<unsigned long long> g_launches{0};
 static std::atomic<int> g_timing{0};
 static std::atomic<float> g_main_ms{0.f}, g_build_ms{0.f};
 
+static thread_local int t_timing_off = 0;
+ThreadTimingOff::ThreadTimingOff() { t_timing_off++; }
+ThreadTimingOff::~ThreadTimingOff() { t_timing_off--; }
+
 void note_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memory_order_relaxed); }
-bool timing_on() { return g_timing.load(std::memory_order_relaxed) != 0; }
+bool timing_on() { return g_timing.load(std::memory_order_relaxed) != 0 && t_timing_off == 0; }
 void set_last_main_ms(float ms) { g_main_ms.store(ms); }
 void set_last_build_ms(float ms) { g_build_ms.store(ms); }
 
