@@ -151,6 +151,155 @@ def stats_of(td):
     return s
 
 
+# ---- batched group-by (4096 independent queries) ---------------------------------------
+
+class Batch:
+    """4096 group-by queries (SUM/COUNT/MAX of val by key), one table each:
+    rows log-uniform in [1K, 2M], key U[0, K) with K log-uniform in [16, 65536],
+    val U[0, 1).  Graphs are built once and executed repeatedly (prepared
+    queries); columns are written straight into td vectors."""
+
+    def __init__(self, td, n_queries=4096, seed=4, first=None):
+        import ctypes as C
+        import numpy as np
+        from teide_b200 import workloads
+        from teide_b200.td import F64, I64, OP_COUNT, OP_MAX, OP_SUM
+        self.td = td
+        rows, ks = workloads.config4_shapes(n_queries=n_queries, seed=seed)
+        if first:
+            rows, ks = rows[:first], ks[:first]
+        self.rows = int(rows.sum())
+        self.n = len(rows)
+        self.tables, self.graphs, self.roots = [], [], []
+        for i, (n, k) in enumerate(zip(rows, ks)):
+            r = np.random.default_rng(seed * 100_000 + i)
+            kv, kview = td.vec_alloc(I64, int(n))
+            vv, vview = td.vec_alloc(F64, int(n))
+            kview[:] = r.integers(0, int(k), int(n), dtype=np.int64)
+            r.random(out=vview)
+            t = td.table({"key": kv, "val": vv})
+            td.release(kv)
+            td.release(vv)
+            g = td.graph(t)
+            self.roots.append(g.group([g.scan("key")], [OP_SUM, OP_COUNT, OP_MAX], [g.scan("val")] * 3))
+            self.tables.append(t)
+            self.graphs.append(g)
+        self.G = (C.c_void_p * self.n)(*[g.g for g in self.graphs])
+        self.R = (C.c_void_p * self.n)(*self.roots)
+        if hasattr(td.lib, "td_execute_batch"):       # Teide itself has no batch entry
+            td.lib.td_execute_batch.restype = C.c_void_p
+            td.lib.td_execute_batch.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+
+    def batched(self):
+        r = self.td.check(self.td.lib.td_execute_batch(self.G, self.R, self.n), "td_execute_batch")
+        self.td.release(r)
+
+    def plain(self):
+        """One td_execute per query (one query per launch sequence)."""
+        for g, root in zip(self.graphs, self.roots):
+            self.td.release(g.execute(root, optimize=False))
+
+
+def batch_main(args, td, L, rank, world, local, barrier, max_over_ranks):
+    import torch
+    b = Batch(td, seed=4 + 1000 * rank)
+    for t in b.tables:
+        st = L.td_gpu_pin(t)
+        if st:
+            raise RuntimeError(f"td_gpu_pin failed: {st}")
+    L.tdg_set_timing(0)
+    b.batched()                                 # autotune (or load the tuned shape) + graph capture
+    clk = Clocks(local).__enter__()
+    for _ in range(args.warmup):
+        b.batched()
+    barrier()
+    l0 = L.tdg_launch_count()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    tc0 = time.monotonic()
+    ev0.record()
+    for _ in range(args.steps):
+        b.batched()
+    ev1.record()
+    torch.cuda.synchronize()
+    tc1 = time.monotonic()
+    launches = L.tdg_launch_count() - l0
+    elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    value = b.n * world * args.steps / elapsed
+    # aggregation kernel alone (direct launches with CUDA events, no graph)
+    L.tdg_set_timing(1)
+    main_ms = []
+    for _ in range(max(3, args.steps)):
+        b.batched()
+        main_ms.append(L.tdg_last_main_ms())
+    L.tdg_set_timing(0)
+    # plain: the same queries, one td_execute each
+    b.plain()
+    barrier()
+    plain_steps = 2
+    ev0.record()
+    for _ in range(plain_steps):
+        b.plain()
+    ev1.record()
+    torch.cuda.synchronize()
+    time.sleep(0.3)
+    clk.__exit__(None, None, None)
+    plain_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    plain_value = b.n * world * plain_steps / plain_elapsed
+    # end to end: host tables, every step uploads every query's columns
+    for t in b.tables:
+        L.td_gpu_unpin(t)
+    L.td_gpu_trim()
+    b.batched()
+    barrier()
+    e2e_steps = args.e2e_steps or 2
+    ev0.record()
+    for _ in range(e2e_steps):
+        b.batched()
+    ev1.record()
+    torch.cuda.synchronize()
+    e2e_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+    s_e2e = stats_of(td)
+    hbm, peak_kind = peaks()
+    mean_main = statistics.median(main_ms)
+    alg = 16 * b.rows
+    achieved = alg / (mean_main / 1e3) / 1e9 if mean_main > 0 else None
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+        "config": {"workload": "batch", "queries_per_step": b.n, "rows_per_step": b.rows,
+                   "algorithmic_bytes_per_step": alg, "aggs": "SUM/COUNT/MAX(val) by key",
+                   "l2": "inputs larger than L2 (no flush)", "tables": "resident in HBM (td_gpu_pin)",
+                   "launch": "td_execute_batch: one persistent kernel, replayed CUDA graph",
+                   "parallelism": f"replicas{world}"},
+        "plain": {"value": plain_value, "unit": "queries/s", "steps": plain_steps,
+                  "how": "one td_execute per query, same resident tables", "speedup": value / plain_value},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": (achieved / hbm) if achieved else None,
+                     "traffic": profile_traffic("batch_group_cfg4.md"), "kernel": "k_batch_agg",
+                     "bytes_per_launch": alg, "mean_launch_ms": mean_main, "peak_source": peak_kind},
+        "e2e": {"value": b.n * world * e2e_steps / e2e_elapsed, "unit": "queries/s",
+                "h2d_bytes_per_step": int(s_e2e.h2d), "d2h_bytes_per_step": int(s_e2e.d2h), "steps": e2e_steps},
+        "gpu_launches": int(launches),
+        "clocks": clk.summary(tc0, tc1),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
+        rtd, q, desc = reference_sample("batch", 0)
+        q()
+        t0 = time.perf_counter()
+        n = 0
+        while n < 2 or time.perf_counter() - t0 < 10:
+            q()
+            n += 1
+        dt = (time.perf_counter() - t0) / n
+        line["cpu_baseline"] = {"value": BATCH_REF_QUERIES / dt, "unit": "queries/s", "cores": os.cpu_count(),
+                                "kind": "reference", "sample": desc + f", mean of {n} runs"}
+    return line
+
+
+BATCH_REF_QUERIES = 512
+
+
 # ---- CPU reference ---------------------------------------------------------------------
 
 def reference_sample(workload, scale_rows):
@@ -160,6 +309,10 @@ def reference_sample(workload, scale_rows):
     from teide_b200 import workloads
     from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM, Td
     td = Td(REF_LIB)
+    if workload == "batch":
+        b = Batch(td, first=BATCH_REF_QUERIES)
+        desc = (f"the first {b.n} of the 4096 queries ({b.rows / 1e6:.1f}M rows), one td_execute each")
+        return td, b.plain, desc
     if workload == "join_group":
         b, p = workloads.config3(n_build=10_000_000, n_probe=scale_rows, seed=33)
         bt, pt = td.table(b), td.table(p)
@@ -192,7 +345,8 @@ def reference_arm(args):
     if not os.path.exists(REF_LIB):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libteide_ref.so not built"}))
         return
-    rows = {"join_group": 10_000_000, "group_radix": 20_000_000, "readme_group": 10_000_000}[args.workload]
+    rows = {"join_group": 10_000_000, "group_radix": 20_000_000, "readme_group": 10_000_000,
+            "batch": BATCH_REF_QUERIES}[args.workload]
     td, q, desc = reference_sample(args.workload, rows)
     for _ in range(args.warmup):
         q()
@@ -201,14 +355,15 @@ def reference_arm(args):
         q()
     dt = (time.perf_counter() - t0) / args.steps
     v = rows / dt
+    unit = "queries/s" if args.workload == "batch" else "rows/s"
     cores = os.cpu_count()
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": v, "unit": "rows/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": unit, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
         "config": {"workload": args.workload, "sample": desc},
-        "cpu_baseline": {"value": v, "unit": "rows/s", "cores": cores, "kind": "reference", "sample": desc},
-        "e2e": {"value": v, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": v, "unit": unit, "cores": cores, "kind": "reference", "sample": desc},
+        "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
 
@@ -220,7 +375,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="teide_b200", choices=["teide_b200", "reference"])
-    ap.add_argument("--workload", default="join_group", choices=["join_group", "group_radix", "readme_group"])
+    ap.add_argument("--workload", default="join_group", choices=["join_group", "group_radix", "readme_group", "batch"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -250,9 +405,6 @@ def main():
     L.td_gpu_unpin.argtypes = [__import__("ctypes").c_void_p]
     L.tdg_set_timing(1)
 
-    tabs, rows, alg_bytes, main_bytes = make_tables(td, args.workload, rank, "cuda")
-    torch.cuda.empty_cache()
-
     def barrier():
         if dist:
             dist.barrier()
@@ -264,6 +416,18 @@ def main():
         t = torch.tensor([x], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.workload == "batch":
+        line = batch_main(args, td, L, rank, world, local, barrier, max_over_ranks)
+        if rank == 0:
+            print(json.dumps(line))
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    tabs, rows, alg_bytes, main_bytes = make_tables(td, args.workload, rank, "cuda")
+    torch.cuda.empty_cache()
 
     # ---- resident: tables pinned in HBM ----
     for t in tabs.values():

@@ -254,6 +254,61 @@ tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_plan* jplan
                               const tdg_group_desc* g, const tdg_group_plan* gplan, void* gws,
                               const tdg_group_out* out, void* stream);
 
+/* ---- batched group-by ------------------------------------------------------------
+ * Many independent group-bys of one shape -- one integer key column with a
+ * known range, aggregates over one value column -- run as ONE persistent
+ * kernel that pulls (query, tile) work items from a queue, so thousands of
+ * small or uneven queries cost one launch instead of thousands.  No
+ * counterpart in Teide's CPU engine (each query there is its own
+ * exec_group call, exec.c:5542).
+ *
+ * tdg_batch_prepare uploads the work description into ws (it synchronizes);
+ * tdg_batch_run is asynchronous, allocates nothing and never synchronizes,
+ * so a caller can capture it in a CUDA graph once and replay it.
+ * Output: rows grouped by query (query order), keys ascending within a
+ * query; columns query index, key, one 8-byte column per aggregate. */
+typedef struct tdg_batch_query {
+    tdg_col key;           /* integer key column */
+    tdg_col val;           /* value column the aggregates read */
+    int64_t nrows;
+    int64_t key_min;       /* every key k satisfies key_min <= k < key_min + n_slots */
+    int64_t n_slots;
+} tdg_batch_query;
+
+typedef struct tdg_batch_desc {
+    int32_t n_queries;
+    int32_t n_aggs;        /* OP_SUM, OP_COUNT, OP_MIN, OP_MAX, OP_AVG over val */
+    int32_t agg_ops[TDG_MAX_AGGS];
+    const tdg_batch_query* queries;   /* host array of n_queries */
+} tdg_batch_desc;
+
+typedef struct tdg_batch_plan {
+    int64_t tile_rows;     /* rows per work item (autotuned) */
+    int32_t ctas_per_sm;   /* persistent CTAs per SM (autotuned) */
+    int32_t smem_slots;    /* queries with at most this many slots aggregate in shared memory */
+    int64_t n_items;
+    int64_t total_slots;   /* capacity each output column needs */
+    size_t  ws_bytes;
+    int32_t n_queries;
+    int32_t n_aggs;
+    int32_t agg_ops[TDG_MAX_AGGS];
+    int32_t val_f64;       /* the value columns are F64 (all queries alike) */
+    int32_t words;         /* 8-byte words per slot record */
+} tdg_batch_plan;
+
+typedef struct tdg_batch_out {
+    int64_t* query;                /* total_slots rows */
+    int64_t* key;
+    void*    aggs[TDG_MAX_AGGS];   /* 8-byte values (I64, or F64 when the value column is F64 / AVG) */
+    int64_t* d_n_rows;             /* one int64: rows written */
+} tdg_batch_out;
+
+/* tile_rows / ctas_per_sm of 0 pick defaults. */
+tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_rows, int32_t ctas_per_sm,
+                               tdg_batch_plan* plan);
+tdg_status tdg_batch_prepare(const tdg_batch_desc* d, const tdg_batch_plan* plan, void* ws, void* stream);
+tdg_status tdg_batch_run(const tdg_batch_plan* plan, void* ws, const tdg_batch_out* out, void* stream);
+
 /* Device properties used by the planners (SM count, shared memory). */
 int32_t tdg_device_sm_count(void);
 
@@ -262,8 +317,11 @@ int32_t tdg_device_sm_count(void);
  * around its main streaming kernel (the fused select [+ probe] + aggregate
  * launch) on the stream it was given, and tdg_join_build around its build
  * kernel; the last durations are read back here in milliseconds.  Timing
- * adds no synchronization beyond the one each call already does. */
+ * adds no synchronization beyond the one each call already does, except in
+ * tdg_batch_run, which waits for its aggregation kernel's end event (and
+ * records nothing while its stream is being captured into a CUDA graph). */
 void     tdg_set_timing(int32_t on);
+int32_t  tdg_timing_enabled(void);
 float    tdg_last_main_ms(void);
 float    tdg_last_build_ms(void);
 /* Kernels launched by this library since the process started. */

@@ -47,6 +47,20 @@ void     td_gpu_last_stats(td_gpu_stats_t* out);
 /* Release cached device memory that no resident table uses. */
 void     td_gpu_trim(void);
 
+/* Run n group-by graphs as one batched GPU launch.  Each graph is a
+ * td_group over its bound table with one integer key (td_scan) and
+ * aggregates reading one value column (td_scan; COUNT may read anything),
+ * with the same aggregate list and column types in every graph, and keys
+ * dense enough for direct indexing (key range at most max(2^20, 4 x rows));
+ * anything else returns TD_ERR_NYI (TD_ERR_TYPE for mixed column types).  The result is ONE table: "_query" (index into graphs), the key
+ * column, then one column per aggregate (named as td_group names them), rows
+ * grouped by query in argument order with keys ascending.  A repeated batch
+ * (same tables, same key ranges) replays a cached CUDA graph; its tile size
+ * and CTA count come from an autotuner whose choices persist in a JSON file
+ * ($TD_TUNE_CACHE, else ~/.cache/teide_b200_tune.json). */
+td_t*    td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n);
+void     td_gpu_batch_cache_clear(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,420 @@
+// Batched group-by: many independent queries in one persistent launch.
+//
+// Teide runs each group-by as its own exec_group call (exec.c:5542-6879),
+// with its own thread-pool dispatches.  For thousands of small or uneven
+// queries the per-query launch and synchronization cost dominates on a GPU,
+// so here all queries of one shape share one launch:
+//
+//   work items   each query is cut into tiles of tile_rows rows; a CTA takes
+//                the next item from a global counter (atomicAdd), so long and
+//                short queries balance across the 148 SMs;
+//   accumulate   a query with at most smem_slots slots (and a tile at least
+//                twice that long) aggregates its tile in shared memory and
+//                merges once; other tiles update the query's slot records in
+//                global memory (L2-resident per query);
+//   emit         one CTA per query writes its non-empty slots, keys ascending,
+//                at the query's offset from an exclusive scan of group counts.
+//
+// tdg_batch_run issues only kernels and memsets on the given stream (no
+// allocation, no host synchronization), so the host can capture it once in
+// a CUDA graph and replay it; tdg_batch_prepare writes the work description
+// (per-query descriptors and the item -> query map) into the workspace.
+#include "tdg_common.cuh"
+#include <string.h>
+#include <vector>
+
+namespace tdg {
+
+constexpr int kBatchThreads = 256;
+constexpr int64_t kDefaultTile = 16384;
+constexpr int kDefaultSmemSlots = 2048;
+constexpr int kEmitBlock = 256;
+constexpr int64_t kMaxDenseSlots = 1 << 20;
+
+enum : int32_t { BK_COUNT = 0, BK_SUM_I, BK_SUM_F, BK_MIN_I, BK_MAX_I, BK_MIN_F, BK_MAX_F };
+
+struct BQ {
+    tdg_col key, val;
+    int64_t nrows, key_min, n_slots, acc_off, first_item;
+};
+
+struct BatchK {
+    const BQ* q;
+    const int32_t* item_q;
+    int64_t n_items, tile_rows, total_slots;
+    unsigned long long* rec;
+    unsigned long long* counter;
+    int32_t* err;
+    int64_t* qcount;
+    int64_t* qoff;
+    int32_t n_queries, W, na, smem_slots;
+    int32_t kind[TDG_MAX_AGGS];
+    int32_t ai[TDG_MAX_AGGS];
+    int32_t op[TDG_MAX_AGGS];
+    unsigned long long finit[TDG_MAX_AGGS + 2];
+};
+
+struct BLayout { size_t hdr, q, item_q, qcount, qoff, rec, total; };
+
+static size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
+
+static BLayout blayout(int64_t n_queries, int64_t n_items, int64_t total_slots, int W) {
+    BLayout L;
+    size_t o = 0;
+    L.hdr = o; o += 256;
+    L.q = o; o += al((size_t)n_queries * sizeof(BQ));
+    L.item_q = o; o += al((size_t)n_items * 4);
+    L.qcount = o; o += al((size_t)n_queries * 8);
+    L.qoff = o; o += al((size_t)(n_queries + 1) * 8);
+    L.rec = o; o += al((size_t)total_slots * 8 * W);
+    L.total = o;
+    return L;
+}
+
+__host__ __device__ inline unsigned long long binit(int kind) {
+    return (kind == BK_MIN_I || kind == BK_MIN_F) ? (unsigned long long)INT64_MAX
+         : (kind == BK_MAX_I || kind == BK_MAX_F) ? (unsigned long long)INT64_MIN : 0ULL;
+}
+
+static BatchK make_bk(const tdg_batch_plan* p, void* ws) {
+    BatchK B;
+    memset(&B, 0, sizeof(B));
+    const BLayout L = blayout(p->n_queries, p->n_items, p->total_slots, p->words);
+    char* w = (char*)ws;
+    B.counter = (unsigned long long*)(w + L.hdr);
+    B.err = (int32_t*)(w + L.hdr + 16);
+    B.q = (const BQ*)(w + L.q);
+    B.item_q = (const int32_t*)(w + L.item_q);
+    B.qcount = (int64_t*)(w + L.qcount);
+    B.qoff = (int64_t*)(w + L.qoff);
+    B.rec = (unsigned long long*)(w + L.rec);
+    B.n_items = p->n_items;
+    B.tile_rows = p->tile_rows;
+    B.total_slots = p->total_slots;
+    B.n_queries = p->n_queries;
+    B.W = p->words;
+    B.na = p->n_aggs;
+    B.smem_slots = p->smem_slots;
+    int ai = 0;
+    for (int a = 0; a < p->n_aggs; a++) {
+        const int op = p->agg_ops[a], f = p->val_f64;
+        B.op[a] = op;
+        B.kind[a] = op == A_COUNT ? BK_COUNT : op == A_MIN ? (f ? BK_MIN_F : BK_MIN_I)
+                  : op == A_MAX ? (f ? BK_MAX_F : BK_MAX_I) : (f ? BK_SUM_F : BK_SUM_I);
+        B.ai[a] = op == A_COUNT ? -1 : ai++;
+        if (B.ai[a] >= 0) B.finit[1 + B.ai[a]] = binit(B.kind[a]);
+    }
+    return B;
+}
+
+__global__ void k_batch_init(const BatchK B) {
+    const int lane = threadIdx.x & 31;
+    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const int W = B.W;
+    const int step = 32 % W;
+    const int64_t nchunks = (B.total_slots + 31) >> 5;
+    for (int64_t ch = warp; ch < nchunks; ch += nwarps) {
+        const int64_t recs = B.total_slots - ch * 32 < 32 ? B.total_slots - ch * 32 : 32;
+        const int words = (int)(recs * W);
+        unsigned long long* base = B.rec + ch * 32 * W;
+        int f = lane % W;
+        for (int j = lane; j < words; j += 32) {
+            base[j] = B.finit[f];
+            f += step;
+            if (f >= W) f -= W;
+        }
+    }
+}
+
+__device__ __forceinline__ void bupd(unsigned long long* a, int kind, int64_t iv, double fv, bool global) {
+    switch (kind) {
+        case BK_SUM_I: atomicAdd(a, (unsigned long long)iv); break;
+        case BK_SUM_F: atomicAdd((double*)a, fv); break;
+        case BK_MIN_I:
+            if (!global || iv < *(volatile long long*)a) atomicMin((long long*)a, (long long)iv);
+            break;
+        case BK_MAX_I:
+            if (!global || iv > *(volatile long long*)a) atomicMax((long long*)a, (long long)iv);
+            break;
+        case BK_MIN_F:
+            if (fv == fv) {
+                const long long o = f2ord(fv);
+                if (!global || o < *(volatile long long*)a) atomicMin((long long*)a, o);
+            }
+            break;
+        case BK_MAX_F:
+            if (fv == fv) {
+                const long long o = f2ord(fv);
+                if (!global || o > *(volatile long long*)a) atomicMax((long long*)a, o);
+            }
+            break;
+        default: break;
+    }
+}
+
+__device__ __forceinline__ void bmerge(unsigned long long* a, int kind, unsigned long long v) {
+    switch (kind) {
+        case BK_SUM_I: atomicAdd(a, v); break;
+        case BK_SUM_F: atomicAdd((double*)a, __longlong_as_double((long long)v)); break;
+        case BK_MIN_I: case BK_MIN_F: if ((long long)v != INT64_MAX) atomicMin((long long*)a, (long long)v); break;
+        case BK_MAX_I: case BK_MAX_F: if ((long long)v != INT64_MIN) atomicMax((long long*)a, (long long)v); break;
+        default: break;
+    }
+}
+
+// The persistent kernel: CTAs pull (query, tile) items until the queue drains.
+__global__ void __launch_bounds__(kBatchThreads) k_batch_agg(const BatchK B) {
+    extern __shared__ unsigned long long sm[];
+    __shared__ long long s_item;
+    uint32_t* scnt = (uint32_t*)sm;
+    unsigned long long* sacc = sm + ((B.smem_slots * 4 + 7) >> 3);
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = (long long)atomicAdd(B.counter, 1ULL);
+        __syncthreads();
+        const int64_t item = s_item;
+        if (item >= B.n_items) break;
+        const int q = B.item_q[item];
+        const BQ Q = B.q[q];
+        const int64_t r0 = (item - Q.first_item) * B.tile_rows;
+        const int64_t r1 = r0 + B.tile_rows < Q.nrows ? r0 + B.tile_rows : Q.nrows;
+        const bool use_smem = Q.n_slots <= B.smem_slots && (r1 - r0) >= 2 * Q.n_slots;
+        const int64_t S = Q.n_slots;
+        if (use_smem) {
+            for (int64_t s = threadIdx.x; s < S; s += blockDim.x) scnt[s] = 0;
+            for (int a = 0; a < B.na; a++)
+                if (B.ai[a] >= 0)
+                    for (int64_t s = threadIdx.x; s < S; s += blockDim.x) sacc[B.ai[a] * S + s] = B.finit[1 + B.ai[a]];
+            __syncthreads();
+        }
+        for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
+            const int64_t k = ld_i(Q.key, r) - Q.key_min;
+            if (k < 0 || k >= S) { atomicCAS(B.err, 0, E_DOMAIN); continue; }
+            const bool vf = Q.val.type == T_F64;
+            const double fv = vf ? ld_f(Q.val, r) : 0.0;
+            const int64_t iv = vf ? 0 : ld_i(Q.val, r);
+            if (use_smem) {
+                atomicAdd(&scnt[k], 1u);
+                for (int a = 0; a < B.na; a++)
+                    if (B.ai[a] >= 0) bupd(&sacc[B.ai[a] * S + k], B.kind[a], iv, fv, false);
+            } else {
+                unsigned long long* rec = B.rec + (Q.acc_off + k) * B.W;
+                atomicAdd(rec, 1ULL);
+                for (int a = 0; a < B.na; a++)
+                    if (B.ai[a] >= 0) bupd(rec + 1 + B.ai[a], B.kind[a], iv, fv, true);
+            }
+        }
+        if (use_smem) {
+            __syncthreads();
+            for (int64_t s = threadIdx.x; s < S; s += blockDim.x) {
+                const uint32_t c = scnt[s];
+                if (!c) continue;
+                unsigned long long* rec = B.rec + (Q.acc_off + s) * B.W;
+                atomicAdd(rec, (unsigned long long)c);
+                for (int a = 0; a < B.na; a++)
+                    if (B.ai[a] >= 0) bmerge(rec + 1 + B.ai[a], B.kind[a], sacc[B.ai[a] * S + s]);
+            }
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kEmitBlock) k_batch_count(const BatchK B) {
+    __shared__ int red[32];
+    const BQ Q = B.q[blockIdx.x];
+    int c = 0;
+    for (int64_t s = threadIdx.x; s < Q.n_slots; s += blockDim.x) c += B.rec[(Q.acc_off + s) * B.W] != 0;
+    int tot;
+    block_excl_scan(c, &tot, red);
+    if (threadIdx.x == 0) B.qcount[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(1024) k_batch_scan(const BatchK B, int64_t* d_total) {
+    __shared__ long long part[1024];
+    const int64_t m = B.n_queries;
+    const int64_t per = (m + blockDim.x - 1) / blockDim.x;
+    const int64_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
+    long long sum = 0;
+    for (int64_t i = b; i < e; i++) sum += B.qcount[i];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        long long v = threadIdx.x >= (unsigned)o ? part[threadIdx.x - o] : 0;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    long long run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    for (int64_t i = b; i < e; i++) { B.qoff[i] = run; run += B.qcount[i]; }
+    if (threadIdx.x == blockDim.x - 1) {
+        B.qoff[m] = part[blockDim.x - 1];
+        // a key outside its query's [key_min, key_min + n_slots) range is
+        // reported as a negative row count (the host maps it to an error)
+        *d_total = *(volatile int32_t*)B.err ? -1 : part[blockDim.x - 1];
+    }
+}
+
+struct BOut {
+    int64_t* query;
+    int64_t* key;
+    void* aggs[TDG_MAX_AGGS];
+};
+
+__global__ void __launch_bounds__(kEmitBlock) k_batch_emit(const BatchK B, const BOut O) {
+    __shared__ int red[32];
+    const int q = blockIdx.x;
+    const BQ Q = B.q[q];
+    int64_t out = B.qoff[q];
+    for (int64_t s0 = 0; s0 < Q.n_slots; s0 += blockDim.x) {
+        const int64_t s = s0 + threadIdx.x;
+        const unsigned long long* rec = s < Q.n_slots ? B.rec + (Q.acc_off + s) * B.W : nullptr;
+        const unsigned long long c = rec ? rec[0] : 0;
+        int tot;
+        const int pre = block_excl_scan(c ? 1 : 0, &tot, red);
+        if (c) {
+            const int64_t o = out + pre;
+            O.query[o] = q;
+            O.key[o] = Q.key_min + s;
+            for (int a = 0; a < B.na; a++) {
+                const int kind = B.kind[a];
+                uint64_t r;
+                if (kind == BK_COUNT) {
+                    r = c;
+                } else {
+                    const unsigned long long v = rec[1 + B.ai[a]];
+                    if (B.op[a] == A_AVG) {
+                        const double sum = kind == BK_SUM_F ? __longlong_as_double((long long)v) : (double)(long long)v;
+                        r = (uint64_t)__double_as_longlong(sum / (double)c);
+                    } else if (kind == BK_MIN_F || kind == BK_MAX_F) {
+                        r = (uint64_t)__double_as_longlong(ord2f((long long)v));
+                    } else {
+                        r = v;
+                    }
+                }
+                ((uint64_t*)O.aggs[a])[o] = r;
+            }
+        }
+        out += tot;
+    }
+}
+
+}  // namespace tdg
+
+using namespace tdg;
+
+extern "C" tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_rows, int32_t ctas_per_sm,
+                                          tdg_batch_plan* p) {
+    if (!d || !p || (d->n_queries > 0 && !d->queries)) return E_TYPE;
+    if (d->n_aggs < 1 || d->n_aggs > TDG_MAX_AGGS || d->n_queries < 0) return E_NYI;
+    memset(p, 0, sizeof(*p));
+    p->tile_rows = tile_rows > 0 ? tile_rows : kDefaultTile;
+    p->ctas_per_sm = ctas_per_sm > 0 ? ctas_per_sm : 0;
+    p->smem_slots = kDefaultSmemSlots;
+    p->n_queries = d->n_queries;
+    p->n_aggs = d->n_aggs;
+    int n_acc = 0;
+    for (int a = 0; a < d->n_aggs; a++) {
+        const int op = d->agg_ops[a];
+        if (op != A_SUM && op != A_COUNT && op != A_MIN && op != A_MAX && op != A_AVG) return E_NYI;
+        p->agg_ops[a] = op;
+        n_acc += op != A_COUNT;
+    }
+    p->words = 1 + n_acc == 3 ? 4 : 1 + n_acc;
+    // shared accumulators: 32-bit counts + n_acc 8-byte values per slot in 48 KB
+    const int fit = (int)((48 * 1024 - 8) / (4 + 8 * (size_t)n_acc));
+    p->smem_slots = fit < kDefaultSmemSlots ? fit : kDefaultSmemSlots;
+    p->val_f64 = d->n_queries > 0 && d->queries[0].val.type == T_F64;
+    for (int i = 0; i < d->n_queries; i++) {
+        const tdg_batch_query& q = d->queries[i];
+        if (!is_int_class(q.key.type) || !elem_size(q.val.type, q.val.attrs)) return E_TYPE;
+        if ((q.val.type == T_F64) != (p->val_f64 != 0)) return E_TYPE;
+        if (q.n_slots < 1 || q.nrows < 0) return E_RANGE;
+        // direct-indexed records only: a key range far wider than the query
+        // (sparse keys) belongs to the hash-table group-by, not the batch
+        if (q.n_slots > kMaxDenseSlots && q.n_slots > 4 * q.nrows) return E_NYI;
+        p->n_items += (q.nrows + p->tile_rows - 1) / p->tile_rows;
+        p->total_slots += q.n_slots;
+    }
+    if (p->n_items > INT32_MAX) return E_RANGE;
+    p->ws_bytes = blayout(p->n_queries, p->n_items, p->total_slots, p->words).total;
+    return E_OK;
+}
+
+extern "C" tdg_status tdg_batch_prepare(const tdg_batch_desc* d, const tdg_batch_plan* p, void* ws, void* stream) {
+    if (!d || !p || !ws) return E_TYPE;
+    const BLayout L = blayout(p->n_queries, p->n_items, p->total_slots, p->words);
+    std::vector<BQ> qs((size_t)p->n_queries);
+    std::vector<int32_t> item_q((size_t)p->n_items);
+    int64_t acc = 0, item = 0;
+    for (int i = 0; i < p->n_queries; i++) {
+        const tdg_batch_query& q = d->queries[i];
+        BQ& b = qs[i];
+        b.key = q.key; b.val = q.val;
+        b.nrows = q.nrows; b.key_min = q.key_min; b.n_slots = q.n_slots;
+        b.acc_off = acc;
+        b.first_item = item;
+        const int64_t tiles = (q.nrows + p->tile_rows - 1) / p->tile_rows;
+        for (int64_t t = 0; t < tiles; t++) item_q[(size_t)(item + t)] = i;
+        item += tiles;
+        acc += q.n_slots;
+    }
+    if (item != p->n_items || acc != p->total_slots) return E_RANGE;
+    cudaStream_t s = (cudaStream_t)stream;
+    char* w = (char*)ws;
+    if (cudaMemsetAsync(w + L.hdr, 0, 256, s) != cudaSuccess ||
+        (p->n_queries && cudaMemcpyAsync(w + L.q, qs.data(), qs.size() * sizeof(BQ), cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+        (p->n_items && cudaMemcpyAsync(w + L.item_q, item_q.data(), item_q.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        return E_IO;
+    }
+    return E_OK;
+}
+
+extern "C" tdg_status tdg_batch_run(const tdg_batch_plan* p, void* ws, const tdg_batch_out* out, void* stream) {
+    if (!p || !ws || !out) return E_TYPE;
+    cudaStream_t s = (cudaStream_t)stream;
+    BatchK B = make_bk(p, ws);
+    cudaMemsetAsync(B.counter, 0, 256, s);   // work counter and error word
+    if (p->total_slots > 0) {
+        const int g = grid_for((const void*)k_batch_init, kThreads, 0, (p->total_slots * p->words + 31) / 32 * 32);
+        (note_launch(), k_batch_init<<<g, kThreads, 0, s>>>(B));
+    }
+    int n_acc = 0;
+    for (int a = 0; a < p->n_aggs; a++) n_acc += p->agg_ops[a] != A_COUNT;
+    const size_t smem = (((size_t)p->smem_slots * 4 + 7) & ~(size_t)7) + (size_t)p->smem_slots * 8 * n_acc;
+    if (p->n_items > 0) {
+        int per_sm = p->ctas_per_sm;
+        if (per_sm <= 0) {
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_batch_agg, kBatchThreads, smem) != cudaSuccess || per_sm < 1)
+                per_sm = 1;
+        }
+        int64_t g = (int64_t)per_sm * sm_count();
+        if (g > p->n_items) g = p->n_items;
+        // instrumentation: time the aggregation kernel, never inside a capture
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusActive;
+        EventTimer t;
+        const bool timed = cs == cudaStreamCaptureStatusNone && timing_on();
+        if (timed) t.start(s);
+        (note_launch(), k_batch_agg<<<(unsigned)g, kBatchThreads, smem, s>>>(B));
+        if (timed) {
+            t.stop(s);
+            cudaEventSynchronize(t.b);
+            set_last_main_ms(t.ms());
+        }
+    }
+    BOut O;
+    memset(&O, 0, sizeof(O));
+    O.query = out->query;
+    O.key = out->key;
+    for (int a = 0; a < p->n_aggs; a++) O.aggs[a] = out->aggs[a];
+    if (p->n_queries > 0) {
+        (note_launch(), k_batch_count<<<(unsigned)p->n_queries, kEmitBlock, 0, s>>>(B));
+        (note_launch(), k_batch_scan<<<1, 1024, 0, s>>>(B, out->d_n_rows));
+        (note_launch(), k_batch_emit<<<(unsigned)p->n_queries, kEmitBlock, 0, s>>>(B, O));
+    } else {
+        cudaMemsetAsync(out->d_n_rows, 0, 8, s);
+    }
+    return launch_status();
+}

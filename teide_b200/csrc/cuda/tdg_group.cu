@@ -465,9 +465,9 @@ __global__ void __launch_bounds__(kThreads) k_select_hot(const GroupK G) {
 // is a direct array whose aggregate inputs all come from the probe side, the
 // build pass stores in map[key - kmin] the build row's share of the group
 // slot (sum over build-side group keys of (key - min) * stride), or EMPTY.
-// The probe then needs one small random read per row -- a 2-byte entry when
-// the slots fit in 16 bits, so a 10M-row build side is a 20 MB map that stays
-// in L2 -- instead of the head[] lookup plus the build-column gather.
+// The probe then needs one 4-byte random read per row -- a 10M-row build side
+// is a 40 MB map that stays in L2 -- instead of the head[] lookup plus the
+// build-column gather.
 template <typename PT> struct Empty;
 template <> struct Empty<uint16_t> { static constexpr uint16_t v = 0xFFFF; };
 template <> struct Empty<uint32_t> { static constexpr uint32_t v = 0xFFFFFFFFu; };
@@ -933,19 +933,17 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     G.hot_cap = 0;
     tdg_status st = prepare(G, s);
     if (st) return st;
-    const bool narrow = p->n_slots < 0xFFFF;
+    // 32-bit entries: the build's atomicCAS is native (a 16-bit CAS is a loop
+    // on the containing word), and 4 bytes per key still keeps a 10M-row
+    // build side's map (40 MB) in L2.
+    const bool narrow = false;
     void* map = J->head;
     cudaMemsetAsync(map, 0xFF, (size_t)J->n_slots * (narrow ? 2 : 4), s);
     EventTimer tb;
     tb.start(s);
     if (n_right > 0) {
-        if (narrow) {
-            const int g = grid_for((const void*)k_payload_build<uint16_t>, kThreads, 0, n_right);
-            (note_launch(), k_payload_build<uint16_t><<<g, kThreads, 0, s>>>(G, *J, (uint16_t*)map, n_right, G.err + 1));
-        } else {
-            const int g = grid_for((const void*)k_payload_build<uint32_t>, kThreads, 0, n_right);
-            (note_launch(), k_payload_build<uint32_t><<<g, kThreads, 0, s>>>(G, *J, (uint32_t*)map, n_right, G.err + 1));
-        }
+        const int g = grid_for((const void*)k_payload_build<uint32_t>, kThreads, 0, n_right);
+        (note_launch(), k_payload_build<uint32_t><<<g, kThreads, 0, s>>>(G, *J, (uint32_t*)map, n_right, G.err + 1));
     }
     tb.stop(s);
     int32_t flags[2] = {0, 0};
@@ -974,15 +972,10 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
         (note_launch(), k_payload_probe<PKV, SMV, PT, W><<<g, kThreads, smem, s>>>(                      \
             G, P, prog, J->lkeys[0], J->kmin, J->n_slots, (const PT*)map, n_left));                      \
     }
-    TDG_PL(0, true, uint16_t, true) TDG_PL(0, false, uint16_t, true)
     TDG_PL(0, true, uint32_t, true) TDG_PL(0, false, uint32_t, true)
-    TDG_PL(1, true, uint16_t, true) TDG_PL(1, false, uint16_t, true)
     TDG_PL(1, true, uint32_t, true) TDG_PL(1, false, uint32_t, true)
-    TDG_PL(0, true, uint16_t, false) TDG_PL(0, false, uint16_t, false)
     TDG_PL(0, true, uint32_t, false) TDG_PL(0, false, uint32_t, false)
-    TDG_PL(1, true, uint16_t, false) TDG_PL(1, false, uint16_t, false)
     TDG_PL(1, true, uint32_t, false) TDG_PL(1, false, uint32_t, false)
-    TDG_PL(2, true, uint16_t, false) TDG_PL(2, false, uint16_t, false)
     TDG_PL(2, true, uint32_t, false) TDG_PL(2, false, uint32_t, false)
 #undef TDG_PL
     tm.stop(s);

@@ -1,0 +1,409 @@
+/*
+ * td_execute_batch: many group-by graphs as one batched launch.
+ *
+ * Every graph must be a td_group over its bound table with one integer key
+ * (td_scan) and aggregates that all read one value column (td_scan; COUNT may
+ * read anything), with the same aggregate list in every graph.  The batch is
+ * lowered to the tdg_batch_* kernels: one persistent kernel pulls
+ * (query, tile) work items from a queue (tdg_batch.cu).
+ *
+ * Repeated batches are cheap: the last few batches' device work descriptions,
+ * scratch and an instantiated CUDA graph of tdg_batch_run are cached, keyed
+ * by the exact batch (device column addresses, row counts, key ranges,
+ * aggregate list), so a repeated batch is one cudaGraphLaunch plus the
+ * result copy.  Resident tables (td_gpu_pin) keep those addresses stable.
+ *
+ * Tile size and persistent CTAs per SM come from an autotuner: the first
+ * time a batch of a given shape class runs, a few candidates are timed with
+ * CUDA events and the fastest is stored in a JSON file ($TD_TUNE_CACHE, else
+ * ~/.cache/teide_b200_tune.json) that later processes read.
+ *
+ * Result: one TD_TABLE with "_query" (I64, index of the graph), the key
+ * column (named as the scanned key of the first graph) and one column per
+ * aggregate (named like td_group's output), rows grouped by query in
+ * argument order, keys ascending within a query.
+ */
+#include "internal.h"
+#include <cuda_runtime_api.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <pthread.h>
+#include <string.h>
+#include <sys/stat.h>
+
+#define BATCH_CACHE 4
+
+typedef struct {
+    uint64_t        sig;
+    int64_t         n;
+    tdg_batch_plan  plan;
+    void*           ws;
+    tdg_batch_out   out;
+    void*           bufs[TDG_MAX_AGGS + 3];
+    int             n_bufs;
+    cudaGraphExec_t exec;
+    int             used;       /* LRU stamp */
+} bcache_t;
+
+static bcache_t bcache[BATCH_CACHE];
+static int bstamp;
+static pthread_mutex_t bcache_mu = PTHREAD_MUTEX_INITIALIZER;   /* cache + its graphs */
+
+static uint64_t fnv64(uint64_t h, const void* p, size_t n) {
+    const unsigned char* b = p;
+    for (size_t i = 0; i < n; i++) { h ^= b[i]; h *= 1099511628211ULL; }
+    return h;
+}
+
+static void bcache_drop(bcache_t* e) {
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    tdb_dev_free_persistent(e->ws);
+    for (int i = 0; i < e->n_bufs; i++) tdb_dev_free_persistent(e->bufs[i]);
+    memset(e, 0, sizeof(*e));
+}
+
+/* ---- autotuner persistence ------------------------------------------------------ */
+static void tune_path(char* buf, size_t n) {
+    const char* env = getenv("TD_TUNE_CACHE");
+    if (env && *env) { snprintf(buf, n, "%s", env); return; }
+    const char* home = getenv("HOME");
+    snprintf(buf, n, "%s/.cache/teide_b200_tune.json", home ? home : "/tmp");
+}
+
+/* Shape class of a batch: log2 buckets of query count, mean rows, mean slots. */
+static void tune_key(const tdg_batch_desc* d, char* key, size_t n) {
+    double rows = 0, slots = 0;
+    for (int i = 0; i < d->n_queries; i++) { rows += (double)d->queries[i].nrows; slots += (double)d->queries[i].n_slots; }
+    int q = d->n_queries > 0 ? (int)log2((double)d->n_queries) : 0;
+    int r = d->n_queries > 0 && rows > 0 ? (int)log2(rows / d->n_queries) : 0;
+    int s = d->n_queries > 0 && slots > 0 ? (int)log2(slots / d->n_queries) : 0;
+    snprintf(key, n, "batch:q%d:r%d:s%d:a%d", q, r, s, d->n_aggs);
+}
+
+static int tune_load(const char* key, int64_t* tile, int32_t* ctas) {
+    char path[1024];
+    tune_path(path, sizeof(path));
+    FILE* f = fopen(path, "r");
+    if (!f) return 0;
+    char line[512];
+    int found = 0;
+    while (fgets(line, sizeof(line), f)) {
+        char k[256];
+        long long t;
+        int c;
+        if (sscanf(line, " \"%255[^\"]\": {\"tile_rows\": %lld, \"ctas_per_sm\": %d", k, &t, &c) == 3 &&
+            strcmp(k, key) == 0) {
+            *tile = t;
+            *ctas = c;
+            found = 1;
+        }
+    }
+    fclose(f);
+    return found;
+}
+
+static void tune_store(const char* key, int64_t tile, int32_t ctas) {
+    char path[1024], tmp[1100];
+    tune_path(path, sizeof(path));
+    /* keep other entries: one JSON object, one entry per line */
+    char* lines[256];
+    int n = 0;
+    FILE* f = fopen(path, "r");
+    if (f) {
+        char line[512];
+        while (n < 255 && fgets(line, sizeof(line), f)) {
+            char k[256];
+            if (sscanf(line, " \"%255[^\"]\":", k) == 1 && strcmp(k, key) != 0) {
+                size_t l = strlen(line);
+                while (l && (line[l - 1] == '\n' || line[l - 1] == ',')) line[--l] = 0;
+                lines[n++] = strdup(line);
+            }
+        }
+        fclose(f);
+    }
+    char mine[512];
+    snprintf(mine, sizeof(mine), "  \"%s\": {\"tile_rows\": %lld, \"ctas_per_sm\": %d}", key, (long long)tile, ctas);
+    lines[n++] = strdup(mine);
+    char dir[1024];
+    snprintf(dir, sizeof(dir), "%s", path);
+    char* slash = strrchr(dir, '/');
+    if (slash) { *slash = 0; mkdir(dir, 0755); }
+    snprintf(tmp, sizeof(tmp), "%s.tmp", path);
+    f = fopen(tmp, "w");
+    if (f) {
+        fprintf(f, "{\n");
+        for (int i = 0; i < n; i++) fprintf(f, "%s%s\n", lines[i], i + 1 < n ? "," : "");
+        fprintf(f, "}\n");
+        fclose(f);
+        rename(tmp, path);
+    }
+    for (int i = 0; i < n; i++) free(lines[i]);
+}
+
+/* ---- lowering ---------------------------------------------------------------------- */
+typedef struct {
+    tdg_batch_query q;
+    int64_t key_name, val_name;
+    int8_t key_type, val_type;
+    uint8_t key_attrs, val_attrs;
+} bq_host_t;
+
+static int lower_one(tdb_ctx* c, td_graph_t* g, td_op_t* root, uint16_t* ops, int* n_ops, bq_host_t* out) {
+    if (!root || root->opcode != OP_GROUP || !g->table) return TD_ERR_NYI;
+    td_op_ext_t* ext = tdb_find_ext(g, root->id);
+    if (!ext || ext->n_keys != 1 || ext->n_aggs < 1) return TD_ERR_NYI;
+    td_op_ext_t* kx = tdb_find_ext(g, ext->keys[0]->id);
+    if (!kx || kx->base.opcode != OP_SCAN) return TD_ERR_NYI;
+    td_t* kcol = td_table_get_col(g->table, kx->sym);
+    if (!kcol) return TD_ERR_SCHEMA;
+    td_t* vcol = NULL;
+    int64_t vname = -1;
+    for (int a = 0; a < ext->n_aggs; a++) {
+        td_op_ext_t* ax = tdb_find_ext(g, ext->agg_ins[a]->id);
+        if (ext->agg_ops[a] == OP_COUNT && (!ax || ax->base.opcode != OP_SCAN)) continue;
+        if (!ax || ax->base.opcode != OP_SCAN) return TD_ERR_NYI;
+        td_t* v = td_table_get_col(g->table, ax->sym);
+        if (!v) return TD_ERR_SCHEMA;
+        if (vcol && v != vcol) return TD_ERR_NYI;
+        vcol = v;
+        vname = ax->sym;
+    }
+    if (!vcol) vcol = kcol, vname = kx->sym;
+    if (*n_ops == 0) {
+        *n_ops = ext->n_aggs;
+        for (int a = 0; a < ext->n_aggs; a++) ops[a] = ext->agg_ops[a];
+    } else {
+        if (*n_ops != ext->n_aggs) return TD_ERR_NYI;
+        for (int a = 0; a < ext->n_aggs; a++) if (ops[a] != ext->agg_ops[a]) return TD_ERR_NYI;
+    }
+    tdb_devcol dk, dv;
+    int st = tdb_col_device(c, kcol, 1, &dk);
+    if (!st) st = tdb_col_device(c, vcol, 0, &dv);
+    if (st) return st;
+    if (!dk.has_stats) return TD_ERR_TYPE;
+    memset(out, 0, sizeof(*out));
+    out->q.key = (tdg_col){ dk.dptr, dk.type, dk.attrs, 0, {0} };
+    out->q.val = (tdg_col){ dv.dptr, dv.type, dv.attrs, 0, {0} };
+    out->q.nrows = kcol->len;
+    if (kcol->len == 0 || dk.kmax < dk.kmin) { out->q.key_min = 0; out->q.n_slots = 1; }
+    else { out->q.key_min = dk.kmin; out->q.n_slots = dk.kmax - dk.kmin + 1; }
+    out->key_name = kx->sym;
+    out->val_name = vname;
+    out->key_type = kcol->type;
+    out->key_attrs = kcol->attrs & TD_SYM_W_MASK;
+    out->val_type = vcol->type;
+    out->val_attrs = vcol->attrs & TD_SYM_W_MASK;
+    return TD_OK;
+}
+
+static int alloc_outputs(bcache_t* e) {
+    size_t rows = (size_t)(e->plan.total_slots > 0 ? e->plan.total_slots : 1);
+    e->n_bufs = 0;
+    void** b = e->bufs;
+    if (!(b[e->n_bufs++] = tdb_dev_alloc_persistent(rows * 8))) return TD_ERR_OOM;
+    if (!(b[e->n_bufs++] = tdb_dev_alloc_persistent(rows * 8))) return TD_ERR_OOM;
+    if (!(b[e->n_bufs++] = tdb_dev_alloc_persistent(8))) return TD_ERR_OOM;
+    e->out.query = b[0];
+    e->out.key = b[1];
+    e->out.d_n_rows = b[2];
+    for (int a = 0; a < e->plan.n_aggs; a++) {
+        if (!(b[e->n_bufs++] = tdb_dev_alloc_persistent(rows * 8))) return TD_ERR_OOM;
+        e->out.aggs[a] = b[e->n_bufs - 1];
+    }
+    return TD_OK;
+}
+
+/* Time one configuration of the batch kernel (ms), or a negative value. */
+static float time_config(tdb_ctx* c, const tdg_batch_desc* d, int64_t tile, int32_t ctas, bcache_t* scratch) {
+    tdg_batch_plan p;
+    if (tdg_batch_plan_make(d, tile, ctas, &p)) return -1;
+    void* ws = tdb_dev_alloc(c, p.ws_bytes);
+    if (!ws) return -1;
+    if (tdg_batch_prepare(d, &p, ws, c->stream)) return -1;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    float best = -1;
+    for (int rep = 0; rep < 3; rep++) {
+        cudaEventRecord(a, (cudaStream_t)c->stream);
+        int st = tdg_batch_run(&p, ws, &scratch->out, c->stream);
+        cudaEventRecord(b, (cudaStream_t)c->stream);
+        if (st || cudaEventSynchronize(b) != cudaSuccess) { best = -1; break; }
+        float ms;
+        cudaEventElapsedTime(&ms, a, b);
+        if (rep > 0 && (best < 0 || ms < best)) best = ms;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return best;
+}
+
+static void autotune(tdb_ctx* c, const tdg_batch_desc* d, int64_t* tile, int32_t* ctas) {
+    char key[128];
+    tune_key(d, key, sizeof(key));
+    if (tune_load(key, tile, ctas)) return;
+    *tile = 0;
+    *ctas = 0;
+    if (getenv("TD_NO_AUTOTUNE")) return;
+    bcache_t scratch;
+    memset(&scratch, 0, sizeof(scratch));
+    if (tdg_batch_plan_make(d, 4096, 0, &scratch.plan) || alloc_outputs(&scratch)) { bcache_drop(&scratch); return; }
+    static const int64_t tiles[] = {4096, 16384, 65536};
+    static const int32_t ctass[] = {0, 2, 4};
+    float best = -1;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            float ms = time_config(c, d, tiles[i], ctass[j], &scratch);
+            if (ms > 0 && (best < 0 || ms < best)) { best = ms; *tile = tiles[i]; *ctas = ctass[j]; }
+        }
+    bcache_drop(&scratch);
+    if (best > 0) tune_store(key, *tile, *ctas);
+}
+
+static int64_t agg_out_name(uint16_t op, int64_t base) {
+    const char* sfx = op == OP_SUM ? "_sum" : op == OP_COUNT ? "_count" : op == OP_AVG ? "_mean"
+                    : op == OP_MIN ? "_min" : "_max";
+    td_t* s = td_sym_str(base);
+    char buf[300];
+    int n = s ? (int)td_str_len(s) : 0;
+    if (n > 250) n = 250;
+    if (s) memcpy(buf, td_str_ptr(s), (size_t)n);
+    memcpy(buf + n, sfx, strlen(sfx));
+    return td_sym_intern(buf, (size_t)n + strlen(sfx));
+}
+
+td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
+    if (!graphs || !roots || n < 0 || n > INT32_MAX) return TD_ERR_PTR(TD_ERR_RANGE);
+    atomic_store(&tdb_cancel_flag, 0);
+    tdb_ctx c;
+    int st = tdb_ctx_begin(&c);
+    if (st) return TD_ERR_PTR(st);
+    pthread_mutex_lock(&bcache_mu);
+    td_t* res = NULL;
+    bq_host_t* hq = calloc((size_t)(n ? n : 1), sizeof(bq_host_t));
+    tdg_batch_query* qs = calloc((size_t)(n ? n : 1), sizeof(tdg_batch_query));
+    uint16_t ops[TDG_MAX_AGGS];
+    int n_ops = 0;
+    if (!hq || !qs) { st = TD_ERR_OOM; goto done; }
+    for (int64_t i = 0; i < n && !st; i++) {
+        st = lower_one(&c, graphs[i], roots[i], ops, &n_ops, &hq[i]);
+        qs[i] = hq[i].q;
+        /* one output schema: every query's key and value columns share types */
+        if (!st && i > 0 && (hq[i].key_type != hq[0].key_type || hq[i].key_attrs != hq[0].key_attrs ||
+                             hq[i].val_type != hq[0].val_type || hq[i].val_attrs != hq[0].val_attrs))
+            st = TD_ERR_TYPE;
+    }
+    if (st) goto done;
+    if (n_ops > TDG_MAX_AGGS) { st = TD_ERR_NYI; goto done; }
+    tdg_batch_desc d;
+    memset(&d, 0, sizeof(d));
+    d.n_queries = (int32_t)n;
+    d.n_aggs = n_ops;
+    for (int a = 0; a < n_ops; a++) d.agg_ops[a] = ops[a];
+    d.queries = qs;
+
+    uint64_t sig = fnv64(1469598103934665603ULL, qs, sizeof(tdg_batch_query) * (size_t)n);
+    sig = fnv64(sig, &d.agg_ops, sizeof(d.agg_ops));
+    bcache_t* e = NULL;
+    for (int i = 0; i < BATCH_CACHE; i++) if (bcache[i].ws && bcache[i].sig == sig && bcache[i].n == n) e = &bcache[i];
+    if (!e) {
+        int64_t tile;
+        int32_t ctas;
+        autotune(&c, &d, &tile, &ctas);
+        int victim = 0;
+        for (int i = 1; i < BATCH_CACHE; i++) if (bcache[i].used < bcache[victim].used) victim = i;
+        e = &bcache[victim];
+        bcache_drop(e);
+        e->sig = sig;
+        e->n = n;
+        if ((st = tdg_batch_plan_make(&d, tile, ctas, &e->plan))) { bcache_drop(e); goto done; }
+        e->ws = tdb_dev_alloc_persistent(e->plan.ws_bytes);
+        if (!e->ws || alloc_outputs(e)) { bcache_drop(e); st = TD_ERR_OOM; goto done; }
+        if ((st = tdg_batch_prepare(&d, &e->plan, e->ws, c.stream))) { bcache_drop(e); goto done; }
+        /* capture the run once; replays reuse the instantiated graph */
+        cudaGraph_t graph = NULL;
+        cudaStream_t s = (cudaStream_t)c.stream;
+        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            int rs = tdg_batch_run(&e->plan, e->ws, &e->out, c.stream);
+            if (cudaStreamEndCapture(s, &graph) == cudaSuccess && !rs && graph) {
+                if (cudaGraphInstantiate(&e->exec, graph, 0) != cudaSuccess) e->exec = NULL;
+            }
+            if (graph) cudaGraphDestroy(graph);
+        }
+        cudaGetLastError();
+    }
+    e->used = ++bstamp;
+    if ((st = tdb_check_cancel())) goto done;
+    tdb_note_kernel();
+    if (e->exec && !tdg_timing_enabled()) {   /* timing runs the kernels directly */
+        if (cudaGraphLaunch(e->exec, (cudaStream_t)c.stream) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; goto done; }
+    } else if ((st = tdg_batch_run(&e->plan, e->ws, &e->out, c.stream))) {
+        goto done;
+    }
+    int64_t rows = 0;
+    if ((st = tdb_d2h(&c, &rows, e->out.d_n_rows, 8))) goto done;
+    if (rows < 0) { st = TD_ERR_DOMAIN; goto done; }   /* key outside its statistics */
+    res = td_table_new(2 + n_ops);
+    if (!res || TD_IS_ERR(res)) { st = TD_ERR_OOM; res = NULL; goto done; }
+    /* device columns are 8 bytes wide; keys and MIN/MAX of narrower integer
+     * columns are narrowed back to the column's type, as td_group returns them */
+    typedef struct { void* d; int8_t t; uint8_t attrs; int64_t name; } outcol_t;
+    outcol_t cols[TDG_MAX_AGGS + 2];
+    int nc = 0;
+    cols[nc++] = (outcol_t){ e->out.query, TD_I64, 0, td_sym_intern("_query", 6) };
+    cols[nc++] = (outcol_t){ e->out.key, n ? hq[0].key_type : TD_I64, n ? hq[0].key_attrs : 0,
+                             n ? hq[0].key_name : td_sym_intern("key", 3) };
+    for (int a = 0; a < n_ops; a++) {
+        int8_t t = ops[a] == OP_COUNT ? TD_I64 : (ops[a] == OP_AVG || e->plan.val_f64) ? TD_F64
+                 : (ops[a] == OP_SUM || !n) ? TD_I64 : hq[0].val_type;
+        cols[nc++] = (outcol_t){ e->out.aggs[a], t, (ops[a] == OP_MIN || ops[a] == OP_MAX) && n ? hq[0].val_attrs : 0,
+                                 agg_out_name(ops[a], n ? hq[0].val_name : 0) };
+    }
+    for (int j = 0; j < nc && !st; j++) {
+        int wide = td_sym_elem_size(cols[j].t, cols[j].attrs) == 8;
+        td_t* v = td_vec_new(wide ? cols[j].t : TD_I64, rows);
+        if (!v || TD_IS_ERR(v)) { st = TD_ERR_OOM; break; }
+        v->len = rows;
+        if (wide && cols[j].t == TD_SYM) v->attrs = cols[j].attrs;
+        if ((size_t)rows * 8 >= ((size_t)8 << 20)) tdb_pin_host(v);
+        st = tdb_d2h(&c, td_data(v), cols[j].d, (size_t)rows * 8);
+        if (!st && !wide) {
+            td_t* nv = td_vec_new(cols[j].t, rows);
+            if (!nv || TD_IS_ERR(nv)) st = TD_ERR_OOM;
+            else {
+                nv->len = rows;
+                if (cols[j].t == TD_SYM) nv->attrs = cols[j].attrs;
+                const int64_t* w = (const int64_t*)td_data(v);
+                for (int64_t i = 0; i < rows; i++) {
+                    if (cols[j].t == TD_SYM) td_write_sym(td_data(nv), i, (uint64_t)w[i], TD_SYM, cols[j].attrs);
+                    else switch (td_elem_size(cols[j].t)) {
+                        case 4: ((int32_t*)td_data(nv))[i] = (int32_t)w[i]; break;
+                        case 2: ((int16_t*)td_data(nv))[i] = (int16_t)w[i]; break;
+                        default: ((uint8_t*)td_data(nv))[i] = (uint8_t)w[i]; break;
+                    }
+                }
+                td_release(v);
+                v = nv;
+            }
+        }
+        if (!st) {
+            td_t* r2 = td_table_add_col(res, cols[j].name, v);
+            if (TD_IS_ERR(r2)) st = TD_ERR_CODE(r2); else res = r2;
+        }
+        td_release(v);
+    }
+done:
+    pthread_mutex_unlock(&bcache_mu);
+    if (st && res) { td_release(res); res = NULL; }
+    free(hq);
+    free(qs);
+    tdb_ctx_end(&c);
+    return st ? TD_ERR_PTR(st) : res;
+}
+
+void td_gpu_batch_cache_clear(void) {
+    pthread_mutex_lock(&bcache_mu);
+    for (int i = 0; i < BATCH_CACHE; i++) bcache_drop(&bcache[i]);
+    pthread_mutex_unlock(&bcache_mu);
+}

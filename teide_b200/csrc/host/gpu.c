@@ -356,7 +356,18 @@ int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
     if (!col || TD_IS_ERR(col) || col->type <= 0 || col->type == TD_TABLE || col->type == TD_LIST ||
         col->type == TD_SEL)
         return TD_ERR_TYPE;
-    if (col->attrs & TD_ATTR_SLICE) return TD_ERR_NYI;
+    if (col->attrs & TD_ATTR_SLICE) {
+        /* a view into the parent's device copy; the parent's min/max bound
+         * the slice's values, so they stay valid planning statistics */
+        td_t* parent = col->slice_parent;
+        if (!parent || TD_IS_ERR(parent) || (parent->attrs & TD_ATTR_SLICE)) return TD_ERR_NYI;
+        if (col->slice_offset < 0 || col->slice_offset + col->len > parent->len) return TD_ERR_RANGE;
+        int st = tdb_col_device(c, parent, want_stats, out);
+        if (st) return st;
+        out->dptr = (char*)out->dptr + (size_t)col->slice_offset * td_sym_elem_size(parent->type, parent->attrs);
+        out->len = col->len;
+        return TD_OK;
+    }
     uint64_t serial = tdb_block_serial(col);
     pthread_mutex_lock(&mu);
     int i = find_mirror_locked(col);
@@ -436,6 +447,7 @@ td_err_t td_gpu_pin(td_t* tbl) {
     int64_t nc = tbl->type == TD_TABLE ? td_table_ncols(tbl) : 1;
     for (int64_t j = 0; j < nc && !st; j++) {
         td_t* col = tbl->type == TD_TABLE ? td_table_get_col_idx(tbl, j) : tbl;
+        if (col && !TD_IS_ERR(col) && (col->attrs & TD_ATTR_SLICE)) col = col->slice_parent;  /* pin the data */
         if (!col || col->type <= 0 || col->type == TD_TABLE || col->type == TD_LIST) continue;
         pthread_mutex_lock(&mu);
         int have = find_mirror_locked(col) >= 0;

@@ -196,18 +196,25 @@ void* td_vec_get(td_t* vec, int64_t idx) {
     return (char*)td_data(vec) + (size_t)idx * td_sym_elem_size(vec->type, vec->attrs);
 }
 
-/* Slices are materialized copies here: every column the GPU reads must be a
- * dense block, and a copy keeps td_data() valid for the caller. */
+/* A slice is a header-only view [offset, offset + len) of its parent vector
+ * (src/vec/vec.c:185-212 in Teide): TD_ATTR_SLICE, slice_parent retained,
+ * slice_offset.  Slices of slices resolve to the ultimate parent.  On the
+ * GPU a slice of a resident column is read in place (no copy). */
 td_t* td_vec_slice(td_t* vec, int64_t offset, int64_t len) {
     if (!vec || TD_IS_ERR(vec)) return vec;
-    if (offset < 0 || len < 0 || offset + len > vec->len) return TD_ERR_PTR(TD_ERR_RANGE);
-    size_t esz = td_sym_elem_size(vec->type, vec->attrs);
-    td_t* v = vec->type == TD_SYM ? td_sym_vec_new(vec->attrs & TD_SYM_W_MASK, len)
-                                  : td_vec_new(vec->type, len);
-    if (!v || TD_IS_ERR(v)) return v;
-    memcpy(td_data(v), (char*)td_data(vec) + (size_t)offset * esz, (size_t)len * esz);
-    v->len = len;
-    return v;
+    if (offset < 0 || len < 0 || offset > vec->len || len > vec->len - offset) return TD_ERR_PTR(TD_ERR_RANGE);
+    td_t* parent = vec;
+    int64_t off = offset;
+    if (vec->attrs & TD_ATTR_SLICE) { parent = vec->slice_parent; off += vec->slice_offset; }
+    td_t* s = td_alloc(0);
+    if (!s) return TD_ERR_PTR(TD_ERR_OOM);
+    s->type = parent->type;
+    s->attrs = TD_ATTR_SLICE | (parent->attrs & TD_SYM_W_MASK);
+    s->len = len;
+    s->slice_parent = parent;
+    s->slice_offset = off;
+    td_retain(parent);
+    return s;
 }
 
 td_t* td_vec_concat(td_t* a, td_t* b) {

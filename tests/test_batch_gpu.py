@@ -1,0 +1,117 @@
+"""td_execute_batch: many group-by graphs in one launch (BASELINE config 4 shape).
+
+Each query's rows in the packed result must equal the oracle's group-by of
+that query's table (keys, COUNT exact; SUM/MAX of F64 within 1e-12), and a
+repeated call -- which replays the cached CUDA graph -- must return the same
+rows."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import oracle
+from teide_b200 import workloads
+from teide_b200.td import OP_COUNT, OP_MAX, OP_SUM
+
+pytestmark = pytest.mark.gpu
+
+
+def _bind(td):
+    L = td.lib
+    L.td_execute_batch.restype = C.c_void_p
+    L.td_execute_batch.argtypes = [C.c_void_p, C.c_void_p, C.c_int64]
+    L.td_gpu_pin.argtypes = [C.c_void_p]
+    return L
+
+
+def run_batch(td, tables, ops=(OP_SUM, OP_COUNT, OP_MAX)):
+    L = _bind(td)
+    graphs, roots = [], []
+    for t in tables:
+        g = td.graph(t)
+        roots.append(g.group([g.scan("key")], list(ops), [g.scan("val")] * len(ops)))
+        graphs.append(g)
+    G = (C.c_void_p * len(graphs))(*[g.g for g in graphs])
+    R = (C.c_void_p * len(roots))(*roots)
+    r = td.check(L.td_execute_batch(G, R, len(graphs)), "batch")
+    out = td.table_dict(r)
+    td.release(r)
+    for g in graphs:
+        g.free()
+    return out
+
+
+def test_batch_matches_oracle_per_query(gpu, tmp_path, monkeypatch):
+    monkeypatch.setenv("TD_TUNE_CACHE", str(tmp_path / "tune.json"))
+    rows, ks = workloads.config4_shapes(n_queries=96, seed=41, rows=(1, 300_000), groups=(1, 70_000))
+    datas = [workloads.config4_query(int(r), int(k), seed=1000 + i) for i, (r, k) in enumerate(zip(rows, ks))]
+    tables = [gpu.table(d) for d in datas]
+    L = _bind(gpu)
+    for t in tables:
+        assert L.td_gpu_pin(t) == 0
+    first = run_batch(gpu, tables)
+    again = run_batch(gpu, tables)                   # cached graph replay
+    assert list(first) == ["_query", "key", "val_sum", "val_count", "val_max"]
+    for name in ("_query", "key", "val_count", "val_max"):
+        assert np.array_equal(first[name], again[name]), name
+    assert np.allclose(first["val_sum"], again["val_sum"], rtol=1e-12, atol=1e-9)
+    q = first["_query"]
+    assert np.all(np.diff(q) >= 0)                    # grouped by query, in order
+    for i, d in enumerate(datas):
+        sel = q == i
+        want = oracle.group({"key": d["key"]}, [(OP_SUM, "val", d["val"]), (OP_COUNT, "val", None),
+                                                (OP_MAX, "val", d["val"])])
+        assert np.array_equal(first["key"][sel], want["key"]), i
+        assert np.array_equal(first["val_count"][sel], want["val_count"]), i
+        assert np.allclose(first["val_sum"][sel], want["val_sum"], rtol=1e-12, atol=1e-9), i
+        assert np.array_equal(first["val_max"][sel], want["val_max"]), i
+    for t in tables:
+        gpu.release(t)
+
+
+def test_batch_rejects_mixed_shapes(gpu):
+    a = gpu.table({"key": np.arange(10, dtype=np.int64), "val": np.ones(10)})
+    b = gpu.table({"key": np.arange(10, dtype=np.int64), "val": np.ones(10)})
+    L = _bind(gpu)
+    ga, gb = gpu.graph(a), gpu.graph(b)
+    ra = ga.group([ga.scan("key")], [OP_SUM], [ga.scan("val")])
+    rb = gb.group([gb.scan("key")], [OP_MAX], [gb.scan("val")])
+    G = (C.c_void_p * 2)(ga.g, gb.g)
+    R = (C.c_void_p * 2)(ra, rb)
+    p = L.td_execute_batch(G, R, 2) or 0
+    assert p == 7                                     # TD_ERR_NYI
+    ga.free(); gb.free()
+    gpu.release(a); gpu.release(b)
+
+
+def test_batch_equals_per_query_execute_narrow_types(gpu):
+    """I32 keys and I32 values: keys and MIN/MAX come back as I32, SUM as I64,
+    AVG as F64 -- the same columns td_execute returns for each graph."""
+    from teide_b200.td import I32, OP_AVG, OP_MIN
+    r = np.random.default_rng(7)
+    datas = []
+    for i in range(20):
+        n = int(r.integers(0, 50_000))
+        lo = int(r.integers(-1000, 1000))
+        datas.append({"key": (r.integers(lo, lo + int(r.integers(1, 3000)), n).astype(np.int32), I32),
+                      "val": (r.integers(-2**31, 2**31 - 1, n).astype(np.int32), I32)})
+    tables = [gpu.table(d) for d in datas]
+    ops = (OP_SUM, OP_MIN, OP_MAX, OP_AVG, OP_COUNT)
+    got = run_batch(gpu, tables, ops)
+    q = got["_query"]
+    for i, t in enumerate(tables):
+        g = gpu.graph(t)
+        root = g.group([g.scan("key")], list(ops), [g.scan("val")] * len(ops))
+        p = g.execute(root, optimize=False)
+        want = gpu.table_dict(p)
+        gpu.release(p)
+        g.free()
+        sel = q == i
+        for name, col in want.items():
+            assert got[name].dtype == col.dtype, name
+            if col.dtype.kind == "f":
+                assert np.allclose(got[name][sel], col, rtol=1e-12), (i, name)
+            else:
+                assert np.array_equal(got[name][sel], col), (i, name)
+    for t in tables:
+        gpu.release(t)
