@@ -111,17 +111,17 @@ class Clocks:
 
 # ---- workloads through the td.h API ------------------------------------------------
 
-def make_tables(td, workload, rank, device):
+def make_tables(td, workload, rank, device, scale=1.0):
     from teide_b200 import workloads
     if workload == "join_group":
-        b, p = workloads.config3(seed=3 + 1000 * rank, device=device)
+        b, p = workloads.config3(n_probe=int(100_000_000 * scale), seed=3 + 1000 * rank, device=device)
         bt, pt = td.table(b), td.table(p)
         return {"build": bt, "probe": pt}, len(p["fk"]), 16 * len(b["pk"]) + 24 * len(p["fk"]), 24 * len(p["fk"])
     if workload == "group_radix":
-        c = workloads.config2(seed=2 + 1000 * rank, device=device)
+        c = workloads.config2(n=int(200_000_000 * scale), seed=2 + 1000 * rank, device=device)
         t = td.table(c)
         return {"t": t}, len(c["key"]), 24 * len(c["key"]), 24 * len(c["key"])
-    c = workloads.config1(seed=1 + 1000 * rank)
+    c = workloads.config1(n=int(10_000_000 * scale), seed=1 + 1000 * rank)
     t = td.table(c)
     return {"t": t}, len(c["flag"]), 24 * len(c["flag"]), 24 * len(c["flag"])
 
@@ -202,7 +202,7 @@ class Batch:
 
 def batch_main(args, td, L, rank, world, local, barrier, max_over_ranks):
     import torch
-    b = Batch(td, seed=4 + 1000 * rank)
+    b = Batch(td, seed=4 + 1000 * rank, first=max(1, int(round(4096 * args.scale))))
     for t in b.tables:
         st = L.td_gpu_pin(t)
         if st:
@@ -233,32 +233,40 @@ def batch_main(args, td, L, rank, world, local, barrier, max_over_ranks):
         main_ms.append(L.tdg_last_main_ms())
     L.tdg_set_timing(0)
     # plain: the same queries, one td_execute each
-    b.plain()
-    barrier()
-    plain_steps = 2
-    ev0.record()
-    for _ in range(plain_steps):
+    plain = None
+    if not args.no_plain:
         b.plain()
-    ev1.record()
-    torch.cuda.synchronize()
+        barrier()
+        plain_steps = 2
+        ev0.record()
+        for _ in range(plain_steps):
+            b.plain()
+        ev1.record()
+        torch.cuda.synchronize()
+        plain_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+        plain_value = b.n * world * plain_steps / plain_elapsed
+        plain = {"value": plain_value, "unit": "queries/s", "steps": plain_steps,
+                 "how": "one td_execute per query, same resident tables", "speedup": value / plain_value}
     time.sleep(0.3)
     clk.__exit__(None, None, None)
-    plain_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
-    plain_value = b.n * world * plain_steps / plain_elapsed
     # end to end: host tables, every step uploads every query's columns
-    for t in b.tables:
-        L.td_gpu_unpin(t)
-    L.td_gpu_trim()
-    b.batched()
-    barrier()
-    e2e_steps = args.e2e_steps or 2
-    ev0.record()
-    for _ in range(e2e_steps):
+    e2e = None
+    if not args.no_e2e:
+        for t in b.tables:
+            L.td_gpu_unpin(t)
+        L.td_gpu_trim()
         b.batched()
-    ev1.record()
-    torch.cuda.synchronize()
-    e2e_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
-    s_e2e = stats_of(td)
+        barrier()
+        e2e_steps = args.e2e_steps or 2
+        ev0.record()
+        for _ in range(e2e_steps):
+            b.batched()
+        ev1.record()
+        torch.cuda.synchronize()
+        e2e_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+        s_e2e = stats_of(td)
+        e2e = {"value": b.n * world * e2e_steps / e2e_elapsed, "unit": "queries/s",
+               "h2d_bytes_per_step": int(s_e2e.h2d), "d2h_bytes_per_step": int(s_e2e.d2h), "steps": e2e_steps}
     hbm, peak_kind = peaks()
     mean_main = statistics.median(main_ms)
     alg = 16 * b.rows
@@ -271,15 +279,13 @@ def batch_main(args, td, L, rank, world, local, barrier, max_over_ranks):
                    "algorithmic_bytes_per_step": alg, "aggs": "SUM/COUNT/MAX(val) by key",
                    "l2": "inputs larger than L2 (no flush)", "tables": "resident in HBM (td_gpu_pin)",
                    "launch": "td_execute_batch: one persistent kernel, replayed CUDA graph",
-                   "parallelism": f"replicas{world}"},
-        "plain": {"value": plain_value, "unit": "queries/s", "steps": plain_steps,
-                  "how": "one td_execute per query, same resident tables", "speedup": value / plain_value},
+                   "parallelism": f"replicas{world}", "scale": args.scale},
+        "plain": plain,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None,
-                     "traffic": profile_traffic("batch_group_cfg4.md"), "kernel": "k_batch_agg",
+                     "traffic": profile_traffic("k_batch_agg_batch.md"), "kernel": "k_batch_agg",
                      "bytes_per_launch": alg, "mean_launch_ms": mean_main, "peak_source": peak_kind},
-        "e2e": {"value": b.n * world * e2e_steps / e2e_elapsed, "unit": "queries/s",
-                "h2d_bytes_per_step": int(s_e2e.h2d), "d2h_bytes_per_step": int(s_e2e.d2h), "steps": e2e_steps},
+        "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clk.summary(tc0, tc1),
     }
@@ -378,6 +384,10 @@ def main():
     ap.add_argument("--workload", default="join_group", choices=["join_group", "group_radix", "readme_group", "batch"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-table (upload) pass")
+    ap.add_argument("--no-plain", action="store_true", help="batch: skip the one-query-per-launch pass")
+    ap.add_argument("--scale", type=float, default=1.0,
+                    help="fraction of the workload size (smaller cases for profiler captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)
@@ -426,7 +436,7 @@ def main():
             dist.destroy_process_group()
         return
 
-    tabs, rows, alg_bytes, main_bytes = make_tables(td, args.workload, rank, "cuda")
+    tabs, rows, alg_bytes, main_bytes = make_tables(td, args.workload, rank, "cuda", args.scale)
     torch.cuda.empty_cache()
 
     # ---- resident: tables pinned in HBM ----
@@ -460,41 +470,46 @@ def main():
     value = rows * world * args.steps / elapsed
 
     # ---- end to end: host tables, uploads inside every step ----
-    for t in tabs.values():
-        L.td_gpu_unpin(t)
-    L.td_gpu_trim()
-    e2e_steps = args.e2e_steps or args.steps
-    run_query(td, args.workload, tabs)          # page-locks the host columns once
-    barrier()
-    ev0.record()
-    for _ in range(e2e_steps):
-        run_query(td, args.workload, tabs)
-    ev1.record()
-    torch.cuda.synchronize()
-    e2e_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
-    s_e2e = stats_of(td)
-    e2e_value = rows * world * e2e_steps / e2e_elapsed
+    e2e = None
+    if not args.no_e2e:
+        for t in tabs.values():
+            L.td_gpu_unpin(t)
+        L.td_gpu_trim()
+        e2e_steps = args.e2e_steps or args.steps
+        run_query(td, args.workload, tabs)          # page-locks the host columns once
+        barrier()
+        ev0.record()
+        for _ in range(e2e_steps):
+            run_query(td, args.workload, tabs)
+        ev1.record()
+        torch.cuda.synchronize()
+        e2e_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+        s_e2e = stats_of(td)
+        e2e = {"value": rows * world * e2e_steps / e2e_elapsed, "unit": "rows/s",
+               "h2d_bytes_per_step": int(s_e2e.h2d), "d2h_bytes_per_step": int(s_e2e.d2h), "steps": e2e_steps}
 
     hbm, peak_kind = peaks()
     mean_main = sum(main_ms) / len(main_ms) if main_ms else 0.0
     achieved = main_bytes / (mean_main / 1e3) / 1e9 if mean_main > 0 else None
-    prof = {"join_group": "fused_join_group_cfg3.md", "group_radix": "group_radix_cfg2.md",
-            "readme_group": "readme_group_cfg1.md"}[args.workload]
+    prof = {"join_group": "k_payload_probe_join_group.md", "group_radix": "k_group_group_radix.md",
+            "readme_group": "k_group_readme_group.md"}[args.workload]
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
         "config": {"workload": args.workload, "rows_per_gpu_per_step": rows,
                    "algorithmic_bytes_per_step": alg_bytes, "l2": "inputs larger than L2 (no flush)",
-                   "tables": "resident in HBM (td_gpu_pin)", "parallelism": f"replicas{world}"},
+                   "tables": "resident in HBM (td_gpu_pin)", "parallelism": f"replicas{world}",
+                   "scale": args.scale},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": profile_traffic(prof),
-                     "kernel": "k_group<fused probe + aggregate>", "bytes_per_launch": main_bytes,
+                     "kernel": {"join_group": "k_payload_probe (fused probe + aggregate)",
+                                "group_radix": "k_group", "readme_group": "k_group"}[args.workload],
+                     "bytes_per_launch": main_bytes,
                      "mean_launch_ms": mean_main, "peak_source": peak_kind,
                      "step_frac": alg_bytes / (elapsed / args.steps) / 1e9 / hbm,
                      "build_ms": (sum(build_ms) / len(build_ms)) if build_ms and build_ms[0] else None},
-        "e2e": {"value": e2e_value, "unit": "rows/s", "h2d_bytes_per_step": int(s_e2e.h2d),
-                "d2h_bytes_per_step": int(s_e2e.d2h), "steps": e2e_steps},
+        "e2e": e2e,
         "gpu_launches": int(launches),
         "clocks": clk.summary(tc0, tc1),
         "resident_h2d_bytes_per_step": int(s_res.h2d),

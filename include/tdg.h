@@ -294,6 +294,8 @@ typedef struct tdg_batch_plan {
     int32_t agg_ops[TDG_MAX_AGGS];
     int32_t val_f64;       /* the value columns are F64 (all queries alike) */
     int32_t words;         /* 8-byte words per slot record */
+    int32_t threads;       /* threads per persistent CTA */
+    int32_t smem_bytes;    /* dynamic shared memory per CTA */
 } tdg_batch_plan;
 
 typedef struct tdg_batch_out {
@@ -303,7 +305,12 @@ typedef struct tdg_batch_out {
     int64_t* d_n_rows;             /* one int64: rows written */
 } tdg_batch_out;
 
-/* tile_rows / ctas_per_sm of 0 pick defaults. */
+/* tile_rows / ctas_per_sm of 0 pick defaults.  ctas_per_sm also sets the
+ * shared-memory budget of a persistent CTA: 1 -> 1024 threads and most of
+ * the SM's shared memory, 2 -> 512 threads and half of it, otherwise 256
+ * threads and 48 KB.  A query whose key range fits that budget is cut into
+ * tiles of at least 8 rows per slot, so its shared aggregates are flushed
+ * rarely. */
 tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_rows, int32_t ctas_per_sm,
                                tdg_batch_plan* plan);
 tdg_status tdg_batch_prepare(const tdg_batch_desc* d, const tdg_batch_plan* plan, void* ws, void* stream);
@@ -322,6 +329,8 @@ int32_t tdg_device_sm_count(void);
  * records nothing while its stream is being captured into a CUDA graph). */
 void     tdg_set_timing(int32_t on);
 int32_t  tdg_timing_enabled(void);
+/* A host that replays captured tdg launches (a CUDA graph) counts them here. */
+void     tdg_count_launches(uint64_t n);
 float    tdg_last_main_ms(void);
 float    tdg_last_build_ms(void);
 /* Kernels launched by this library since the process started. */

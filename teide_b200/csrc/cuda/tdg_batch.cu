@@ -26,8 +26,11 @@
 namespace tdg {
 
 constexpr int kBatchThreads = 256;
+constexpr int kBatchMaxThreads = 1024;
 constexpr int64_t kDefaultTile = 16384;
-constexpr int kDefaultSmemSlots = 2048;
+constexpr int kStaticSmemReserve = 256;   // the kernel's own __shared__ words
+constexpr int64_t kRowsPerSlot = 8;       // shared-path tiles hold >= 8 rows per slot
+constexpr int kBR = 4;                    // rows per thread per chunk
 constexpr int kEmitBlock = 256;
 constexpr int64_t kMaxDenseSlots = 1 << 20;
 
@@ -35,13 +38,13 @@ enum : int32_t { BK_COUNT = 0, BK_SUM_I, BK_SUM_F, BK_MIN_I, BK_MAX_I, BK_MIN_F,
 
 struct BQ {
     tdg_col key, val;
-    int64_t nrows, key_min, n_slots, acc_off, first_item;
+    int64_t nrows, key_min, n_slots, acc_off, first_item, tile_rows;
 };
 
 struct BatchK {
     const BQ* q;
     const int32_t* item_q;
-    int64_t n_items, tile_rows, total_slots;
+    int64_t n_items, total_slots;
     unsigned long long* rec;
     unsigned long long* counter;
     int32_t* err;
@@ -89,7 +92,6 @@ static BatchK make_bk(const tdg_batch_plan* p, void* ws) {
     B.qoff = (int64_t*)(w + L.qoff);
     B.rec = (unsigned long long*)(w + L.rec);
     B.n_items = p->n_items;
-    B.tile_rows = p->tile_rows;
     B.total_slots = p->total_slots;
     B.n_queries = p->n_queries;
     B.W = p->words;
@@ -128,25 +130,27 @@ __global__ void k_batch_init(const BatchK B) {
 }
 
 __device__ __forceinline__ void bupd(unsigned long long* a, int kind, int64_t iv, double fv, bool global) {
+    // global MIN/MAX: an L2 read filters updates that cannot win; the stored
+    // extreme only moves toward the row's value, so a stale read never loses one
     switch (kind) {
         case BK_SUM_I: atomicAdd(a, (unsigned long long)iv); break;
         case BK_SUM_F: atomicAdd((double*)a, fv); break;
         case BK_MIN_I:
-            if (!global || iv < *(volatile long long*)a) atomicMin((long long*)a, (long long)iv);
+            if (!global || iv < __ldcg((const long long*)a)) atomicMin((long long*)a, (long long)iv);
             break;
         case BK_MAX_I:
-            if (!global || iv > *(volatile long long*)a) atomicMax((long long*)a, (long long)iv);
+            if (!global || iv > __ldcg((const long long*)a)) atomicMax((long long*)a, (long long)iv);
             break;
         case BK_MIN_F:
             if (fv == fv) {
                 const long long o = f2ord(fv);
-                if (!global || o < *(volatile long long*)a) atomicMin((long long*)a, o);
+                if (!global || o < __ldcg((const long long*)a)) atomicMin((long long*)a, o);
             }
             break;
         case BK_MAX_F:
             if (fv == fv) {
                 const long long o = f2ord(fv);
-                if (!global || o > *(volatile long long*)a) atomicMax((long long*)a, o);
+                if (!global || o > __ldcg((const long long*)a)) atomicMax((long long*)a, o);
             }
             break;
         default: break;
@@ -164,7 +168,7 @@ __device__ __forceinline__ void bmerge(unsigned long long* a, int kind, unsigned
 }
 
 // The persistent kernel: CTAs pull (query, tile) items until the queue drains.
-__global__ void __launch_bounds__(kBatchThreads) k_batch_agg(const BatchK B) {
+__global__ void __launch_bounds__(kBatchMaxThreads) k_batch_agg(const BatchK B) {
     extern __shared__ unsigned long long sm[];
     __shared__ long long s_item;
     uint32_t* scnt = (uint32_t*)sm;
@@ -177,8 +181,8 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch_agg(const BatchK B) {
         if (item >= B.n_items) break;
         const int q = B.item_q[item];
         const BQ Q = B.q[q];
-        const int64_t r0 = (item - Q.first_item) * B.tile_rows;
-        const int64_t r1 = r0 + B.tile_rows < Q.nrows ? r0 + B.tile_rows : Q.nrows;
+        const int64_t r0 = (item - Q.first_item) * Q.tile_rows;
+        const int64_t r1 = r0 + Q.tile_rows < Q.nrows ? r0 + Q.tile_rows : Q.nrows;
         const bool use_smem = Q.n_slots <= B.smem_slots && (r1 - r0) >= 2 * Q.n_slots;
         const int64_t S = Q.n_slots;
         if (use_smem) {
@@ -188,21 +192,59 @@ __global__ void __launch_bounds__(kBatchThreads) k_batch_agg(const BatchK B) {
                     for (int64_t s = threadIdx.x; s < S; s += blockDim.x) sacc[B.ai[a] * S + s] = B.finit[1 + B.ai[a]];
             __syncthreads();
         }
-        for (int64_t r = r0 + threadIdx.x; r < r1; r += blockDim.x) {
-            const int64_t k = ld_i(Q.key, r) - Q.key_min;
-            if (k < 0 || k >= S) { atomicCAS(B.err, 0, E_DOMAIN); continue; }
-            const bool vf = Q.val.type == T_F64;
-            const double fv = vf ? ld_f(Q.val, r) : 0.0;
-            const int64_t iv = vf ? 0 : ld_i(Q.val, r);
+        // rows in chunks of kBR per thread: the chunk's loads issue together,
+        // and the CTA keeps the chunk two ahead in flight as an L2 prefetch
+        const int64_t chunk = (int64_t)blockDim.x * kBR;
+        const int vsz = elem_size(Q.val.type, Q.val.attrs), ksz = elem_size(Q.key.type, Q.key.attrs);
+        if (threadIdx.x < 2) {
+            const int64_t e = r0 + 2 * chunk < r1 ? r0 + 2 * chunk : r1;
+            const tdg_col& c = threadIdx.x ? Q.val : Q.key;
+            const int64_t z = threadIdx.x ? vsz : ksz;
+            l2_prefetch((const char*)c.data + r0 * z, (e - r0) * z);
+        }
+        const bool vf = Q.val.type == T_F64;
+        for (int64_t c0 = r0; c0 < r1; c0 += chunk) {
+            if (threadIdx.x < 2) {
+                const int64_t p0 = c0 + 2 * chunk, p1 = p0 + chunk < r1 ? p0 + chunk : r1;
+                if (p0 < p1) {
+                    const tdg_col& c = threadIdx.x ? Q.val : Q.key;
+                    const int64_t z = threadIdx.x ? vsz : ksz;
+                    l2_prefetch((const char*)c.data + p0 * z, (p1 - p0) * z);
+                }
+            }
+            int64_t k[kBR], iv[kBR];
+            double fv[kBR];
+            bool ok[kBR];
+#pragma unroll
+            for (int j = 0; j < kBR; j++) {
+                const int64_t r = c0 + j * (int64_t)blockDim.x + threadIdx.x;
+                ok[j] = r < r1;
+                k[j] = ok[j] ? ld_i(Q.key, r) - Q.key_min : 0;
+                fv[j] = ok[j] && vf ? ld_f(Q.val, r) : 0.0;
+                iv[j] = ok[j] && !vf ? ld_i(Q.val, r) : 0;
+            }
+#pragma unroll
+            for (int j = 0; j < kBR; j++)
+                if (ok[j] && (k[j] < 0 || k[j] >= S)) { atomicCAS(B.err, 0, E_DOMAIN); ok[j] = false; }
             if (use_smem) {
-                atomicAdd(&scnt[k], 1u);
+#pragma unroll
+                for (int j = 0; j < kBR; j++) if (ok[j]) atomicAdd(&scnt[k[j]], 1u);
                 for (int a = 0; a < B.na; a++)
-                    if (B.ai[a] >= 0) bupd(&sacc[B.ai[a] * S + k], B.kind[a], iv, fv, false);
+                    if (B.ai[a] >= 0) {
+#pragma unroll
+                        for (int j = 0; j < kBR; j++)
+                            if (ok[j]) bupd(&sacc[B.ai[a] * S + k[j]], B.kind[a], iv[j], fv[j], false);
+                    }
             } else {
-                unsigned long long* rec = B.rec + (Q.acc_off + k) * B.W;
-                atomicAdd(rec, 1ULL);
+                unsigned long long* base = B.rec + Q.acc_off * B.W;
+#pragma unroll
+                for (int j = 0; j < kBR; j++) if (ok[j]) atomicAdd(base + k[j] * B.W, 1ULL);
                 for (int a = 0; a < B.na; a++)
-                    if (B.ai[a] >= 0) bupd(rec + 1 + B.ai[a], B.kind[a], iv, fv, true);
+                    if (B.ai[a] >= 0) {
+#pragma unroll
+                        for (int j = 0; j < kBR; j++)
+                            if (ok[j]) bupd(base + k[j] * B.W + 1 + B.ai[a], B.kind[a], iv[j], fv[j], true);
+                    }
             }
         }
         if (use_smem) {
@@ -302,6 +344,16 @@ __global__ void __launch_bounds__(kEmitBlock) k_batch_emit(const BatchK B, const
 
 using namespace tdg;
 
+// Per-query tile: a query whose slots fit in shared memory gets tiles of at
+// least kRowsPerSlot rows per slot (fewer flushes of its shared aggregates).
+static int64_t query_tile(const tdg_batch_query& q, const tdg_batch_plan* p) {
+    if (q.n_slots <= p->smem_slots) {
+        const int64_t t = q.n_slots * kRowsPerSlot;
+        return t > p->tile_rows ? t : p->tile_rows;
+    }
+    return p->tile_rows;
+}
+
 extern "C" tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_rows, int32_t ctas_per_sm,
                                           tdg_batch_plan* p) {
     if (!d || !p || (d->n_queries > 0 && !d->queries)) return E_TYPE;
@@ -309,7 +361,6 @@ extern "C" tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_
     memset(p, 0, sizeof(*p));
     p->tile_rows = tile_rows > 0 ? tile_rows : kDefaultTile;
     p->ctas_per_sm = ctas_per_sm > 0 ? ctas_per_sm : 0;
-    p->smem_slots = kDefaultSmemSlots;
     p->n_queries = d->n_queries;
     p->n_aggs = d->n_aggs;
     int n_acc = 0;
@@ -320,9 +371,25 @@ extern "C" tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_
         n_acc += op != A_COUNT;
     }
     p->words = 1 + n_acc == 3 ? 4 : 1 + n_acc;
-    // shared accumulators: 32-bit counts + n_acc 8-byte values per slot in 48 KB
-    const int fit = (int)((48 * 1024 - 8) / (4 + 8 * (size_t)n_acc));
-    p->smem_slots = fit < kDefaultSmemSlots ? fit : kDefaultSmemSlots;
+    // 1 CTA per SM: 1024 threads and most of the SM's shared memory; 2: 512
+    // threads and half of it; otherwise 256 threads in the default 48 KB.
+    // The kernel's static __shared__ words come out of the same budget.
+    size_t budget = 48 * 1024;
+    p->threads = kBatchThreads;
+    if (p->ctas_per_sm == 1 || p->ctas_per_sm == 2) {
+        int optin = 0, dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess || optin <= 0) {
+            cudaGetLastError();
+            optin = 48 * 1024;
+        }
+        budget = p->ctas_per_sm == 1 ? (size_t)optin : (size_t)optin / 2;
+        p->threads = p->ctas_per_sm == 1 ? 1024 : 512;
+    }
+    budget -= kStaticSmemReserve;
+    // shared accumulators: 32-bit counts + n_acc 8-byte values per slot
+    p->smem_slots = (int32_t)((budget - 8) / (4 + 8 * (size_t)n_acc));
+    p->smem_bytes = (int32_t)(((((size_t)p->smem_slots * 4) + 7) & ~(size_t)7) + (size_t)p->smem_slots * 8 * n_acc);
     p->val_f64 = d->n_queries > 0 && d->queries[0].val.type == T_F64;
     for (int i = 0; i < d->n_queries; i++) {
         const tdg_batch_query& q = d->queries[i];
@@ -332,7 +399,8 @@ extern "C" tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_
         // direct-indexed records only: a key range far wider than the query
         // (sparse keys) belongs to the hash-table group-by, not the batch
         if (q.n_slots > kMaxDenseSlots && q.n_slots > 4 * q.nrows) return E_NYI;
-        p->n_items += (q.nrows + p->tile_rows - 1) / p->tile_rows;
+        const int64_t t = query_tile(q, p);
+        p->n_items += (q.nrows + t - 1) / t;
         p->total_slots += q.n_slots;
     }
     if (p->n_items > INT32_MAX) return E_RANGE;
@@ -353,12 +421,18 @@ extern "C" tdg_status tdg_batch_prepare(const tdg_batch_desc* d, const tdg_batch
         b.nrows = q.nrows; b.key_min = q.key_min; b.n_slots = q.n_slots;
         b.acc_off = acc;
         b.first_item = item;
-        const int64_t tiles = (q.nrows + p->tile_rows - 1) / p->tile_rows;
+        b.tile_rows = query_tile(q, p);
+        const int64_t tiles = (q.nrows + b.tile_rows - 1) / b.tile_rows;
         for (int64_t t = 0; t < tiles; t++) item_q[(size_t)(item + t)] = i;
         item += tiles;
         acc += q.n_slots;
     }
     if (item != p->n_items || acc != p->total_slots) return E_RANGE;
+    if (p->smem_bytes > 48 * 1024 &&
+        cudaFuncSetAttribute((const void*)k_batch_agg, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return E_IO;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     char* w = (char*)ws;
     if (cudaMemsetAsync(w + L.hdr, 0, 256, s) != cudaSuccess ||
@@ -380,13 +454,12 @@ extern "C" tdg_status tdg_batch_run(const tdg_batch_plan* p, void* ws, const tdg
         const int g = grid_for((const void*)k_batch_init, kThreads, 0, (p->total_slots * p->words + 31) / 32 * 32);
         (note_launch(), k_batch_init<<<g, kThreads, 0, s>>>(B));
     }
-    int n_acc = 0;
-    for (int a = 0; a < p->n_aggs; a++) n_acc += p->agg_ops[a] != A_COUNT;
-    const size_t smem = (((size_t)p->smem_slots * 4 + 7) & ~(size_t)7) + (size_t)p->smem_slots * 8 * n_acc;
+    const size_t smem = (size_t)p->smem_bytes;
+    const int threads = p->threads > 0 ? p->threads : kBatchThreads;
     if (p->n_items > 0) {
         int per_sm = p->ctas_per_sm;
         if (per_sm <= 0) {
-            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_batch_agg, kBatchThreads, smem) != cudaSuccess || per_sm < 1)
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)k_batch_agg, threads, smem) != cudaSuccess || per_sm < 1)
                 per_sm = 1;
         }
         int64_t g = (int64_t)per_sm * sm_count();
@@ -397,7 +470,7 @@ extern "C" tdg_status tdg_batch_run(const tdg_batch_plan* p, void* ws, const tdg
         EventTimer t;
         const bool timed = cs == cudaStreamCaptureStatusNone && timing_on();
         if (timed) t.start(s);
-        (note_launch(), k_batch_agg<<<(unsigned)g, kBatchThreads, smem, s>>>(B));
+        (note_launch(), k_batch_agg<<<(unsigned)g, threads, smem, s>>>(B));
         if (timed) {
             t.stop(s);
             cudaEventSynchronize(t.b);

@@ -294,6 +294,54 @@ __device__ inline int block_excl_scan(int v, int* total, int* scratch) {
     return warp_off + x - v;
 }
 
+// ---- L2 prefetch of streamed column ranges ------------------------------------------
+// cp.async.bulk.prefetch.L2 asks the copy engine to pull a contiguous range
+// into L2 without registers, shared memory or a completion wait, so a CTA can
+// keep the next tile's DRAM reads in flight while its threads work on the
+// current tile.  The range is shrunk inward to 16-byte boundaries (the
+// instruction's alignment rule), so it never touches bytes outside
+// [p, p + bytes); the few edge bytes are simply loaded without a prefetch.
+__device__ __forceinline__ void l2_prefetch(const void* p, int64_t bytes) {
+    if (bytes <= 0) return;
+    const unsigned long long a = (unsigned long long)p;
+    unsigned long long lo = (a + 15ull) & ~15ull;
+    const unsigned long long hi = (a + (unsigned long long)bytes) & ~15ull;
+    while (lo < hi) {
+        const unsigned long long left = hi - lo;
+        const unsigned sz = (unsigned)(left < (1ull << 20) ? left : (1ull << 20));
+        asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\t"
+                     "cp.async.bulk.prefetch.L2.global [g], %1;\n\t}" :: "l"(lo), "r"(sz) : "memory");
+        lo += sz;
+    }
+}
+
+// Columns a kernel streams row by row (probe side / plain table side).
+constexpr int kMaxPf = 16;
+struct PfCols {
+    const char* p[kMaxPf];
+    int32_t esz[kMaxPf];
+    int32_t n;
+    int32_t pad;
+};
+
+// Threads 0..n-1 of a CTA each prefetch rows [r0, r1) of one column.
+__device__ __forceinline__ void prefetch_rows(const PfCols& F, int64_t r0, int64_t r1) {
+    if ((int)threadIdx.x < F.n && r0 < r1) {
+        const int64_t e = F.esz[threadIdx.x];
+        l2_prefetch(F.p[threadIdx.x] + r0 * e, (r1 - r0) * e);
+    }
+}
+
+inline void pf_add(PfCols& F, const tdg_col& c) {
+    if (!c.data || F.n >= kMaxPf) return;
+    for (int i = 0; i < F.n; i++) if (F.p[i] == (const char*)c.data) return;
+    const int e = elem_size(c.type, c.attrs);
+    if (e <= 0) return;
+    F.p[F.n] = (const char*)c.data;
+    F.esz[F.n] = e;
+    F.n++;
+}
+
 // ---- host-side helpers ------------------------------------------------------------
 Pred make_pred(const tdg_expr* prog, const uint64_t* sel, int* pk);
 int sm_count();

@@ -414,6 +414,7 @@ extern "C" tdg_status tdg_select_gather(int64_t n, const tdg_expr* pred, const u
 
 extern "C" void tdg_set_timing(int32_t on) { g_timing.store(on ? 1 : 0); }
 extern "C" int32_t tdg_timing_enabled(void) { return g_timing.load(); }
+extern "C" void tdg_count_launches(uint64_t n) { note_launch((int)n); }
 extern "C" float tdg_last_main_ms(void) { return g_main_ms.load(); }
 extern "C" float tdg_last_build_ms(void) { return g_build_ms.load(); }
 extern "C" uint64_t tdg_launch_count(void) { return g_launches.load(); }

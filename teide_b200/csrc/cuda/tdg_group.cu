@@ -75,6 +75,7 @@ struct GroupK {
     uint32_t* sample_cnt;
     int64_t* hot;                 // hot slot list
     int32_t* hot_n;
+    PfCols pf;                    // streamed columns the main kernels prefetch into L2
 };
 
 struct OutK {
@@ -153,11 +154,13 @@ __device__ __forceinline__ void ld_items_f(const tdg_col& c, const int64_t (&r)[
 // which after the first rows of a group is almost always.
 template <bool GL>
 __device__ __forceinline__ void upd_min(unsigned long long* a, long long v) {
-    if (!GL || v < *(volatile long long*)a) atomicMin((long long*)a, v);
+    // the L2 read (ld.global.cg) is only a filter: the stored extreme only
+    // moves toward v, so a stale read can cost an extra atomic, never a lost one
+    if (!GL || v < __ldcg((const long long*)a)) atomicMin((long long*)a, v);
 }
 template <bool GL>
 __device__ __forceinline__ void upd_max(unsigned long long* a, long long v) {
-    if (!GL || v > *(volatile long long*)a) atomicMax((long long*)a, v);
+    if (!GL || v > __ldcg((const long long*)a)) atomicMax((long long*)a, v);
 }
 
 // Merge one accumulator value (already in accumulator form) into another.
@@ -391,6 +394,8 @@ __global__ void __launch_bounds__(kThreads, TDG_MINB) k_group(const GroupK G, co
     const SmemView V = smem_setup<MODE>(G, sm);
     const int64_t tile = (int64_t)kThreads * kItems;
     for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
+        const int64_t nb = base + (int64_t)gridDim.x * tile;        // this CTA's next tile
+        prefetch_rows(G.pf, nb, nb + tile < n ? nb + tile : n);
         int64_t rp[kItems], rb[kItems];
         bool m[kItems];
 #pragma unroll
@@ -502,6 +507,8 @@ __global__ void __launch_bounds__(kThreads, TDG_MINB) k_payload_probe(const Grou
     const SmemView V = smem_setup<MODE>(G, sm);
     const int64_t tile = (int64_t)kThreads * kItems;
     for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
+        const int64_t nb = base + (int64_t)gridDim.x * tile;        // this CTA's next tile
+        prefetch_rows(G.pf, nb, nb + tile < n ? nb + tile : n);
         int64_t rp[kItems], rb[kItems], kv[kItems], slot[kItems];
         bool m[kItems];
 #pragma unroll
@@ -891,9 +898,26 @@ static tdg_status launch_sample(const GroupK& G, const Pred& P, const tdg_expr& 
     return launch_status();
 }
 
+// Streamed (row-indexed, probe-side) columns of a launch, for L2 prefetch.
+static void set_prefetch(GroupK& G, const Pred& P, const tdg_expr& prog, int pk, const JoinK* J) {
+    memset(&G.pf, 0, sizeof(G.pf));
+    if (pk == 1)
+        for (int i = 0; i < P.n; i++) pf_add(G.pf, P.t[i].col);
+    if (pk == 2)
+        for (int i = 0; i < prog.n_cols; i++) pf_add(G.pf, prog.cols[i]);
+    if (J)
+        for (int k = 0; k < J->nk; k++) pf_add(G.pf, J->lkeys[k]);
+    for (int k = 0; k < G.nk; k++)
+        if (!G.key[k].side) pf_add(G.pf, G.key[k]);
+    for (int a = 0; a < G.na; a++)
+        if (G.kind[a] != K_COUNT && !G.in[a].side) pf_add(G.pf, G.in[a]);
+}
+
 template <bool JOIN>
-static tdg_status dispatch(int pk, const GroupK& G, bool smem, const Pred& P, const tdg_expr& prog,
+static tdg_status dispatch(int pk, const GroupK& G0, bool smem, const Pred& P, const tdg_expr& prog,
                            const JoinK& J, int64_t n, cudaStream_t s, EventTimer& tm) {
+    GroupK G = G0;
+    set_prefetch(G, P, prog, pk, JOIN ? &J : nullptr);
     const int mode = G.method == TDG_GROUP_HASH ? 2 : (smem ? 0 : 1);
     tdg_status st = E_OK;
     if (G.hot_cap && n > 0) {
@@ -963,6 +987,7 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     const bool sm = p->smem != 0;
     const bool w8 = pk != 2 && group_w8(G, P, J);
     const size_t smem = sm ? smem_full_bytes(G.S, G.n_acc) : 0;
+    set_prefetch(G, P, prog, pk, J);
     EventTimer tm;
     tm.start(s);
 #define TDG_PL(PKV, SMV, PT, W)                                                                         \

@@ -44,6 +44,7 @@ typedef struct {
     int             n_bufs;
     cudaGraphExec_t exec;
     int             used;       /* LRU stamp */
+    uint64_t        launches;   /* kernels in the captured graph */
 } bcache_t;
 
 static bcache_t bcache[BATCH_CACHE];
@@ -250,10 +251,10 @@ static void autotune(tdb_ctx* c, const tdg_batch_desc* d, int64_t* tile, int32_t
     memset(&scratch, 0, sizeof(scratch));
     if (tdg_batch_plan_make(d, 4096, 0, &scratch.plan) || alloc_outputs(&scratch)) { bcache_drop(&scratch); return; }
     static const int64_t tiles[] = {4096, 16384, 65536};
-    static const int32_t ctass[] = {0, 2, 4};
+    static const int32_t ctass[] = {0, 1, 2, 4};   /* 1 and 2: large shared-memory modes */
     float best = -1;
     for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++) {
+        for (int j = 0; j < 4; j++) {
             float ms = time_config(c, d, tiles[i], ctass[j], &scratch);
             if (ms > 0 && (best < 0 || ms < best)) { best = ms; *tile = tiles[i]; *ctas = ctass[j]; }
         }
@@ -325,7 +326,9 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
         cudaGraph_t graph = NULL;
         cudaStream_t s = (cudaStream_t)c.stream;
         if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            uint64_t l0 = tdg_launch_count();
             int rs = tdg_batch_run(&e->plan, e->ws, &e->out, c.stream);
+            e->launches = tdg_launch_count() - l0;
             if (cudaStreamEndCapture(s, &graph) == cudaSuccess && !rs && graph) {
                 if (cudaGraphInstantiate(&e->exec, graph, 0) != cudaSuccess) e->exec = NULL;
             }
@@ -338,6 +341,7 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
     tdb_note_kernel();
     if (e->exec && !tdg_timing_enabled()) {   /* timing runs the kernels directly */
         if (cudaGraphLaunch(e->exec, (cudaStream_t)c.stream) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; goto done; }
+        tdg_count_launches(e->launches);
     } else if ((st = tdg_batch_run(&e->plan, e->ws, &e->out, c.stream))) {
         goto done;
     }
