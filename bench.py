@@ -306,7 +306,144 @@ def batch_main(args, td, L, rank, world, local, barrier, max_over_ranks):
 BATCH_REF_QUERIES = 512
 
 
+# ---- served mix (request loop over resident tables) ------------------------------------
+
+def serve_main(args, td, L, rank, world, local, barrier, max_over_ranks):
+    """Poisson arrivals at 2000 q/s of the served mix over resident tables:
+    70% filter + group-by on the 200M-row Zipf table, 30% filter + join +
+    group-by on the 10M / 100M-row join tables, each over a random row range
+    of 100K..50M rows.  The same trace runs through a td_server with 8 slots
+    and with 1 slot (one query at a time), open loop (requests submitted at
+    their arrival times) and closed loop (all submitted at once: throughput
+    at saturation)."""
+    import numpy as np
+    import torch
+    from teide_b200 import serve, workloads
+    scale = args.scale
+    n_group, n_probe = int(200_000_000 * scale), int(100_000_000 * scale)
+    c2 = workloads.config2(n=n_group, seed=2 + 1000 * rank, device="cuda")
+    b, p = workloads.config3(n_probe=n_probe, seed=3 + 1000 * rank, device="cuda")
+    tg, tb, tp = td.table(c2), td.table(b), td.table(p)
+    del c2, b, p
+    torch.cuda.empty_cache()
+    for t in (tg, tb, tp):
+        st = L.td_gpu_pin(t)
+        if st:
+            raise RuntimeError(f"td_gpu_pin failed: {st}")
+    n_req = args.requests
+    raw = workloads.config5_requests(n_req, rate=2000.0, seed=5 + rank, group_rows=n_group, probe_rows=n_probe,
+                                     len_range=(100_000, max(100_000, int(50_000_000 * scale))))
+    reqs = [serve.Request(*r) for r in raw]
+    serve.build(td, reqs, tg, tb, tp)
+    alg = sum(24 * r.n + (16 * 10_000_000 if r.kind == "join" else 0) for r in reqs)
+    warm = reqs[:min(len(reqs), 32)]
+    out = {}
+    clk = Clocks(local).__enter__()
+    tc0 = time.monotonic()
+    for name, slots in (("served", args.slots), ("one_at_a_time", 1)):
+        with serve.Server(td, slots=slots) as srv:
+            serve.run_closed(srv, warm)                      # warm-up: caches, pinned result blocks
+            barrier()
+            lat, makespan, _ = serve.run_open_loop(srv, reqs)
+            closed = serve.run_closed(srv, reqs)
+            st = srv.stats()
+        out[name] = {"qps": len(reqs) / makespan, "p50_ms": float(np.percentile(lat, 50) * 1e3),
+                     "p99_ms": float(np.percentile(lat, 99) * 1e3), "makespan_s": makespan,
+                     "closed_qps": len(reqs) / closed, "closed_s": closed,
+                     "peak_in_flight": int(st.peak_in_flight), "slots": slots}
+    tc1 = time.monotonic()
+    time.sleep(0.3)
+    clk.__exit__(None, None, None)
+    serve.release(td, reqs)
+    for t in (tg, tb, tp):
+        L.td_gpu_unpin(t)
+        td.release(t)
+    sv, one = out["served"], out["one_at_a_time"]
+    value = max_over_ranks(1.0 / sv["qps"])
+    value = world / value
+    hbm, peak_kind = peaks()
+    achieved = alg / sv["closed_s"] / 1e9
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
+        _, q, desc = reference_sample("serve", 0)
+        secs = q()
+        cpu = {"value": SERVE_REF_REQUESTS / secs, "unit": "queries/s", "cores": os.cpu_count(),
+               "kind": "reference", "sample": desc}
+    return {
+        "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": 1,
+        "warmup": len(warm), "ms_per_step": sv["makespan_s"] * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+        "config": {"workload": "serve", "requests": len(reqs), "arrivals": "Poisson 2000 q/s",
+                   "mix": "70% filter+group (200M-row Zipf table), 30% filter+join+group (10M/100M)",
+                   "range_rows": "U[100K, 50M]", "tables": "resident in HBM (td_gpu_pin), loaded once",
+                   "slots": args.slots, "admission": "FIFO by estimated device bytes vs 90% of free HBM",
+                   "algorithmic_bytes": alg, "scale": scale, "timing": "host CLOCK_MONOTONIC per request",
+                   "parallelism": f"replicas{world}"},
+        "served": sv, "plain": one,
+        "speedup_open_loop": sv["qps"] / one["qps"], "speedup_closed_loop": sv["closed_qps"] / one["closed_qps"],
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "kernel": "whole served pipeline (closed loop)", "peak_source": peak_kind},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
+                "note": "tables are resident by design; results are host td_t tables"},
+        "gpu_launches": None,
+        "clocks": clk.summary(tc0, tc1),
+        "cpu_baseline": cpu,
+    }
+
+
 # ---- CPU reference ---------------------------------------------------------------------
+
+SERVE_REF_ROWS, SERVE_REF_REQUESTS = 60_000_000, 16
+
+
+def serve_reference(td):
+    """Teide one query at a time over a sample of the served mix: 16 requests
+    drawn like the GPU trace (ranges U[100K, 50M]) from 60M-row tables of the
+    same shapes.  Each range is copied into its own table before the clock
+    starts; the query runs Teide's filter -> group and filter -> join -> group
+    graphs.  The returned callable gives the seconds spent in queries."""
+    from gpu_pipelines import const
+    from teide_b200 import serve as sv
+    from teide_b200 import workloads
+    c2 = workloads.config2(n=SERVE_REF_ROWS, seed=32)
+    b, p = workloads.config3(n_build=10_000_000, n_probe=SERVE_REF_ROWS, seed=33)
+    raw = workloads.config5_requests(SERVE_REF_REQUESTS, seed=55, group_rows=SERVE_REF_ROWS,
+                                     probe_rows=SERVE_REF_ROWS)
+    bt = td.table(b)
+
+    def run(graph_tbl, build):
+        g = td.graph(graph_tbl)
+        try:
+            return g.execute(build(g))
+        finally:
+            g.free()
+
+    def q():
+        total = 0.0
+        for kind, off, n, thr, _ in raw:
+            src = c2 if kind == "group" else p
+            tt = td.table({k: v[off:off + n] for k, v in src.items()})
+            t0 = time.perf_counter()
+            col = "v1" if kind == "group" else "qty"
+            ft = run(tt, lambda g: g.filter(g.const_table(tt), g.op("gt", g.scan(col), const(g, thr))))
+            if kind == "group":
+                r = run(ft, lambda g: g.group([g.scan("key")], [a for a, _ in sv.GROUP_AGGS],
+                                              [g.scan(x) for _, x in sv.GROUP_AGGS]))
+            else:
+                jt = run(ft, lambda g: g.join(g.const_table(ft), [g.scan("fk")], g.const_table(bt),
+                                              [g.scan("pk")], 0))
+                r = run(jt, lambda g: g.group([g.scan("cat")], [a for a, _ in sv.JOIN_AGGS],
+                                              [g.scan(x) for _, x in sv.JOIN_AGGS]))
+                td.release(jt)
+            td.release(r)
+            td.release(ft)
+            total += time.perf_counter() - t0
+            td.release(tt)
+        return total
+    desc = (f"{SERVE_REF_REQUESTS} requests of the served mix over 60M-row tables of the same shapes, "
+            "one at a time (filter graph then group / join + group graphs)")
+    return td, q, desc
+
 
 def reference_sample(workload, scale_rows):
     """Teide's CPU engine on a bounded sample of the workload: returns
@@ -315,6 +452,8 @@ def reference_sample(workload, scale_rows):
     from teide_b200 import workloads
     from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM, Td
     td = Td(REF_LIB)
+    if workload == "serve":
+        return serve_reference(td)
     if workload == "batch":
         b = Batch(td, first=BATCH_REF_QUERIES)
         desc = (f"the first {b.n} of the 4096 queries ({b.rows / 1e6:.1f}M rows), one td_execute each")
@@ -352,16 +491,21 @@ def reference_arm(args):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libteide_ref.so not built"}))
         return
     rows = {"join_group": 10_000_000, "group_radix": 20_000_000, "readme_group": 10_000_000,
-            "batch": BATCH_REF_QUERIES}[args.workload]
+            "batch": BATCH_REF_QUERIES, "serve": SERVE_REF_REQUESTS}[args.workload]
     td, q, desc = reference_sample(args.workload, rows)
-    for _ in range(args.warmup):
-        q()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        q()
-    dt = (time.perf_counter() - t0) / args.steps
+    if args.workload == "serve":                 # q() reports its own query seconds
+        for _ in range(min(args.warmup, 1)):
+            q()
+        dt = sum(q() for _ in range(max(1, min(args.steps, 2)))) / max(1, min(args.steps, 2))
+    else:
+        for _ in range(args.warmup):
+            q()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            q()
+        dt = (time.perf_counter() - t0) / args.steps
     v = rows / dt
-    unit = "queries/s" if args.workload == "batch" else "rows/s"
+    unit = "queries/s" if args.workload in ("batch", "serve") else "rows/s"
     cores = os.cpu_count()
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": unit, "n_gpus": args.gpus,
@@ -381,11 +525,13 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="teide_b200", choices=["teide_b200", "reference"])
-    ap.add_argument("--workload", default="join_group", choices=["join_group", "group_radix", "readme_group", "batch"])
+    ap.add_argument("--workload", default="join_group", choices=["join_group", "group_radix", "readme_group", "batch", "serve"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-table (upload) pass")
     ap.add_argument("--no-plain", action="store_true", help="batch: skip the one-query-per-launch pass")
+    ap.add_argument("--requests", type=int, default=2000, help="serve: requests in the trace")
+    ap.add_argument("--slots", type=int, default=8, help="serve: queries in flight at once")
     ap.add_argument("--scale", type=float, default=1.0,
                     help="fraction of the workload size (smaller cases for profiler captures)")
     args = ap.parse_args()
@@ -427,8 +573,9 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    if args.workload == "batch":
-        line = batch_main(args, td, L, rank, world, local, barrier, max_over_ranks)
+    if args.workload in ("batch", "serve"):
+        fn = batch_main if args.workload == "batch" else serve_main
+        line = fn(args, td, L, rank, world, local, barrier, max_over_ranks)
         if rank == 0:
             print(json.dumps(line))
         if dist:

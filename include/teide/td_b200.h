@@ -61,6 +61,55 @@ void     td_gpu_trim(void);
 td_t*    td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n);
 void     td_gpu_batch_cache_clear(void);
 
+/* ---- serving: a request loop over resident tables ------------------------------
+ * td_server_new starts `slots` worker threads.  Each pulls submitted requests
+ * in arrival order and runs td_execute on its own CUDA stream, so up to
+ * `slots` queries are in flight on the GPU at once and a request that arrives
+ * while others run starts as soon as a slot frees up and its estimated device
+ * bytes fit in the budget (hbm_budget, or 0 for 90% of the GPU's free memory
+ * when the server starts).  The queue head is never bypassed; a request that
+ * alone exceeds the budget runs when nothing else is in flight.
+ *
+ * Each submitted graph must stay alive, and must not be executed elsewhere,
+ * until td_server_wait has returned its result.  est_bytes = 0 asks
+ * td_server_estimate.  td_server_submit returns a ticket >= 0, or a negated
+ * td_err_t (TD_ERR_RANGE when queue_cap requests are already outstanding).
+ * td_server_wait blocks until that ticket's result is ready and hands it to
+ * the caller (release it with td_release); the times are CLOCK_MONOTONIC
+ * nanoseconds.  td_server_free finishes every queued request, then stops. */
+typedef struct td_server td_server_t;
+
+typedef struct {
+    int64_t submit_ns;          /* td_server_submit */
+    int64_t start_ns;           /* a worker started td_execute */
+    int64_t end_ns;             /* the result table was complete on the host */
+    int64_t est_bytes;          /* device bytes reserved for it while it ran */
+    int32_t status;             /* td_err_t of the execution */
+    int32_t in_flight_at_start; /* queries running (itself included) when it started */
+} td_server_timing_t;
+
+typedef struct {
+    uint64_t completed;
+    int64_t  queued;            /* submitted, not yet started */
+    int32_t  in_flight;
+    int32_t  peak_in_flight;
+    int32_t  slots;
+    int32_t  pad;
+    uint64_t budget_bytes;
+    uint64_t reserved_bytes;
+    uint64_t peak_reserved_bytes;
+} td_server_stats_t;
+
+td_server_t* td_server_new(int32_t slots, size_t hbm_budget, int64_t queue_cap);
+int64_t      td_server_submit(td_server_t* s, td_graph_t* g, td_op_t* root, size_t est_bytes);
+td_t*        td_server_wait(td_server_t* s, int64_t ticket, td_server_timing_t* timing);
+void         td_server_stats(td_server_t* s, td_server_stats_t* out);
+void         td_server_free(td_server_t* s);
+/* Device bytes a query may need beyond resident columns: uploads of columns
+ * that are not resident plus a per-row scratch bound (64 bytes per row of the
+ * largest input table, 16 per row of the others). */
+size_t       td_server_estimate(td_graph_t* g, td_op_t* root);
+
 #ifdef __cplusplus
 }
 #endif

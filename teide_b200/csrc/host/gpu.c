@@ -137,7 +137,11 @@ int td_gpu_device_count(void) {
     return gpu_probe < 0 ? 0 : gpu_probe;
 }
 
+static int gpu_dev;                       /* the executor's device */
+static _Thread_local int tls_dev_set;      /* this thread has made it current */
+
 int tdb_gpu_ensure(void) {
+    if (tls_dev_set) return TD_OK;
     if (!tdb_gpu_available()) return TD_ERR_IO;
     pthread_mutex_lock(&mu);
     if (!gpu_ready) {
@@ -145,9 +149,15 @@ int tdb_gpu_ensure(void) {
         int dev = env ? atoi(env) : -1;
         if (dev >= 0) cudaSetDevice(dev);
         if (cudaFree(0) != cudaSuccess) { cudaGetLastError(); pthread_mutex_unlock(&mu); return TD_ERR_IO; }
+        cudaGetDevice(&gpu_dev);
         gpu_ready = 1;
     }
+    const int dev = gpu_dev;
     pthread_mutex_unlock(&mu);
+    /* every thread that calls in (server workers included) works on the same
+     * device as the first one, whatever its own current device was */
+    if (cudaSetDevice(dev) != cudaSuccess) { cudaGetLastError(); return TD_ERR_IO; }
+    tls_dev_set = 1;
     return TD_OK;
 }
 
@@ -163,15 +173,70 @@ typedef struct {
 
 static mirror_t* mirrors; static int n_mir, cap_mir;
 
-static int find_mirror_locked(td_t* v) {
-    uint64_t s = tdb_block_serial(v);
-    for (int i = 0; i < n_mir; i++) if (mirrors[i].host == v && mirrors[i].serial == s) return i;
-    return -1;
+/* Hash index host pointer -> mirror slot (open addressing, -1 = empty).
+ * Thousands of resident columns are common (one small table per batched
+ * query), and every td_free asks whether its vector has a mirror, so the
+ * lookup must not scan.  Inserts update the index in place; drops (rare)
+ * mark it stale and the next lookup rebuilds it. */
+static int* mh; static uint32_t mh_cap; static int mh_valid;
+
+static uint32_t mh_slot(const td_t* v, uint32_t cap) {
+    uint64_t x = (uint64_t)(uintptr_t)v;
+    x ^= x >> 29;
+    x *= 0x9E3779B97F4A7C15ull;
+    return (uint32_t)(x >> 32) & (cap - 1);
 }
+
+static void mh_insert(int i) {
+    uint32_t h = mh_slot(mirrors[i].host, mh_cap);
+    while (mh[h] >= 0) h = (h + 1) & (mh_cap - 1);
+    mh[h] = i;
+}
+
+static void mh_rebuild_locked(void) {
+    uint32_t cap = 64;
+    while (cap < (uint32_t)n_mir * 2 + 2) cap <<= 1;
+    if (cap != mh_cap) {
+        free(mh);
+        mh = malloc((size_t)cap * sizeof(int));
+        mh_cap = mh ? cap : 0;
+    }
+    mh_valid = 0;
+    if (!mh) return;
+    memset(mh, 0xFF, (size_t)mh_cap * sizeof(int));
+    for (int i = 0; i < n_mir; i++) mh_insert(i);
+    mh_valid = 1;
+}
+
+/* after mirrors[n_mir - 1] was appended */
+static void mh_added_locked(void) {
+    if (mh_valid && mh_cap >= (uint32_t)n_mir * 2 + 2) mh_insert(n_mir - 1);
+    else mh_valid = 0;
+}
+
+/* Slot of v's mirror; any_serial also matches a mirror of an earlier block at v. */
+static int lookup_locked(td_t* v, int any_serial) {
+    if (!n_mir) return -1;
+    const uint64_t s = any_serial ? 0 : tdb_block_serial(v);
+    if (!mh_valid || mh_cap < (uint32_t)n_mir * 2 + 2) mh_rebuild_locked();
+    if (!mh_valid) {
+        for (int i = 0; i < n_mir; i++)
+            if (mirrors[i].host == v && (any_serial || mirrors[i].serial == s)) return i;
+        return -1;
+    }
+    for (uint32_t h = mh_slot(v, mh_cap);; h = (h + 1) & (mh_cap - 1)) {
+        const int i = mh[h];
+        if (i < 0) return -1;
+        if (mirrors[i].host == v && (any_serial || mirrors[i].serial == s)) return i;
+    }
+}
+
+static int find_mirror_locked(td_t* v) { return lookup_locked(v, 0); }
 
 static void drop_mirror_locked(int i) {
     void* p = mirrors[i].dc.dptr;
     mirrors[i] = mirrors[--n_mir];
+    mh_valid = 0;
     pthread_mutex_unlock(&mu);
     arena_free(p);
     pthread_mutex_lock(&mu);
@@ -180,8 +245,17 @@ static void drop_mirror_locked(int i) {
 void tdb_mirror_forget(td_t* v) {
     if (!v || TD_IS_ERR(v) || !n_mir) return;
     pthread_mutex_lock(&mu);
-    for (int i = n_mir - 1; i >= 0; i--) if (mirrors[i].host == v) drop_mirror_locked(i);
+    for (int i = lookup_locked(v, 1); i >= 0; i = lookup_locked(v, 1)) drop_mirror_locked(i);
     pthread_mutex_unlock(&mu);
+}
+
+int tdb_col_resident(td_t* col) {
+    if (col && !TD_IS_ERR(col) && (col->attrs & TD_ATTR_SLICE)) col = col->slice_parent;
+    if (!col || TD_IS_ERR(col)) return 0;
+    pthread_mutex_lock(&mu);
+    const int r = find_mirror_locked(col) >= 0;
+    pthread_mutex_unlock(&mu);
+    return r;
 }
 
 void tdb_gpu_on_free(td_t* v, tdb_block_prefix* p) {
@@ -435,6 +509,7 @@ void tdb_adopt_mirror(tdb_ctx* c, td_t* host, void* dptr) {
     memset(&dc, 0, sizeof(dc));
     dc.dptr = dptr; dc.len = host->len; dc.type = host->type; dc.attrs = host->attrs;
     mirrors[n_mir++] = (mirror_t){ host, tdb_block_serial(host), dc, col_bytes(host) };
+    mh_added_locked();
     pthread_mutex_unlock(&mu);
     c->tmp[k] = c->tmp[--c->n_tmp];
 }
@@ -466,6 +541,7 @@ td_err_t td_gpu_pin(td_t* tbl) {
             mirrors = nm; cap_mir = ncap;
         }
         mirrors[n_mir++] = (mirror_t){ col, tdb_block_serial(col), dc, col_bytes(col) };
+        mh_added_locked();
         pthread_mutex_unlock(&mu);
     }
     tdb_ctx_end(&c);

@@ -90,5 +90,7 @@ extern _Atomic(int) tdb_cancel_flag;
 
 /* ---- executor ------------------------------------------------------------------ */
 td_t* tdb_exec(td_graph_t* g, td_op_t* root);
+/* 1 when the column (or a slice's parent) has a resident device copy. */
+int   tdb_col_resident(td_t* col);
 
 #endif

@@ -116,3 +116,24 @@ def config4_query(rows, k, seed):
     """One batched query's table: key U[0,K), val U[0,1)."""
     r = np.random.default_rng(seed)
     return {"key": r.integers(0, k, rows, dtype=np.int64), "val": r.random(rows)}
+
+
+def config5_requests(n, rate=2000.0, seed=5, group_rows=200_000_000, probe_rows=100_000_000,
+                     join_frac=0.3, len_range=(100_000, 50_000_000)):
+    """The served mix: n requests with Poisson arrivals at `rate` per second.
+    70% filter + group-by over the group table (v1 > t, t ~ U[-1e6, 1e6]),
+    30% filter + join + group-by over the probe table (qty > t, t ~ U{1..100});
+    each reads a contiguous row range [off, off + len) with len ~ U[100K, 50M]
+    (clipped to the table) and off uniform over the valid starts.
+    Returns a list of (kind, off, len, threshold, arrival_seconds)."""
+    r = np.random.default_rng(seed)
+    arrivals = np.cumsum(r.exponential(1.0 / rate, n))
+    out = []
+    for i in range(n):
+        join = r.random() < join_frac
+        rows = probe_rows if join else group_rows
+        ln = int(min(r.integers(len_range[0], len_range[1] + 1), rows))
+        off = int(r.integers(0, rows - ln + 1))
+        t = int(r.integers(1, 101)) if join else int(r.integers(-1_000_000, 1_000_001))
+        out.append(("join" if join else "group", off, ln, t, float(arrivals[i])))
+    return out
