@@ -317,6 +317,11 @@ __device__ __forceinline__ void accumulate_at(const GroupK& G, const SmemView& V
         hidx[i] = -1;
         if (MODE == 0) hidx[i] = ok[i] ? (int)slot[i] : -1;
         else if (V.n_hot && ok[i]) hidx[i] = hot_find(V, slot[i]);
+        // a cold record's line is fetched now, so the N rows' DRAM round trips
+        // overlap instead of queueing behind the MIN/MAX filter reads below
+        if (MODE != 0 && ok[i] && hidx[i] < 0)
+            asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tprefetch.global.L2 [g];\n\t}"
+                         :: "l"(grec(G, slot[i])));
         if (ok[i]) {
             if (hidx[i] >= 0) atomicAdd(&V.cnt[hidx[i]], 1u);
             else atomicAdd(grec(G, slot[i]), 1ULL);
