@@ -126,9 +126,20 @@ def make_tables(td, workload, rank, device, scale=1.0):
     return {"t": t}, len(c["flag"]), 24 * len(c["flag"]), 24 * len(c["flag"])
 
 
-def run_query(td, workload, tabs):
+def run_query(td, workload, tabs, world=1):
+    """One step.  With several ranks every rank runs its shard and the partial
+    groups are merged across ranks (teide_b200.shard) inside the step."""
     from gpu_pipelines import fused_join_group, readme_group
     from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
+    if world > 1:
+        from teide_b200 import shard
+        if workload == "join_group":
+            return shard.sharded_join_group(td, tabs["build"], tabs["probe"], ("qty", "gt", 10), "fk", "pk",
+                                            ["cat"], [(OP_SUM, "price"), (OP_COUNT, "price")])
+        if workload == "group_radix":
+            return shard.sharded_group(td, tabs["t"], ["key"], [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"),
+                                                               (OP_MAX, "v1"), (OP_AVG, "v2")], pred=("v1", "gt", 0))
+        return shard.sharded_group(td, tabs["t"], ["region"], [(OP_SUM, "amount")], pred=("flag", "eq", 0))
     if workload == "join_group":
         return fused_join_group(td, tabs["build"], tabs["probe"], ("qty", "gt", 10), "fk", "pk", ["cat"],
                                 [(OP_SUM, "price"), (OP_COUNT, "price")], as_dict=False)
@@ -593,7 +604,7 @@ def main():
             raise RuntimeError(f"td_gpu_pin failed: {st}")
     clk = Clocks(local).__enter__()
     for _ in range(args.warmup):
-        run_query(td, args.workload, tabs)
+        run_query(td, args.workload, tabs, world)
     barrier()
     l0 = L.tdg_launch_count()
     main_ms, build_ms = [], []
@@ -601,7 +612,7 @@ def main():
     tc0 = time.monotonic()
     ev0.record()
     for _ in range(args.steps):
-        run_query(td, args.workload, tabs)
+        run_query(td, args.workload, tabs, world)
         main_ms.append(L.tdg_last_main_ms())
         build_ms.append(L.tdg_last_build_ms())
     ev1.record()
@@ -623,11 +634,11 @@ def main():
             L.td_gpu_unpin(t)
         L.td_gpu_trim()
         e2e_steps = args.e2e_steps or args.steps
-        run_query(td, args.workload, tabs)          # page-locks the host columns once
+        run_query(td, args.workload, tabs, world)          # page-locks the host columns once
         barrier()
         ev0.record()
         for _ in range(e2e_steps):
-            run_query(td, args.workload, tabs)
+            run_query(td, args.workload, tabs, world)
         ev1.record()
         torch.cuda.synchronize()
         e2e_elapsed = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
@@ -646,7 +657,10 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
         "config": {"workload": args.workload, "rows_per_gpu_per_step": rows,
                    "algorithmic_bytes_per_step": alg_bytes, "l2": "inputs larger than L2 (no flush)",
-                   "tables": "resident in HBM (td_gpu_pin)", "parallelism": f"replicas{world}",
+                   "tables": "resident in HBM (td_gpu_pin)",
+                   "parallelism": f"shards{world}" if world > 1 else "single",
+                   "exchange": ("partial groups merged across ranks (all-gather, or all-to-all by key hash "
+                                "when large) inside every step") if world > 1 else None,
                    "scale": args.scale},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": profile_traffic(prof),

@@ -100,6 +100,10 @@ def table_slice(td, tbl, off, n):
     return out
 
 
+def _const(g, k):
+    return g.f64(k) if isinstance(k, float) else g.i64(k)
+
+
 GROUP_AGGS = [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")]
 JOIN_AGGS = [(OP_SUM, "price"), (OP_COUNT, "price")]
 
