@@ -1,0 +1,103 @@
+"""Failure paths on the GPU, made on the host: the device-memory limit turns
+an allocation failure into TD_ERR_OOM and the context stays usable; td_cancel
+before td_execute is cleared by it (Teide resets the flag on entry), and a
+cancel racing running queries yields either a correct result or
+TD_ERR_CANCEL, never a wrong one."""
+import ctypes as C
+import threading
+
+import numpy as np
+import pytest
+
+import oracle
+from gpu_pipelines import readme_group
+from teide_b200.td import OP_SUM, TdError
+
+pytestmark = pytest.mark.gpu
+
+TD_ERR_OOM, TD_ERR_CANCEL = 1, 11
+
+
+def _table(gpu, n=2_000_000, seed=9):
+    r = np.random.default_rng(seed)
+    d = {"flag": r.integers(0, 4, n, dtype=np.int64), "region": r.integers(0, 64, n, dtype=np.int64),
+         "amount": r.random(n) * 1000}
+    return d, gpu.table(d)
+
+
+def _want(d):
+    return oracle.group({"region": d["region"]}, [(OP_SUM, "amount", d["amount"])], mask=d["flag"] == 0)
+
+
+def _stats(gpu):
+    class St(C.Structure):
+        _fields_ = [("h2d", C.c_uint64), ("d2h", C.c_uint64), ("calls", C.c_uint64), ("live", C.c_uint64),
+                    ("peak", C.c_uint64), ("gm", C.c_int32), ("jm", C.c_int32), ("fused", C.c_int32),
+                    ("pad", C.c_int32)]
+    s = St()
+    gpu.lib.td_gpu_last_stats(C.byref(s))
+    return s
+
+
+def test_memory_limit_gives_oom_and_recovers(gpu):
+    d, t = _table(gpu)
+    L = gpu.lib
+    L.td_gpu_set_mem_limit.argtypes = [C.c_size_t]
+    try:
+        readme_group(gpu, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])   # warm caches
+        live0 = _stats(gpu).live                      # device bytes held after a good query
+        L.td_gpu_trim()
+        L.td_gpu_set_mem_limit(64 << 10)              # far below the 48 MB upload
+        with pytest.raises(TdError) as e:
+            readme_group(gpu, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+        assert e.value.code == TD_ERR_OOM
+        L.td_gpu_set_mem_limit(0)
+        got = readme_group(gpu, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+        want = _want(d)
+        assert np.array_equal(got["region"], want["region"])
+        assert np.allclose(got["amount_sum"], want["amount_sum"], rtol=1e-12)
+        assert _stats(gpu).live == live0              # the failed query left nothing allocated
+    finally:
+        L.td_gpu_set_mem_limit(0)
+        gpu.release(t)
+
+
+def test_cancel_before_execute_is_cleared(gpu):
+    d, t = _table(gpu, n=300_000)
+    try:
+        gpu.lib.td_cancel()
+        got = readme_group(gpu, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+        assert np.array_equal(got["region"], _want(d)["region"])
+    finally:
+        gpu.release(t)
+
+
+def test_cancel_racing_queries_never_corrupts(gpu):
+    d, t = _table(gpu)
+    want = _want(d)
+    stop = threading.Event()
+
+    def canceller():
+        while not stop.is_set():
+            gpu.lib.td_cancel()
+
+    th = threading.Thread(target=canceller)
+    th.start()
+    outcomes = []
+    try:
+        for _ in range(30):
+            try:
+                got = readme_group(gpu, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+                assert np.array_equal(got["region"], want["region"])
+                assert np.allclose(got["amount_sum"], want["amount_sum"], rtol=1e-12)
+                outcomes.append("ok")
+            except TdError as e:
+                assert e.code == TD_ERR_CANCEL
+                outcomes.append("cancel")
+    finally:
+        stop.set()
+        th.join()
+    got = readme_group(gpu, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])   # usable afterwards
+    assert np.array_equal(got["region"], want["region"])
+    gpu.release(t)
+    assert len(outcomes) == 30
