@@ -1,0 +1,84 @@
+"""The fused join probe's vector form and its fallbacks: odd probe lengths
+(the last pair is half full), a probe view starting at an odd row (columns
+not 16-byte aligned: the general kernel runs), COUNT only, no filter and two
+filter terms -- each against the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from gpu_pipelines import const
+from teide_b200 import serve, workloads
+from teide_b200.td import OP_COUNT, OP_MAX, OP_SUM
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(td, build_t, probe_t, preds, aggs):
+    g = td.graph(None)
+    try:
+        p = None
+        for c, op, k in preds:
+            q = g.op(op, g.scan(c), const(g, k))
+            p = q if p is None else g.op("and", p, q)
+        left = g.const_table(probe_t) if p is None else g.filter(g.const_table(probe_t), p)
+        g.join(left, [g.scan("fk")], g.const_table(build_t), [g.scan("pk")], 0)
+        r = td.check(td.lib.td_execute(g.g, g.group([g.scan("cat")], [a for a, _ in aggs],
+                                                    [g.scan(n) for _, n in aggs])), "execute")
+    finally:
+        g.free()
+    out = td.table_dict(r)
+    td.release(r)
+    return out
+
+
+def _want(b, p, preds, aggs):
+    m = np.ones(len(p["fk"]), bool)
+    for c, op, k in preds:
+        m &= oracle.compare(op, p[c], k)
+    j = oracle.join(p, b, ["fk"], ["pk"], 0, lmask=m)
+    return oracle.group({"cat": j["cat"]}, [(op, n, None if op == OP_COUNT else j[n]) for op, n in aggs])
+
+
+def _same(got, want):
+    assert list(got) == list(want)
+    for k in want:
+        if want[k].dtype.kind == "f":
+            assert np.allclose(got[k], want[k], rtol=1e-12, atol=1e-9), k
+        else:
+            assert np.array_equal(got[k], want[k]), k
+
+
+CASES = [
+    ([("qty", "gt", 10)], [(OP_SUM, "price"), (OP_COUNT, "price")]),
+    ([], [(OP_COUNT, "price")]),
+    ([], [(OP_SUM, "price"), (OP_MAX, "price")]),
+    ([("qty", "gt", 10), ("qty", "lt", 90)], [(OP_COUNT, "qty")]),
+    ([("qty", "gt", 10), ("price", "lt", 300.0)], [(OP_SUM, "price"), (OP_COUNT, "price")]),
+    ([("qty", "ge", 50)], [(OP_SUM, "qty"), (OP_MAX, "qty"), (OP_COUNT, "qty")]),
+]
+
+
+@pytest.mark.parametrize("preds,aggs", CASES)
+@pytest.mark.parametrize("n_probe", [300_001, 300_000])
+def test_vector_probe_shapes(gpu, preds, aggs, n_probe):
+    b, p = workloads.config3(n_build=50_000, n_probe=n_probe, seed=81)
+    bt, pt = gpu.table(b), gpu.table(p)
+    try:
+        _same(_run(gpu, bt, pt, preds, aggs), _want(b, p, preds, aggs))
+    finally:
+        gpu.release(bt)
+        gpu.release(pt)
+
+
+def test_unaligned_probe_view_falls_back(gpu):
+    b, p = workloads.config3(n_build=50_000, n_probe=200_000, seed=82)
+    bt, pt = gpu.table(b), gpu.table(p)
+    view = serve.table_slice(gpu, pt, 1, 150_001)          # starts 8 bytes into each column
+    try:
+        preds, aggs = CASES[0]
+        sub = {k: v[1:150_002] for k, v in p.items()}
+        _same(_run(gpu, bt, view, preds, aggs), _want(b, sub, preds, aggs))
+    finally:
+        gpu.release(view)
+        gpu.release(bt)
+        gpu.release(pt)
