@@ -362,6 +362,14 @@ void set_last_main_ms(float ms);
 void set_last_build_ms(float ms);
 
 // While alive, this thread's tdg calls record no timing events.
+// While alive, this thread's tdg calls make no allocating CUDA call (no
+// page-locked status buffers either): the entry points that allocate nothing.
+struct ThreadNoAlloc {
+    ThreadNoAlloc();
+    ~ThreadNoAlloc();
+};
+bool no_alloc();
+
 struct ThreadTimingOff {
     ThreadTimingOff();
     ~ThreadTimingOff();

@@ -49,6 +49,11 @@ static std::atomic<int> g_timing{0};
 static std::atomic<float> g_main_ms{0.f}, g_build_ms{0.f};
 
 static thread_local int t_timing_off = 0;
+static thread_local int t_no_alloc = 0;
+ThreadNoAlloc::ThreadNoAlloc() { t_no_alloc++; }
+ThreadNoAlloc::~ThreadNoAlloc() { t_no_alloc--; }
+bool no_alloc() { return t_no_alloc != 0; }
+
 ThreadTimingOff::ThreadTimingOff() { t_timing_off++; }
 ThreadTimingOff::~ThreadTimingOff() { t_timing_off--; }
 

@@ -770,6 +770,53 @@ __global__ void __launch_bounds__(kThreads) k_emit(const GroupK G, const OutK O,
     }
 }
 
+// Small group-bys (S <= kSmallEmit slots): one CTA counts, scans and emits in
+// slot order in a single launch.
+constexpr int64_t kSmallEmit = 65536;
+
+__device__ __forceinline__ void emit_one(const GroupK& G, const OutK& O, int64_t s, const unsigned long long* r,
+                                         unsigned long long c, int64_t o) {
+    for (int k = 0; k < G.nk; k++) {
+        int64_t v;
+        if (G.method == TDG_GROUP_DIRECT) v = G.kmin[k] + (s / G.stride[k]) % G.krange[k];
+        else v = G.ht.keys[(int64_t)k * G.S + s];
+        put_key(O.keys[k], O.kesz[k], o, v);
+    }
+    for (int a = 0; a < G.na; a++) {
+        const int kind = G.kind[a];
+        uint64_t res;
+        if (kind == K_COUNT) {
+            res = c;
+        } else {
+            const unsigned long long v = r[1 + G.ai[a]];
+            if (G.op[a] == A_AVG) {
+                const double sum = kind == K_SUM_F ? __longlong_as_double((long long)v) : (double)(long long)v;
+                res = (uint64_t)__double_as_longlong(sum / (double)c);
+            } else if (kind == K_MIN_F || kind == K_MAX_F) {
+                res = (uint64_t)__double_as_longlong(ord2f((long long)v));
+            } else {
+                res = v;
+            }
+        }
+        ((uint64_t*)O.aggs[a])[o] = res;
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_emit_small(const GroupK G, const OutK O, int64_t* d_total) {
+    __shared__ int red[32];
+    int64_t out = 0;
+    for (int64_t s0 = 0; s0 < G.S; s0 += blockDim.x) {
+        const int64_t s = s0 + threadIdx.x;
+        const unsigned long long* r = s < G.S ? grec(G, s) : nullptr;
+        const unsigned long long c = r ? r[0] : 0;
+        int tot;
+        const int pre = block_excl_scan(c ? 1 : 0, &tot, red);
+        if (c) emit_one(G, O, s, r, c, out + pre);
+        out += tot;
+    }
+    if (threadIdx.x == 0) *d_total = out;
+}
+
 __global__ void __launch_bounds__(1024) k_scan_counts_g(int64_t* counts, int64_t m, int64_t* d_total) {
     __shared__ long long part[1024];
     const int64_t per = (m + blockDim.x - 1) / blockDim.x;
@@ -964,13 +1011,16 @@ static tdg_status prepare(const GroupK& G, cudaStream_t s) {
     return launch_status();
 }
 
+// A few page-locked words per host thread for status read-backs.
+static int32_t* pinned_words() {
+    static thread_local int32_t* w = nullptr;
+    if (no_alloc()) return nullptr;
+    if (!w && cudaMallocHost((void**)&w, 64) != cudaSuccess) { cudaGetLastError(); w = nullptr; }
+    return w;
+}
+
 static tdg_status finish(const GroupK& G, const tdg_group_desc* d, void* ws, const tdg_group_out* out,
-                         cudaStream_t s) {
-    const Layout L = layout_of(G.S, G.n_acc, G.nk, G.method, G.hot_cap != 0);
-    int64_t* counts = (int64_t*)((char*)ws + L.emit);
-    const int64_t chunks = (G.S + kEmitChunk - 1) / kEmitChunk;
-    (note_launch(), k_emit_count<<<(unsigned)chunks, kThreads, 0, s>>>(G, counts));
-    (note_launch(), k_scan_counts_g<<<1, 1024, 0, s>>>(counts, chunks, out->d_n_groups));
+                         cudaStream_t s, int32_t* flag1 = nullptr) {
     OutK O;
     memset(&O, 0, sizeof(O));
     for (int k = 0; k < G.nk; k++) {
@@ -978,13 +1028,26 @@ static tdg_status finish(const GroupK& G, const tdg_group_desc* d, void* ws, con
         O.kesz[k] = elem_size(d->keys[k].type, d->keys[k].attrs);
     }
     for (int a = 0; a < G.na; a++) O.aggs[a] = out->aggs[a];
-    (note_launch(), k_emit<<<(unsigned)chunks, kThreads, 0, s>>>(G, O, counts));
+    if (G.S <= kSmallEmit) {
+        (note_launch(), k_emit_small<<<1, 1024, 0, s>>>(G, O, out->d_n_groups));
+    } else {
+        const Layout L = layout_of(G.S, G.n_acc, G.nk, G.method, G.hot_cap != 0);
+        int64_t* counts = (int64_t*)((char*)ws + L.emit);
+        const int64_t chunks = (G.S + kEmitChunk - 1) / kEmitChunk;
+        (note_launch(), k_emit_count<<<(unsigned)chunks, kThreads, 0, s>>>(G, counts));
+        (note_launch(), k_scan_counts_g<<<1, 1024, 0, s>>>(counts, chunks, out->d_n_groups));
+        (note_launch(), k_emit<<<(unsigned)chunks, kThreads, 0, s>>>(G, O, counts));
+    }
     tdg_status st = launch_status();
     if (st) return st;
-    int32_t err = 0;
-    if (cudaMemcpyAsync(&err, G.err, sizeof(err), cudaMemcpyDeviceToHost, s) != cudaSuccess) return E_IO;
+    int32_t* err = pinned_words();               // page-locked: the copy is asynchronous
+    int32_t local[2] = {0, 0};
+    int32_t* dst = err ? err : local;
+    dst[0] = dst[1] = 0;
+    if (cudaMemcpyAsync(dst, G.err, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) return E_IO;
     if (cudaStreamSynchronize(s) != cudaSuccess) return E_IO;
-    return err;
+    if (flag1) *flag1 = dst[1];
+    return dst[0];
 }
 
 static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
@@ -1092,16 +1155,11 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
         (note_launch(), k_payload_build<uint32_t><<<g, kThreads, 0, s>>>(G, *J, (uint32_t*)map, n_right, G.err + 1));
     }
     tb.stop(s);
-    int32_t flags[2] = {0, 0};
     st = launch_status();
-    if (!st && cudaMemcpyAsync(flags, G.err, sizeof(flags), cudaMemcpyDeviceToHost, s) != cudaSuccess) st = E_IO;
-    if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = E_IO;
-    const float bms = tb.ms();
-    if (st) return st;
-    if (flags[0]) return flags[0];
-    if (flags[1]) return E_OK;                      // duplicate build keys: general path
-    if (tb.on) set_last_build_ms(bms);
-    *used = true;
+    if (st) { tb.ms(); return st; }
+    // the probe runs without waiting for the build's duplicate-key flag; the
+    // flag is read with the error word at the end, and if the build side had
+    // duplicate keys the caller runs the general join instead
     int pk;
     Pred P = make_pred(pred, sel, &pk);
     static tdg_expr empty;
@@ -1157,11 +1215,16 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
 #undef TDG_PL
     tm.stop(s);
     st = launch_status();
-    if (st) { tm.ms(); return st; }
-    st = finish(G, d, ws, out, s);
-    const float ms = tm.ms();
+    if (st) { tm.ms(); tb.ms(); return st; }
+    int32_t dup = 0;
+    st = finish(G, d, ws, out, s, &dup);
+    const float ms = tm.ms(), bms = tb.ms();
+    if (st) return st;
+    if (dup) return E_OK;                           // duplicate build keys: general path
+    *used = true;
     if (tm.on) set_last_main_ms(ms);
-    return st;
+    if (tb.on) set_last_build_ms(bms);
+    return E_OK;
 }
 
 tdg_status group_run_joined(const tdg_group_desc* d, const tdg_group_plan* p, void* ws,

@@ -71,5 +71,6 @@ extern "C" tdg_status tdg_group_run_static(const tdg_group_desc* d, const tdg_ex
     st = static_scratch(&ws);
     if (st) return st;
     ThreadTimingOff no_events;          // no CUDA events either
+    ThreadNoAlloc no_host_buffers;      // nor page-locked status buffers
     return group_run_joined(d, &plan, ws, pred, sel_in, nullptr, 0, 0, out, (cudaStream_t)stream);
 }

@@ -257,16 +257,22 @@ static td_t* vec_like(int8_t type, uint8_t attrs, int64_t n) {
     return v;
 }
 
-/* Copy n elements from the device into a new host vector. */
-static td_t* fetch_vec(ex_t* x, const void* dptr, int8_t type, uint8_t attrs, int64_t n) {
+/* Copy n elements from the device into a new host vector.  With `deferred`
+ * the copy is only queued: the caller synchronizes the stream (once for all
+ * the columns of a result) before reading the vector. */
+static td_t* fetch_vec_q(ex_t* x, const void* dptr, int8_t type, uint8_t attrs, int64_t n, int deferred) {
     td_t* v = vec_like(type, attrs, n);
     if (!v || TD_IS_ERR(v)) return v ? v : TD_ERR_PTR(TD_ERR_OOM);
     size_t bytes = (size_t)n * td_sym_elem_size(type, attrs);
     if (bytes >= ((size_t)8 << 20)) tdb_pin_host(v);     /* DMA straight into the result */
-    int st = tdb_d2h(&x->c, td_data(v), dptr, bytes);
+    int st = deferred ? tdb_d2h_async(&x->c, td_data(v), dptr, bytes) : tdb_d2h(&x->c, td_data(v), dptr, bytes);
     if (st) { td_release(v); return TD_ERR_PTR(st); }
     tdb_adopt_mirror(&x->c, v, (void*)dptr);
     return v;
+}
+
+static td_t* fetch_vec(ex_t* x, const void* dptr, int8_t type, uint8_t attrs, int64_t n) {
+    return fetch_vec_q(x, dptr, type, attrs, n, 0);
 }
 
 /* ---- values ------------------------------------------------------------------------------- */
@@ -530,10 +536,15 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
     tdg_group_plan plan;
     st = tdg_group_plan_make(&d, 0, &plan);
     if (st) return TD_ERR_PTR(st);
+    tdb_trace("group planned");
     void* ws = tdb_dev_alloc(&x->c, plan.ws_bytes);
     tdg_group_out out;
     memset(&out, 0, sizeof(out));
-    out.d_n_groups = tdb_dev_alloc(&x->c, 8);
+    /* the group count lands in mapped host memory: readable once the group-by
+     * (which ends with a stream synchronization) returns, without a copy */
+    void* dng = NULL;
+    volatile int64_t* hng = tdb_host_scalar(&x->c, &dng);
+    out.d_n_groups = hng ? dng : tdb_dev_alloc(&x->c, 8);
     if (!ws || !out.d_n_groups) return TD_ERR_PTR(TD_ERR_OOM);
     for (int k = 0; k < nk; k++) {
         out.keys[k] = tdb_dev_alloc(&x->c, (size_t)plan.max_groups * td_sym_elem_size(keys[k].type, keys[k].attrs));
@@ -552,53 +563,76 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
         tdb_note_methods(plan.method, 0, pp != NULL);
     }
     if (st) return TD_ERR_PTR(st);
+    tdb_trace("group kernels done");
     int64_t ng = 0;
-    st = tdb_d2h(&x->c, &ng, out.d_n_groups, 8);
-    if (st) return TD_ERR_PTR(st);
+    if (hng) ng = *hng;
+    else if ((st = tdb_d2h(&x->c, &ng, out.d_n_groups, 8))) return TD_ERR_PTR(st);
+    tdb_trace("group count read");
 
-    td_t* res = td_table_new(nk + na);
-    if (!res || TD_IS_ERR(res)) return res;
-    for (int k = 0; k < nk; k++) {
-        td_t* col = fetch_vec(x, out.keys[k], keys[k].type, keys[k].attrs, ng);
-        if (TD_IS_ERR(col)) { td_release(res); return col; }
-        int64_t nm = keys[k].name >= 0 ? keys[k].name : (int64_t)k;
-        res = td_table_add_col(res, nm, col);
-        td_release(col);
-        if (TD_IS_ERR(res)) return res;
+    /* every result column is copied with one stream synchronization */
+    td_t* cols[TDG_MAX_KEYS + TDG_MAX_AGGS];
+    td_t* wide[TDG_MAX_AGGS];
+    int8_t otype[TDG_MAX_AGGS];
+    memset(cols, 0, sizeof(cols));
+    memset(wide, 0, sizeof(wide));
+    td_t* err = NULL;
+    for (int k = 0; k < nk && !err; k++) {
+        cols[k] = fetch_vec_q(x, out.keys[k], keys[k].type, keys[k].attrs, ng, 1);
+        if (TD_IS_ERR(cols[k])) { err = cols[k]; cols[k] = NULL; }
     }
-    for (int a = 0; a < na; a++) {
+    for (int a = 0; a < na && !err; a++) {
         uint16_t op = ext->agg_ops[a];
         int is_f = ins[a].col.data && ins[a].col.type == TD_F64;
         int8_t ot = op == OP_AVG ? TD_F64 : op == OP_COUNT ? TD_I64
                   : op == OP_SUM ? (is_f ? TD_F64 : TD_I64)
                   : (ins[a].type ? ins[a].type : TD_I64);
-        td_t* col;
+        otype[a] = ot;
+        td_t* v;
         if (td_sym_elem_size(ot, ins[a].attrs) == 8 || op == OP_AVG || op == OP_COUNT || op == OP_SUM) {
             int8_t vt = (ot == TD_F64 || op == OP_AVG) ? TD_F64 : (td_sym_elem_size(ot, ins[a].attrs) == 8 ? ot : TD_I64);
-            col = fetch_vec(x, out.aggs[a], vt, vt == TD_SYM ? ins[a].attrs : 0, ng);
+            v = fetch_vec_q(x, out.aggs[a], vt, vt == TD_SYM ? ins[a].attrs : 0, ng, 1);
+            if (!TD_IS_ERR(v)) cols[nk + a] = v;
         } else {
-            /* MIN/MAX of a narrow integer column: narrow the int64 results */
-            td_t* wide = fetch_vec(x, out.aggs[a], TD_I64, 0, ng);
-            if (TD_IS_ERR(wide)) { td_release(res); return wide; }
-            col = vec_like(ot, ins[a].attrs, ng);
-            if (!TD_IS_ERR(col)) {
-                const int64_t* w = (const int64_t*)td_data(wide);
-                for (int64_t i = 0; i < ng; i++) {
-                    if (ot == TD_SYM) td_write_sym(td_data(col), i, (uint64_t)w[i], TD_SYM, ins[a].attrs);
-                    else switch (td_elem_size(ot)) {
-                        case 4: ((int32_t*)td_data(col))[i] = (int32_t)w[i]; break;
-                        case 2: ((int16_t*)td_data(col))[i] = (int16_t)w[i]; break;
-                        default: ((uint8_t*)td_data(col))[i] = (uint8_t)w[i]; break;
-                    }
-                }
-            }
-            td_release(wide);
+            /* MIN/MAX of a narrow integer column: int64 results, narrowed below */
+            v = fetch_vec_q(x, out.aggs[a], TD_I64, 0, ng, 1);
+            if (!TD_IS_ERR(v)) wide[a] = v;
         }
-        if (TD_IS_ERR(col)) { td_release(res); return col; }
-        res = td_table_add_col(res, agg_name(op, ins[a].name, a), col);
-        td_release(col);
-        if (TD_IS_ERR(res)) return res;
+        if (TD_IS_ERR(v)) err = v;
     }
+    if (!err && (st = tdb_ctx_sync(&x->c))) err = TD_ERR_PTR(st);
+    for (int a = 0; a < na && !err; a++) {
+        if (!wide[a]) continue;
+        const int8_t ot = otype[a];
+        td_t* col = vec_like(ot, ins[a].attrs, ng);
+        if (TD_IS_ERR(col)) { err = col; break; }
+        const int64_t* w = (const int64_t*)td_data(wide[a]);
+        for (int64_t i = 0; i < ng; i++) {
+            if (ot == TD_SYM) td_write_sym(td_data(col), i, (uint64_t)w[i], TD_SYM, ins[a].attrs);
+            else switch (td_elem_size(ot)) {
+                case 4: ((int32_t*)td_data(col))[i] = (int32_t)w[i]; break;
+                case 2: ((int16_t*)td_data(col))[i] = (int16_t)w[i]; break;
+                default: ((uint8_t*)td_data(col))[i] = (uint8_t)w[i]; break;
+            }
+        }
+        cols[nk + a] = col;
+    }
+    td_t* res = err ? NULL : td_table_new(nk + na);
+    if (!err && (!res || TD_IS_ERR(res))) { err = res ? res : TD_ERR_PTR(TD_ERR_OOM); res = NULL; }
+    for (int j = 0; j < nk + na && !err; j++) {
+        int64_t nm = j < nk ? (keys[j].name >= 0 ? keys[j].name : (int64_t)j)
+                            : agg_name(ext->agg_ops[j - nk], ins[j - nk].name, j - nk);
+        td_t* r2 = td_table_add_col(res, nm, cols[j]);
+        if (TD_IS_ERR(r2)) { err = r2; break; }
+        res = r2;
+    }
+    if (err) tdb_ctx_sync(&x->c);          /* no queued copy may still target a vector freed here */
+    for (int j = 0; j < nk + na; j++) if (cols[j]) td_release(cols[j]);
+    for (int a = 0; a < na; a++) if (wide[a]) td_release(wide[a]);
+    if (err) {
+        if (res) td_release(res);
+        return err;
+    }
+    tdb_trace("group result copied");
     return res;
 }
 
@@ -828,7 +862,9 @@ static td_t* exec_group_node(ex_t* x, td_op_t* op) {
             res = right;
         } else {
             jbuilt_t jb;
+            tdb_trace("join lowering");
             int st = prepare_join(x, jext, &lv, right, &jb, 0);
+            tdb_trace("join prepared");
             if (st) {
                 res = TD_ERR_PTR(st);
             } else {
@@ -1003,5 +1039,8 @@ td_t* tdb_exec(td_graph_t* g, td_op_t* root) {
 td_t* td_execute(td_graph_t* g, td_op_t* root) {
     if (!g || !root) return TD_ERR_PTR(TD_ERR_NYI);
     atomic_store(&tdb_cancel_flag, 0);
-    return tdb_exec(g, root);
+    tdb_trace_begin();
+    td_t* r = tdb_exec(g, root);
+    tdb_trace("td_execute returns");
+    return r;
 }

@@ -20,6 +20,8 @@
  */
 
 #include "internal.h"
+#include <stdio.h>
+#include <time.h>
 #include <cuda_runtime_api.h>
 #include <pthread.h>
 #include <stdlib.h>
@@ -335,6 +337,30 @@ static _Thread_local void* tls_stream;
 static _Thread_local tmirror_t* tls_tm;
 static _Thread_local int tls_ntm, tls_captm;
 
+/* Trace points are buffered per thread and printed when the outermost call
+ * returns ("td_execute returns"), so printing does not skew the intervals. */
+static int trace_on = -1;
+static _Thread_local struct timespec trace_t0;
+static _Thread_local struct { const char* what; double us; } trace_buf[32];
+static _Thread_local int trace_n;
+
+void tdb_trace_begin(void) {
+    if (trace_on < 0) trace_on = getenv("TD_TRACE") != NULL;
+    if (trace_on) { clock_gettime(CLOCK_MONOTONIC, &trace_t0); trace_n = 0; }
+}
+
+void tdb_trace(const char* what) {
+    if (trace_on <= 0) return;
+    struct timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    const double us = (double)(t.tv_sec - trace_t0.tv_sec) * 1e6 + (double)(t.tv_nsec - trace_t0.tv_nsec) / 1e3;
+    if (trace_n < 32) { trace_buf[trace_n].what = what; trace_buf[trace_n].us = us; trace_n++; }
+    if (strcmp(what, "td_execute returns") == 0) {
+        for (int i = 0; i < trace_n; i++) fprintf(stderr, "[td] %9.1f us  %s\n", trace_buf[i].us, trace_buf[i].what);
+        trace_n = 0;
+    }
+}
+
 int tdb_ctx_begin(tdb_ctx* c) {
     memset(c, 0, sizeof(*c));
     int st = tdb_gpu_ensure();
@@ -362,8 +388,11 @@ void* tdb_dev_alloc(tdb_ctx* c, size_t bytes) {
     return p;
 }
 
+static void finish_pending(tdb_ctx* c);
+
 int tdb_ctx_sync(tdb_ctx* c) {
-    if (cudaStreamSynchronize((cudaStream_t)c->stream) != cudaSuccess) { cudaGetLastError(); return TD_ERR_IO; }
+    if (cudaStreamSynchronize((cudaStream_t)c->stream) != cudaSuccess) { cudaGetLastError(); c->n_pending = 0; return TD_ERR_IO; }
+    finish_pending(c);
     return TD_OK;
 }
 
@@ -378,6 +407,7 @@ void tdb_note_methods(int group, int join, int fused) {
 
 void tdb_ctx_end(tdb_ctx* c) {
     if (c->stream) cudaStreamSynchronize((cudaStream_t)c->stream);
+    finish_pending(c);
     for (int i = 0; i < c->n_tmp; i++) arena_free(c->tmp[i]);
     free(c->tmp);
     c->tmp = NULL;
@@ -403,6 +433,74 @@ void tdb_reset_methods(void) {
     pthread_mutex_lock(&mu);
     last_stats.last_group_method = last_stats.last_join_method = last_stats.last_fused = 0;
     pthread_mutex_unlock(&mu);
+}
+
+/* Per-thread page-locked, device-mapped scalars (one page). */
+#define TDB_SCALARS 64
+static _Thread_local int64_t* tls_scalar_h;
+static _Thread_local void* tls_scalar_d;
+
+volatile int64_t* tdb_host_scalar(tdb_ctx* c, void** dev) {
+    if (!tls_scalar_h) {
+        void* h = NULL;
+        if (cudaHostAlloc(&h, TDB_SCALARS * sizeof(int64_t), cudaHostAllocMapped) != cudaSuccess) {
+            cudaGetLastError();
+            return NULL;
+        }
+        void* d = NULL;
+        if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) { cudaGetLastError(); cudaFreeHost(h); return NULL; }
+        tls_scalar_h = h;
+        tls_scalar_d = d;
+    }
+    if (c->n_scalar >= TDB_SCALARS) return NULL;
+    const int i = c->n_scalar++;
+    tls_scalar_h[i] = 0;
+    *dev = (int64_t*)tls_scalar_d + i;
+    return tls_scalar_h + i;
+}
+
+/* Per-thread page-locked staging for small device->host copies: a copy into
+ * pageable memory is synchronous in CUDA, so queued copies land here and are
+ * moved to their destinations when the call synchronizes. */
+#define TDB_STAGE_BYTES ((size_t)4 << 20)
+static _Thread_local char* tls_stage;
+
+int tdb_d2h_async(tdb_ctx* c, void* host, const void* dev, size_t bytes) {
+    if (!bytes) return TD_OK;
+    void* dst = host;
+    const size_t off = (c->stage_used + 255) & ~(size_t)255;
+    if (!tdb_host_is_pinned(host) && off + bytes <= TDB_STAGE_BYTES && c->n_pending < TDB_PENDING) {
+        if (!tls_stage && cudaMallocHost((void**)&tls_stage, TDB_STAGE_BYTES) != cudaSuccess) {
+            cudaGetLastError();
+            tls_stage = NULL;
+        }
+        if (tls_stage) {
+            dst = tls_stage + off;
+            c->pending[c->n_pending].host = host;
+            c->pending[c->n_pending].stage = dst;
+            c->pending[c->n_pending].bytes = bytes;
+            c->n_pending++;
+            c->stage_used = off + bytes;
+        }
+    }
+    if (cudaMemcpyAsync(dst, dev, bytes, cudaMemcpyDeviceToHost, (cudaStream_t)c->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return TD_ERR_IO;
+    }
+    c->d2h_bytes += bytes;
+    return TD_OK;
+}
+
+int tdb_host_is_pinned(const void* p) {
+    struct cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return a.type == cudaMemoryTypeHost;
+}
+
+static void finish_pending(tdb_ctx* c) {
+    for (int i = 0; i < c->n_pending; i++) memcpy(c->pending[i].host, c->pending[i].stage, c->pending[i].bytes);
+    c->n_pending = 0;
+    c->stage_used = 0;
 }
 
 int tdb_d2h(tdb_ctx* c, void* host, const void* dev, size_t bytes) {

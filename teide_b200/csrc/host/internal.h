@@ -63,6 +63,12 @@ typedef struct tdb_ctx {
     int      n_tmp, cap_tmp;
     /* host->device bytes uploaded in this call (for statistics) */
     uint64_t h2d_bytes, d2h_bytes;
+    int      n_scalar;          /* mapped host scalars handed out in this call */
+    /* device->host copies queued into the staging buffer (tdb_d2h_async) */
+#define TDB_PENDING 32
+    struct { void* host; void* stage; size_t bytes; } pending[TDB_PENDING];
+    int      n_pending;
+    size_t   stage_used;
 } tdb_ctx;
 
 int      tdb_gpu_ensure(void);                 /* 0 ok, else td_err_t */
@@ -73,6 +79,14 @@ void     tdb_dev_free_persistent(void* p);
 int      tdb_ctx_begin(tdb_ctx* c);
 void     tdb_ctx_end(tdb_ctx* c);
 int      tdb_ctx_sync(tdb_ctx* c);               /* 0 ok, else td_err_t */
+/* An int64 in page-locked host memory that kernels can write through the
+ * returned device pointer (*dev): once the stream has synchronized, the host
+ * reads it with no copy.  Valid until the end of the call; NULL if none left. */
+volatile int64_t* tdb_host_scalar(tdb_ctx* c, void** dev);
+/* 1 when `p` lies in page-locked memory (a copy to it can be asynchronous). */
+int      tdb_host_is_pinned(const void* p);
+/* Device->host copy queued on the call's stream; tdb_ctx_sync completes it. */
+int      tdb_d2h_async(tdb_ctx* c, void* host, const void* dev, size_t bytes);
 /* device view of a host column, copied into *out; uploads it unless it is
  * resident.  want_stats asks for min/max of an integer column. */
 int      tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out);
@@ -90,6 +104,11 @@ extern _Atomic(int) tdb_cancel_flag;
 
 /* ---- executor ------------------------------------------------------------------ */
 td_t* tdb_exec(td_graph_t* g, td_op_t* root);
+/* Phase tracing: with TD_TRACE set in the environment, each call prints the
+ * microseconds since this thread's td_execute began and a label to stderr. */
+void  tdb_trace(const char* what);
+void  tdb_trace_begin(void);
+
 /* 1 when the column (or a slice's parent) has a resident device copy. */
 int   tdb_col_resident(td_t* col);
 
