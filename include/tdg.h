@@ -296,6 +296,9 @@ typedef struct tdg_batch_plan {
     int32_t words;         /* 8-byte words per slot record */
     int32_t threads;       /* threads per persistent CTA */
     int32_t smem_bytes;    /* dynamic shared memory per CTA */
+    int32_t query_base;    /* added to every emitted query index (0 from plan_make;
+                              a caller running a batch in parts sets it per part) */
+    int32_t pad;
 } tdg_batch_plan;
 
 typedef struct tdg_batch_out {

@@ -50,7 +50,7 @@ struct BatchK {
     int32_t* err;
     int64_t* qcount;
     int64_t* qoff;
-    int32_t n_queries, W, na, smem_slots;
+    int32_t n_queries, W, na, smem_slots, query_base;
     int32_t kind[TDG_MAX_AGGS];
     int32_t ai[TDG_MAX_AGGS];
     int32_t op[TDG_MAX_AGGS];
@@ -97,6 +97,7 @@ static BatchK make_bk(const tdg_batch_plan* p, void* ws) {
     B.W = p->words;
     B.na = p->n_aggs;
     B.smem_slots = p->smem_slots;
+    B.query_base = p->query_base;
     int ai = 0;
     for (int a = 0; a < p->n_aggs; a++) {
         const int op = p->agg_ops[a], f = p->val_f64;
@@ -315,7 +316,7 @@ __global__ void __launch_bounds__(kEmitBlock) k_batch_emit(const BatchK B, const
         const int pre = block_excl_scan(c ? 1 : 0, &tot, red);
         if (c) {
             const int64_t o = out + pre;
-            O.query[o] = q;
+            O.query[o] = (int64_t)q + B.query_base;
             O.key[o] = Q.key_min + s;
             for (int a = 0; a < B.na; a++) {
                 const int kind = B.kind[a];

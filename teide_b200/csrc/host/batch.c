@@ -33,34 +33,65 @@
 #include <sys/stat.h>
 
 #define BATCH_CACHE 4
+#define BATCH_CHUNKS 8
 
+/* One chunk of a batch: a contiguous range of its queries with its own work
+ * description, scratch, outputs and captured CUDA graph. */
 typedef struct {
-    uint64_t        sig;
-    int64_t         n;
+    int32_t         q0, nq;
     tdg_batch_plan  plan;
     void*           ws;
     tdg_batch_out   out;
-    void*           bufs[TDG_MAX_AGGS + 3];
+    void*           bufs[TDG_MAX_AGGS + 2];
     int             n_bufs;
     cudaGraphExec_t exec;
-    int             used;       /* LRU stamp */
     uint64_t        launches;   /* kernels in the captured graph */
+} bchunk_t;
+
+typedef struct {
+    uint64_t    sig;
+    int64_t     n;
+    int         used;           /* LRU stamp */
+    int         n_chunks;
+    bchunk_t    ch[BATCH_CHUNKS];
+    int64_t*    h_rows;         /* page-locked, device-mapped: rows each chunk emitted */
+    void*       d_rows;
+    cudaEvent_t done[BATCH_CHUNKS];
+    int64_t     total_slots;
 } bcache_t;
 
 static bcache_t bcache[BATCH_CACHE];
 static int bstamp;
 static pthread_mutex_t bcache_mu = PTHREAD_MUTEX_INITIALIZER;   /* cache + its graphs */
 
-static uint64_t fnv64(uint64_t h, const void* p, size_t n) {
+/* Signature of a batch: 8 bytes at a time (the query descriptors are 8-byte
+ * multiples), a multiply-xorshift mix per word. */
+static uint64_t sig64(uint64_t h, const void* p, size_t n) {
     const unsigned char* b = p;
-    for (size_t i = 0; i < n; i++) { h ^= b[i]; h *= 1099511628211ULL; }
+    size_t i = 0;
+    for (; i + 8 <= n; i += 8) {
+        uint64_t w;
+        memcpy(&w, b + i, 8);
+        h = (h ^ w) * 0x9E3779B97F4A7C15ULL;
+        h ^= h >> 29;
+    }
+    for (; i < n; i++) h = (h ^ b[i]) * 1099511628211ULL;
     return h;
 }
 
+static void chunk_drop(bchunk_t* ch) {
+    if (ch->exec) cudaGraphExecDestroy(ch->exec);
+    tdb_dev_free_persistent(ch->ws);
+    for (int i = 0; i < ch->n_bufs; i++) tdb_dev_free_persistent(ch->bufs[i]);
+    memset(ch, 0, sizeof(*ch));
+}
+
 static void bcache_drop(bcache_t* e) {
-    if (e->exec) cudaGraphExecDestroy(e->exec);
-    tdb_dev_free_persistent(e->ws);
-    for (int i = 0; i < e->n_bufs; i++) tdb_dev_free_persistent(e->bufs[i]);
+    for (int i = 0; i < e->n_chunks; i++) {
+        chunk_drop(&e->ch[i]);
+        if (e->done[i]) cudaEventDestroy(e->done[i]);
+    }
+    if (e->h_rows) cudaFreeHost(e->h_rows);
     memset(e, 0, sizeof(*e));
 }
 
@@ -198,25 +229,24 @@ static int lower_one(tdb_ctx* c, td_graph_t* g, td_op_t* root, uint16_t* ops, in
     return TD_OK;
 }
 
-static int alloc_outputs(bcache_t* e) {
-    size_t rows = (size_t)(e->plan.total_slots > 0 ? e->plan.total_slots : 1);
-    e->n_bufs = 0;
-    void** b = e->bufs;
-    if (!(b[e->n_bufs++] = tdb_dev_alloc_persistent(rows * 8))) return TD_ERR_OOM;
-    if (!(b[e->n_bufs++] = tdb_dev_alloc_persistent(rows * 8))) return TD_ERR_OOM;
-    if (!(b[e->n_bufs++] = tdb_dev_alloc_persistent(8))) return TD_ERR_OOM;
-    e->out.query = b[0];
-    e->out.key = b[1];
-    e->out.d_n_rows = b[2];
-    for (int a = 0; a < e->plan.n_aggs; a++) {
-        if (!(b[e->n_bufs++] = tdb_dev_alloc_persistent(rows * 8))) return TD_ERR_OOM;
-        e->out.aggs[a] = b[e->n_bufs - 1];
+static int alloc_outputs(bchunk_t* ch, int64_t* d_rows) {
+    size_t rows = (size_t)(ch->plan.total_slots > 0 ? ch->plan.total_slots : 1);
+    ch->n_bufs = 0;
+    void** b = ch->bufs;
+    if (!(b[ch->n_bufs++] = tdb_dev_alloc_persistent(rows * 8))) return TD_ERR_OOM;
+    if (!(b[ch->n_bufs++] = tdb_dev_alloc_persistent(rows * 8))) return TD_ERR_OOM;
+    ch->out.query = b[0];
+    ch->out.key = b[1];
+    ch->out.d_n_rows = d_rows;
+    for (int a = 0; a < ch->plan.n_aggs; a++) {
+        if (!(b[ch->n_bufs++] = tdb_dev_alloc_persistent(rows * 8))) return TD_ERR_OOM;
+        ch->out.aggs[a] = b[ch->n_bufs - 1];
     }
     return TD_OK;
 }
 
 /* Time one configuration of the batch kernel (ms), or a negative value. */
-static float time_config(tdb_ctx* c, const tdg_batch_desc* d, int64_t tile, int32_t ctas, bcache_t* scratch) {
+static float time_config(tdb_ctx* c, const tdg_batch_desc* d, int64_t tile, int32_t ctas, bchunk_t* scratch) {
     tdg_batch_plan p;
     if (tdg_batch_plan_make(d, tile, ctas, &p)) return -1;
     void* ws = tdb_dev_alloc(c, p.ws_bytes);
@@ -247,9 +277,13 @@ static void autotune(tdb_ctx* c, const tdg_batch_desc* d, int64_t* tile, int32_t
     *tile = 0;
     *ctas = 0;
     if (getenv("TD_NO_AUTOTUNE")) return;
-    bcache_t scratch;
+    bchunk_t scratch;
     memset(&scratch, 0, sizeof(scratch));
-    if (tdg_batch_plan_make(d, 4096, 0, &scratch.plan) || alloc_outputs(&scratch)) { bcache_drop(&scratch); return; }
+    int64_t* d_rows = tdb_dev_alloc(c, 8);
+    if (!d_rows || tdg_batch_plan_make(d, 4096, 0, &scratch.plan) || alloc_outputs(&scratch, d_rows)) {
+        chunk_drop(&scratch);
+        return;
+    }
     static const int64_t tiles[] = {4096, 16384, 65536};
     static const int32_t ctass[] = {0, 1, 2, 4};   /* 1 and 2: large shared-memory modes */
     float best = -1;
@@ -258,7 +292,7 @@ static void autotune(tdb_ctx* c, const tdg_batch_desc* d, int64_t* tile, int32_t
             float ms = time_config(c, d, tiles[i], ctass[j], &scratch);
             if (ms > 0 && (best < 0 || ms < best)) { best = ms; *tile = tiles[i]; *ctas = ctass[j]; }
         }
-    bcache_drop(&scratch);
+    chunk_drop(&scratch);
     if (best > 0) tune_store(key, *tile, *ctas);
 }
 
@@ -277,6 +311,7 @@ static int64_t agg_out_name(uint16_t op, int64_t base) {
 td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
     if (!graphs || !roots || n < 0 || n > INT32_MAX) return TD_ERR_PTR(TD_ERR_RANGE);
     atomic_store(&tdb_cancel_flag, 0);
+    tdb_trace_begin();
     tdb_ctx c;
     int st = tdb_ctx_begin(&c);
     if (st) return TD_ERR_PTR(st);
@@ -304,105 +339,190 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
     for (int a = 0; a < n_ops; a++) d.agg_ops[a] = ops[a];
     d.queries = qs;
 
-    uint64_t sig = fnv64(1469598103934665603ULL, qs, sizeof(tdg_batch_query) * (size_t)n);
-    sig = fnv64(sig, &d.agg_ops, sizeof(d.agg_ops));
+    /* Chunks: contiguous query ranges of about equal rows.  Each chunk's
+     * results are copied to the host on a second stream while the next chunks
+     * compute.  Timing (tdg_set_timing) runs one chunk so its kernel time
+     * covers the whole batch. */
+    const int timing = tdg_timing_enabled();
+    int K = timing ? 1 : (int)(n / 64 < BATCH_CHUNKS ? n / 64 : BATCH_CHUNKS);
+    if (K < 1) K = 1;
+    uint64_t sig = sig64(1469598103934665603ULL, qs, sizeof(tdg_batch_query) * (size_t)n);
+    sig = sig64(sig, &d.agg_ops, sizeof(d.agg_ops));
+    sig = sig64(sig, &K, sizeof(K));
     bcache_t* e = NULL;
-    for (int i = 0; i < BATCH_CACHE; i++) if (bcache[i].ws && bcache[i].sig == sig && bcache[i].n == n) e = &bcache[i];
+    for (int i = 0; i < BATCH_CACHE; i++)
+        if (bcache[i].n_chunks && bcache[i].sig == sig && bcache[i].n == n) e = &bcache[i];
     if (!e) {
+        /* chunk boundaries: contiguous query ranges of about equal rows */
+        int32_t q0s[BATCH_CHUNKS + 1];
+        double total = 0, acc = 0;
+        for (int64_t i = 0; i < n; i++) total += (double)qs[i].nrows + 1;
+        int32_t q = 0;
+        for (int k = 0; k < K; k++) {
+            q0s[k] = q;
+            const double goal = total * (k + 1) / K;
+            while (q < n && (k == K - 1 || acc < goal)) { acc += (double)qs[q].nrows + 1; q++; }
+        }
+        q0s[K] = (int32_t)n;
+        /* tile and CTAs tuned on a chunk: that is the launch that runs */
+        tdg_batch_desc d0 = d;
+        d0.n_queries = q0s[1] - q0s[0];
+        d0.queries = qs;
         int64_t tile;
         int32_t ctas;
-        autotune(&c, &d, &tile, &ctas);
+        autotune(&c, &d0, &tile, &ctas);
         int victim = 0;
         for (int i = 1; i < BATCH_CACHE; i++) if (bcache[i].used < bcache[victim].used) victim = i;
         e = &bcache[victim];
         bcache_drop(e);
         e->sig = sig;
         e->n = n;
-        if ((st = tdg_batch_plan_make(&d, tile, ctas, &e->plan))) { bcache_drop(e); goto done; }
-        e->ws = tdb_dev_alloc_persistent(e->plan.ws_bytes);
-        if (!e->ws || alloc_outputs(e)) { bcache_drop(e); st = TD_ERR_OOM; goto done; }
-        if ((st = tdg_batch_prepare(&d, &e->plan, e->ws, c.stream))) { bcache_drop(e); goto done; }
-        /* capture the run once; replays reuse the instantiated graph */
-        cudaGraph_t graph = NULL;
-        cudaStream_t s = (cudaStream_t)c.stream;
-        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-            uint64_t l0 = tdg_launch_count();
-            int rs = tdg_batch_run(&e->plan, e->ws, &e->out, c.stream);
-            e->launches = tdg_launch_count() - l0;
-            if (cudaStreamEndCapture(s, &graph) == cudaSuccess && !rs && graph) {
-                if (cudaGraphInstantiate(&e->exec, graph, 0) != cudaSuccess) e->exec = NULL;
-            }
-            if (graph) cudaGraphDestroy(graph);
+        void* h = NULL;
+        if (cudaHostAlloc(&h, BATCH_CHUNKS * sizeof(int64_t), cudaHostAllocMapped) != cudaSuccess ||
+            cudaHostGetDevicePointer(&e->d_rows, h, 0) != cudaSuccess) {
+            cudaGetLastError();
+            if (h) cudaFreeHost(h);
+            memset(e, 0, sizeof(*e));
+            st = TD_ERR_OOM;
+            goto done;
         }
-        cudaGetLastError();
+        e->h_rows = h;
+        for (int k = 0; k < K && !st; k++) {
+            bchunk_t* ch = &e->ch[k];
+            e->n_chunks = k + 1;
+            ch->q0 = q0s[k];
+            ch->nq = q0s[k + 1] - q0s[k];
+            tdg_batch_desc dc = d;
+            dc.n_queries = ch->nq;
+            dc.queries = qs + ch->q0;
+            if (cudaEventCreateWithFlags(&e->done[k], cudaEventDisableTiming) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; break; }
+            if ((st = tdg_batch_plan_make(&dc, tile, ctas, &ch->plan))) break;
+            ch->plan.query_base = ch->q0;
+            ch->ws = tdb_dev_alloc_persistent(ch->plan.ws_bytes);
+            if (!ch->ws || alloc_outputs(ch, (int64_t*)e->d_rows + k)) { st = TD_ERR_OOM; break; }
+            if ((st = tdg_batch_prepare(&dc, &ch->plan, ch->ws, c.stream))) break;
+            e->total_slots += ch->plan.total_slots;
+            /* capture the run once; replays reuse the instantiated graph */
+            cudaGraph_t graph = NULL;
+            cudaStream_t s = (cudaStream_t)c.stream;
+            if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+                uint64_t l0 = tdg_launch_count();
+                int rs = tdg_batch_run(&ch->plan, ch->ws, &ch->out, c.stream);
+                ch->launches = tdg_launch_count() - l0;
+                if (cudaStreamEndCapture(s, &graph) == cudaSuccess && !rs && graph) {
+                    if (cudaGraphInstantiate(&ch->exec, graph, 0) != cudaSuccess) ch->exec = NULL;
+                }
+                if (graph) cudaGraphDestroy(graph);
+            }
+            cudaGetLastError();
+        }
+        if (st) { bcache_drop(e); goto done; }
     }
     e->used = ++bstamp;
+    tdb_trace("batch lowered");
     if ((st = tdb_check_cancel())) goto done;
     tdb_note_kernel();
-    if (e->exec && !tdg_timing_enabled()) {   /* timing runs the kernels directly */
-        if (cudaGraphLaunch(e->exec, (cudaStream_t)c.stream) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; goto done; }
-        tdg_count_launches(e->launches);
-    } else if ((st = tdg_batch_run(&e->plan, e->ws, &e->out, c.stream))) {
-        goto done;
+    cudaStream_t s = (cudaStream_t)c.stream;
+    for (int k = 0; k < e->n_chunks && !st; k++) {
+        bchunk_t* ch = &e->ch[k];
+        if (ch->exec && !timing) {                /* timing runs the kernels directly */
+            if (cudaGraphLaunch(ch->exec, s) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; break; }
+            tdg_count_launches(ch->launches);
+        } else if ((st = tdg_batch_run(&ch->plan, ch->ws, &ch->out, c.stream))) {
+            break;
+        }
+        if (cudaEventRecord(e->done[k], s) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; }
     }
-    int64_t rows = 0;
-    if ((st = tdb_d2h(&c, &rows, e->out.d_n_rows, 8))) goto done;
-    if (rows < 0) { st = TD_ERR_DOMAIN; goto done; }   /* key outside its statistics */
-    res = td_table_new(2 + n_ops);
-    if (!res || TD_IS_ERR(res)) { st = TD_ERR_OOM; res = NULL; goto done; }
+    if (st) goto done;
+    tdb_trace("batch launched");
+
     /* device columns are 8 bytes wide; keys and MIN/MAX of narrower integer
      * columns are narrowed back to the column's type, as td_group returns them */
-    typedef struct { void* d; int8_t t; uint8_t attrs; int64_t name; } outcol_t;
+    typedef struct { int8_t t; uint8_t attrs; int64_t name; td_t* v; } outcol_t;
     outcol_t cols[TDG_MAX_AGGS + 2];
+    memset(cols, 0, sizeof(cols));
     int nc = 0;
-    cols[nc++] = (outcol_t){ e->out.query, TD_I64, 0, td_sym_intern("_query", 6) };
-    cols[nc++] = (outcol_t){ e->out.key, n ? hq[0].key_type : TD_I64, n ? hq[0].key_attrs : 0,
-                             n ? hq[0].key_name : td_sym_intern("key", 3) };
+    cols[nc++] = (outcol_t){ TD_I64, 0, td_sym_intern("_query", 6), NULL };
+    cols[nc++] = (outcol_t){ n ? hq[0].key_type : TD_I64, n ? hq[0].key_attrs : 0,
+                             n ? hq[0].key_name : td_sym_intern("key", 3), NULL };
     for (int a = 0; a < n_ops; a++) {
-        int8_t t = ops[a] == OP_COUNT ? TD_I64 : (ops[a] == OP_AVG || e->plan.val_f64) ? TD_F64
+        const int val_f64 = e->ch[0].plan.val_f64;
+        int8_t t = ops[a] == OP_COUNT ? TD_I64 : (ops[a] == OP_AVG || val_f64) ? TD_F64
                  : (ops[a] == OP_SUM || !n) ? TD_I64 : hq[0].val_type;
-        cols[nc++] = (outcol_t){ e->out.aggs[a], t, (ops[a] == OP_MIN || ops[a] == OP_MAX) && n ? hq[0].val_attrs : 0,
-                                 agg_out_name(ops[a], n ? hq[0].val_name : 0) };
+        cols[nc++] = (outcol_t){ t, (ops[a] == OP_MIN || ops[a] == OP_MAX) && n ? hq[0].val_attrs : 0,
+                                 agg_out_name(ops[a], n ? hq[0].val_name : 0), NULL };
     }
+    tdb_trace("batch schema");
+    /* wide host columns sized for every slot; lengths are set once known */
+    const int64_t cap = e->total_slots > 0 ? e->total_slots : 1;
     for (int j = 0; j < nc && !st; j++) {
-        int wide = td_sym_elem_size(cols[j].t, cols[j].attrs) == 8;
-        td_t* v = td_vec_new(wide ? cols[j].t : TD_I64, rows);
+        const int wide = td_sym_elem_size(cols[j].t, cols[j].attrs) == 8;
+        td_t* v = td_vec_new(wide ? cols[j].t : TD_I64, cap);
         if (!v || TD_IS_ERR(v)) { st = TD_ERR_OOM; break; }
-        v->len = rows;
         if (wide && cols[j].t == TD_SYM) v->attrs = cols[j].attrs;
-        if ((size_t)rows * 8 >= ((size_t)8 << 20)) tdb_pin_host(v);
-        st = tdb_d2h(&c, td_data(v), cols[j].d, (size_t)rows * 8);
-        if (!st && !wide) {
-            td_t* nv = td_vec_new(cols[j].t, rows);
-            if (!nv || TD_IS_ERR(nv)) st = TD_ERR_OOM;
-            else {
-                nv->len = rows;
-                if (cols[j].t == TD_SYM) nv->attrs = cols[j].attrs;
-                const int64_t* w = (const int64_t*)td_data(v);
-                for (int64_t i = 0; i < rows; i++) {
-                    if (cols[j].t == TD_SYM) td_write_sym(td_data(nv), i, (uint64_t)w[i], TD_SYM, cols[j].attrs);
-                    else switch (td_elem_size(cols[j].t)) {
-                        case 4: ((int32_t*)td_data(nv))[i] = (int32_t)w[i]; break;
-                        case 2: ((int16_t*)td_data(nv))[i] = (int16_t)w[i]; break;
-                        default: ((uint8_t*)td_data(nv))[i] = (uint8_t)w[i]; break;
-                    }
-                }
-                td_release(v);
-                v = nv;
-            }
-        }
-        if (!st) {
-            td_t* r2 = td_table_add_col(res, cols[j].name, v);
-            if (TD_IS_ERR(r2)) st = TD_ERR_CODE(r2); else res = r2;
-        }
-        td_release(v);
+        if ((size_t)cap * 8 >= ((size_t)8 << 20)) tdb_pin_host(v);
+        cols[j].v = v;
     }
+    tdb_trace("batch result vectors");
+    static _Thread_local cudaStream_t copy_stream;
+    if (!st && !copy_stream && cudaStreamCreateWithFlags(&copy_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        copy_stream = NULL;
+        st = TD_ERR_IO;
+    }
+    int64_t rows = 0;
+    for (int k = 0; k < e->n_chunks && !st; k++) {
+        bchunk_t* ch = &e->ch[k];
+        if (cudaEventSynchronize(e->done[k]) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; break; }
+        tdb_trace("batch chunk computed");
+        const int64_t rk = ((volatile int64_t*)e->h_rows)[k];
+        if (rk < 0) { st = TD_ERR_DOMAIN; break; }     /* a key outside its statistics */
+        void* src[TDG_MAX_AGGS + 2];
+        src[0] = ch->out.query;
+        src[1] = ch->out.key;
+        for (int a = 0; a < n_ops; a++) src[2 + a] = ch->out.aggs[a];
+        for (int j = 0; j < nc && !st; j++)
+            if (rk && cudaMemcpyAsync((char*)td_data(cols[j].v) + (size_t)rows * 8, src[j], (size_t)rk * 8,
+                                      cudaMemcpyDeviceToHost, copy_stream) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; }
+        rows += rk;
+    }
+    if (copy_stream && cudaStreamSynchronize(copy_stream) != cudaSuccess) { cudaGetLastError(); if (!st) st = TD_ERR_IO; }
+    if (!st) c.d2h_bytes += (uint64_t)rows * 8 * (uint64_t)nc;
+    tdb_trace("batch results copied");
+    res = st ? NULL : td_table_new(2 + n_ops);
+    if (!st && (!res || TD_IS_ERR(res))) { st = TD_ERR_OOM; res = NULL; }
+    for (int j = 0; j < nc && !st; j++) {
+        td_t* v = cols[j].v;
+        v->len = rows;
+        if (td_sym_elem_size(cols[j].t, cols[j].attrs) != 8) {
+            td_t* nv = td_vec_new(cols[j].t, rows);
+            if (!nv || TD_IS_ERR(nv)) { st = TD_ERR_OOM; break; }
+            nv->len = rows;
+            if (cols[j].t == TD_SYM) nv->attrs = cols[j].attrs;
+            const int64_t* w = (const int64_t*)td_data(v);
+            for (int64_t i = 0; i < rows; i++) {
+                if (cols[j].t == TD_SYM) td_write_sym(td_data(nv), i, (uint64_t)w[i], TD_SYM, cols[j].attrs);
+                else switch (td_elem_size(cols[j].t)) {
+                    case 4: ((int32_t*)td_data(nv))[i] = (int32_t)w[i]; break;
+                    case 2: ((int16_t*)td_data(nv))[i] = (int16_t)w[i]; break;
+                    default: ((uint8_t*)td_data(nv))[i] = (uint8_t)w[i]; break;
+                }
+            }
+            td_release(v);
+            cols[j].v = v = nv;
+        }
+        td_t* r2 = td_table_add_col(res, cols[j].name, v);
+        if (TD_IS_ERR(r2)) st = TD_ERR_CODE(r2); else res = r2;
+    }
+    for (int j = 0; j < nc; j++) if (cols[j].v) td_release(cols[j].v);
+    tdb_trace("batch assembled");
 done:
     pthread_mutex_unlock(&bcache_mu);
     if (st && res) { td_release(res); res = NULL; }
     free(hq);
     free(qs);
     tdb_ctx_end(&c);
+    tdb_trace("td_execute returns");
     return st ? TD_ERR_PTR(st) : res;
 }
 

@@ -43,7 +43,8 @@ def run_batch(td, tables, ops=(OP_SUM, OP_COUNT, OP_MAX)):
 
 def test_batch_matches_oracle_per_query(gpu, tmp_path, monkeypatch):
     monkeypatch.setenv("TD_TUNE_CACHE", str(tmp_path / "tune.json"))
-    rows, ks = workloads.config4_shapes(n_queries=96, seed=41, rows=(1, 300_000), groups=(1, 70_000))
+    # 300 queries: the batch runs as 4 chunks whose results are copied while later chunks compute
+    rows, ks = workloads.config4_shapes(n_queries=300, seed=41, rows=(1, 200_000), groups=(1, 70_000))
     datas = [workloads.config4_query(int(r), int(k), seed=1000 + i) for i, (r, k) in enumerate(zip(rows, ks))]
     tables = [gpu.table(d) for d in datas]
     L = _bind(gpu)
