@@ -264,7 +264,7 @@ static td_t* fetch_vec_q(ex_t* x, const void* dptr, int8_t type, uint8_t attrs, 
     td_t* v = vec_like(type, attrs, n);
     if (!v || TD_IS_ERR(v)) return v ? v : TD_ERR_PTR(TD_ERR_OOM);
     size_t bytes = (size_t)n * td_sym_elem_size(type, attrs);
-    if (bytes >= ((size_t)8 << 20)) tdb_pin_host(v);     /* DMA straight into the result */
+    if (bytes >= ((size_t)2 << 20)) tdb_pin_host(v);     /* heap-mapped block: DMA straight into it */
     int st = deferred ? tdb_d2h_async(&x->c, td_data(v), dptr, bytes) : tdb_d2h(&x->c, td_data(v), dptr, bytes);
     if (st) { td_release(v); return TD_ERR_PTR(st); }
     tdb_adopt_mirror(&x->c, v, (void*)dptr);

@@ -66,9 +66,12 @@ static void* arena_alloc(size_t bytes) {
     size_t sz = round_sz(bytes ? bytes : 1);
     pthread_mutex_lock(&mu);
     if (mem_limit && live_bytes + sz > mem_limit) { pthread_mutex_unlock(&mu); return NULL; }
+    /* best fit among cached blocks up to twice the request: a new cudaMalloc
+     * can synchronize the device and stall every other query's stream, which
+     * costs far more than the unused tail of a larger block */
     int best = -1;
     for (int i = 0; i < n_free; i++)
-        if (freel[i].sz >= sz && freel[i].sz <= sz + sz / 4 + ((size_t)2 << 20) &&
+        if (freel[i].sz >= sz && freel[i].sz <= 2 * sz + ((size_t)2 << 20) &&
             (best < 0 || freel[i].sz < freel[best].sz)) best = i;
     void* p = NULL;
     if (best >= 0) {
@@ -462,7 +465,7 @@ volatile int64_t* tdb_host_scalar(tdb_ctx* c, void** dev) {
 /* Per-thread page-locked staging for small device->host copies: a copy into
  * pageable memory is synchronous in CUDA, so queued copies land here and are
  * moved to their destinations when the call synchronizes. */
-#define TDB_STAGE_BYTES ((size_t)4 << 20)
+#define TDB_STAGE_BYTES ((size_t)16 << 20)
 static _Thread_local char* tls_stage;
 
 int tdb_d2h_async(tdb_ctx* c, void* host, const void* dev, size_t bytes) {
