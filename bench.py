@@ -649,7 +649,7 @@ def main():
     hbm, peak_kind = peaks()
     mean_main = sum(main_ms) / len(main_ms) if main_ms else 0.0
     achieved = main_bytes / (mean_main / 1e3) / 1e9 if mean_main > 0 else None
-    prof = {"join_group": "k_payload_probe_join_group.md", "group_radix": "k_group_group_radix.md",
+    prof = {"join_group": "k_probe_vec_join_group.md", "group_radix": "k_group_group_radix.md",
             "readme_group": "k_group_readme_group.md"}[args.workload]
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
@@ -664,7 +664,7 @@ def main():
                    "scale": args.scale},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": profile_traffic(prof),
-                     "kernel": {"join_group": "k_payload_probe (fused probe + aggregate)",
+                     "kernel": {"join_group": "k_probe_vec (fused probe + aggregate)",
                                 "group_radix": "k_group", "readme_group": "k_group"}[args.workload],
                      "bytes_per_launch": main_bytes,
                      "mean_launch_ms": mean_main, "peak_source": peak_kind,
