@@ -60,6 +60,7 @@ class Td:
             "td_heap_destroy": (None, []), "td_sym_destroy": (None, []),
             "td_vec_new": (P, [C.c_int8, C.c_int64]),
             "td_vec_from_raw": (P, [C.c_int8, P, C.c_int64]),
+            "td_sym_vec_new": (P, [C.c_uint8, C.c_int64]),
             "td_table_new": (P, [C.c_int64]),
             "td_table_add_col": (P, [P, C.c_int64, P]),
             "td_table_get_col": (P, [P, C.c_int64]),
@@ -156,6 +157,18 @@ class Td:
         if arr.dtype == np.bool_:
             arr = arr.astype(np.uint8)
         return self.check(self.lib.td_vec_from_raw(typ, arr.ctypes.data, arr.size), "vec")
+
+    def sym_vec(self, ids, width):
+        """TD_SYM vector of the given dictionary ids at width TD_SYM_W8..W64 (0..3)."""
+        ids = np.asarray(ids)
+        n = len(ids)
+        p = self.check(self.lib.td_sym_vec_new(width, n), "sym_vec")
+        C.cast(p + 24, C.POINTER(C.c_int64))[0] = n
+        if n:
+            dt = SYM_NP[width]
+            buf = (C.c_char * (n * np.dtype(dt).itemsize)).from_address(p + 32)
+            np.frombuffer(buf, dt, n)[:] = ids.astype(dt)
+        return p
 
     def vec_alloc(self, typ, n):
         """New vector of n elements; returns (ptr, writable numpy view)."""

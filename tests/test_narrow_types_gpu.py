@@ -1,0 +1,156 @@
+"""Narrow and dictionary columns against Teide itself (compiled from its
+sources): SYM keys at every adaptive width (1, 2, 4, 8 bytes), I32/I16/U8
+keys and values, narrow MIN/MAX outputs, filters on narrow columns, joins on
+I32 keys.  SYM columns hold interned dictionary ids; the ids differ between
+the two libraries' symbol tables, so SYM keys are compared as strings.  The same tables go through the same td.h calls on both libraries;
+results are compared after a canonical sort -- integers exactly, F64 within
+1e-12 relative."""
+import numpy as np
+import pytest
+
+import oracle
+from gpu_pipelines import const
+from teide_b200.td import I16, I32, OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM, U8
+
+pytestmark = pytest.mark.gpu
+
+N = 200_000
+
+
+NSYM = {0: 100, 1: 5_000, 2: 70_000, 3: 100_000}
+
+
+def _sym_ids(td, n):
+    """Interned ids of the dictionary strings "w0".."w<n-1>" in this library."""
+    ids = np.array([td.sym(f"w{i}") for i in range(n)], dtype=np.int64)
+    return ids
+
+
+def _tables(td, seed, sym_w):
+    r = np.random.default_rng(seed)
+    d = {"s": r.integers(0, NSYM[sym_w], N), "k32": r.integers(-500, 500, N).astype(np.int32),
+         "v64": r.integers(-10**9, 10**9, N), "v32": r.integers(-2**31, 2**31 - 1, N).astype(np.int32),
+         "v16": r.integers(-30_000, 30_000, N).astype(np.int16), "u8": r.integers(0, 256, N).astype(np.uint8),
+         "f": r.standard_normal(N)}
+    ids = _sym_ids(td, NSYM[sym_w])
+    if ids.max() >= 1 << (8 << sym_w) and sym_w < 3:
+        pytest.skip("the symbol table already holds too many names for this SYM width")
+    sv = td.sym_vec(ids[d["s"]], sym_w)
+    t = td.table({"s": sv, "k32": (d["k32"], I32), "v64": d["v64"], "v32": (d["v32"], I32),
+                  "v16": (d["v16"], I16), "u8": (d["u8"], U8), "f": d["f"]})
+    td.release(sv)
+    return t
+
+
+def _group(td, t, keys, aggs, pred=None):
+    """Plain group graph, after a filter graph when pred is given (Teide's
+    two-graph form)."""
+    src = t
+    if pred:
+        g = td.graph(t)
+        try:
+            c, op, k = pred
+            src = td.check(td.lib.td_execute(g.g, g.filter(g.const_table(t), g.op(op, g.scan(c), const(g, k)))))
+        finally:
+            g.free()
+    g = td.graph(src)
+    try:
+        r = td.check(td.lib.td_execute(g.g, g.group([g.scan(n) for n in keys], [a for a, _ in aggs],
+                                                     [g.scan(n) for _, n in aggs])))
+    finally:
+        g.free()
+    out = td.table_dict(r)
+    td.release(r)
+    if src != t:
+        td.release(src)
+    return out
+
+
+def _names(td, out, col="s"):
+    """Replace a SYM result column's ids by their strings (ids differ per library)."""
+    if col in out:
+        u, inv = np.unique(out[col], return_inverse=True)
+        out[col] = np.array([td.sym_name(int(x)) for x in u], dtype=object)[inv]
+    return out
+
+
+def _same(a, b, by):
+    a, b = oracle.canonical(a, by=by), oracle.canonical(b, by=by)
+    assert list(a) == list(b)
+    for k in a:
+        assert a[k].dtype == b[k].dtype, k
+        if a[k].dtype.kind == "f":
+            assert np.allclose(a[k], b[k], rtol=1e-12, atol=1e-12), k
+        else:
+            assert np.array_equal(a[k], b[k]), k
+
+
+# Teide's group-by mishandles MIN/MAX over columns narrower than 8 bytes (a
+# 10-row MAX over an I16 column crashes it; larger ones return columns with
+# corrupt type and name words), so comparisons with Teide use COUNT, SUM and
+# AVG of every width plus MIN/MAX of 8-byte columns, and the narrow MIN/MAX
+# outputs are checked against the oracle (test_narrow_min_max_matches_oracle).
+AGGS = [(OP_COUNT, "v64"), (OP_SUM, "v64"), (OP_MIN, "v64"), (OP_MAX, "f"), (OP_SUM, "v32"), (OP_SUM, "v16"),
+        (OP_SUM, "u8"), (OP_AVG, "v16")]
+NARROW = [(OP_MAX, "v16"), (OP_MIN, "v16"), (OP_MIN, "u8"), (OP_MAX, "u8"), (OP_MAX, "k32")]
+
+
+@pytest.mark.parametrize("sym_w", [0, 1, 2, 3])
+def test_sym_key_group_matches_teide(gpu, ref, sym_w):
+    tg, tr = _tables(gpu, 90 + sym_w, sym_w), _tables(ref, 90 + sym_w, sym_w)
+    try:
+        _same(_names(gpu, _group(gpu, tg, ["s"], AGGS)), _names(ref, _group(ref, tr, ["s"], AGGS)), ["s"])
+    finally:
+        gpu.release(tg)
+        ref.release(tr)
+
+
+@pytest.mark.parametrize("pred", [None, ("k32", "gt", 0), ("v16", "lt", 100), ("u8", "ge", 128)])
+def test_narrow_keys_and_filters_match_teide(gpu, ref, pred):
+    tg, tr = _tables(gpu, 95, 1), _tables(ref, 95, 1)
+    try:
+        for keys in (["k32"], ["k32", "s"], ["u8"]):
+            _same(_names(gpu, _group(gpu, tg, keys, AGGS, pred)), _names(ref, _group(ref, tr, keys, AGGS, pred)), keys)
+    finally:
+        gpu.release(tg)
+        ref.release(tr)
+
+
+def test_i32_join_matches_teide(gpu, ref):
+    r = np.random.default_rng(97)
+    nb, npr = 20_000, 200_000
+    b = {"pk": (r.permutation(nb).astype(np.int32), I32), "cat": (r.integers(0, 50, nb).astype(np.int16), I16)}
+    p = {"fk": (r.integers(0, 24_000, npr).astype(np.int32), I32), "q": r.integers(0, 100, npr)}
+    outs = []
+    for td in (gpu, ref):
+        bt, pt = td.table(b), td.table(p)
+        g = td.graph(pt)
+        try:
+            left = g.filter(g.const_table(pt), g.op("gt", g.scan("q"), g.i64(20)))
+            jr = td.check(td.lib.td_execute(g.g, g.join(left, [g.scan("fk")], g.const_table(bt), [g.scan("pk")], 0)))
+        finally:
+            g.free()
+        outs.append(td.table_dict(jr))
+        td.release(jr)
+        td.release(bt)
+        td.release(pt)
+    _same(outs[0], outs[1], ["fk", "q", "cat"])
+
+
+@pytest.mark.parametrize("sym_w", [2])
+def test_narrow_min_max_matches_oracle(gpu, sym_w):
+    r = np.random.default_rng(99)
+    d = {"s": r.integers(0, 3000, N), "k32": r.integers(-500, 500, N).astype(np.int32),
+         "v16": r.integers(-30_000, 30_000, N).astype(np.int16), "u8": r.integers(0, 256, N).astype(np.uint8)}
+    ids = _sym_ids(gpu, 3000)
+    sv = gpu.sym_vec(ids[d["s"]], sym_w)
+    t = gpu.table({"s": sv, "k32": (d["k32"], I32), "v16": (d["v16"], I16), "u8": (d["u8"], U8)})
+    gpu.release(sv)
+    try:
+        got = _group(gpu, t, ["s"], NARROW)
+        want = oracle.group({"s": ids[d["s"]]}, [(op, c, d[c]) for op, c in NARROW])
+        assert got["s"].dtype == np.uint32
+        got["s"] = got["s"].astype(np.int64)
+        _same(got, want, ["s"])
+    finally:
+        gpu.release(t)
