@@ -240,12 +240,34 @@ __global__ void __launch_bounds__(kBatchMaxThreads) k_batch_agg(const BatchK B) 
                 unsigned long long* base = B.rec + Q.acc_off * B.W;
 #pragma unroll
                 for (int j = 0; j < kBR; j++) if (ok[j]) atomicAdd(base + k[j] * B.W, 1ULL);
-                for (int a = 0; a < B.na; a++)
-                    if (B.ai[a] >= 0) {
+                for (int a = 0; a < B.na; a++) {
+                    const int kind = B.kind[a];
+                    if (B.ai[a] < 0) continue;
+                    const int w = 1 + B.ai[a];
+                    if (kind == BK_SUM_I || kind == BK_SUM_F) {
 #pragma unroll
                         for (int j = 0; j < kBR; j++)
-                            if (ok[j]) bupd(base + k[j] * B.W + 1 + B.ai[a], B.kind[a], iv[j], fv[j], true);
+                            if (ok[j]) bupd(base + k[j] * B.W + w, kind, iv[j], fv[j], true);
+                        continue;
                     }
+                    // MIN/MAX: the four rows' current values are read together (one
+                    // L2 round trip, not four), then only the rows that can win update
+                    const bool fk = kind == BK_MIN_F || kind == BK_MAX_F;
+                    const bool mn = kind == BK_MIN_I || kind == BK_MIN_F;
+                    long long cur[kBR], v[kBR];
+#pragma unroll
+                    for (int j = 0; j < kBR; j++) {
+                        v[j] = fk ? f2ord(fv[j]) : iv[j];
+                        cur[j] = ok[j] ? __ldcg((const long long*)(base + k[j] * B.W + w)) : 0;
+                    }
+#pragma unroll
+                    for (int j = 0; j < kBR; j++) {
+                        if (!ok[j] || (fk && fv[j] != fv[j])) continue;
+                        long long* t = (long long*)(base + k[j] * B.W + w);
+                        if (mn) { if (v[j] < cur[j]) atomicMin(t, v[j]); }
+                        else if (v[j] > cur[j]) atomicMax(t, v[j]);
+                    }
+                }
             }
         }
         if (use_smem) {
