@@ -298,7 +298,7 @@ typedef struct tdg_batch_plan {
     int32_t smem_bytes;    /* dynamic shared memory per CTA */
     int32_t query_base;    /* added to every emitted query index (0 from plan_make;
                               a caller running a batch in parts sets it per part) */
-    int32_t pad;
+    int32_t n_pieces;      /* emit units: each query's slots in pieces of 4096 */
 } tdg_batch_plan;
 
 typedef struct tdg_batch_out {

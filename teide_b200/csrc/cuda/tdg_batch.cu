@@ -48,8 +48,10 @@ struct BatchK {
     unsigned long long* rec;
     unsigned long long* counter;
     int32_t* err;
-    int64_t* qcount;
-    int64_t* qoff;
+    const int32_t* piece_q;       // emit piece -> query
+    const int64_t* piece_s0;      // emit piece -> first slot within the query
+    int64_t* pcount;              // groups per piece, then exclusive offsets
+    int64_t n_pieces;
     int32_t n_queries, W, na, smem_slots, query_base;
     int32_t kind[TDG_MAX_AGGS];
     int32_t ai[TDG_MAX_AGGS];
@@ -57,18 +59,21 @@ struct BatchK {
     unsigned long long finit[TDG_MAX_AGGS + 2];
 };
 
-struct BLayout { size_t hdr, q, item_q, qcount, qoff, rec, total; };
+struct BLayout { size_t hdr, q, item_q, piece_q, piece_s0, pcount, rec, total; };
 
 static size_t al(size_t x) { return (x + 255) & ~(size_t)255; }
 
-static BLayout blayout(int64_t n_queries, int64_t n_items, int64_t total_slots, int W) {
+constexpr int64_t kPiece = 4096;          // slots one emit CTA handles
+
+static BLayout blayout(int64_t n_queries, int64_t n_items, int64_t total_slots, int W, int64_t n_pieces) {
     BLayout L;
     size_t o = 0;
     L.hdr = o; o += 256;
     L.q = o; o += al((size_t)n_queries * sizeof(BQ));
     L.item_q = o; o += al((size_t)n_items * 4);
-    L.qcount = o; o += al((size_t)n_queries * 8);
-    L.qoff = o; o += al((size_t)(n_queries + 1) * 8);
+    L.piece_q = o; o += al((size_t)n_pieces * 4);
+    L.piece_s0 = o; o += al((size_t)n_pieces * 8);
+    L.pcount = o; o += al((size_t)(n_pieces + 1) * 8);
     L.rec = o; o += al((size_t)total_slots * 8 * W);
     L.total = o;
     return L;
@@ -82,14 +87,16 @@ __host__ __device__ inline unsigned long long binit(int kind) {
 static BatchK make_bk(const tdg_batch_plan* p, void* ws) {
     BatchK B;
     memset(&B, 0, sizeof(B));
-    const BLayout L = blayout(p->n_queries, p->n_items, p->total_slots, p->words);
+    const BLayout L = blayout(p->n_queries, p->n_items, p->total_slots, p->words, p->n_pieces);
     char* w = (char*)ws;
     B.counter = (unsigned long long*)(w + L.hdr);
     B.err = (int32_t*)(w + L.hdr + 16);
     B.q = (const BQ*)(w + L.q);
     B.item_q = (const int32_t*)(w + L.item_q);
-    B.qcount = (int64_t*)(w + L.qcount);
-    B.qoff = (int64_t*)(w + L.qoff);
+    B.piece_q = (const int32_t*)(w + L.piece_q);
+    B.piece_s0 = (const int64_t*)(w + L.piece_s0);
+    B.pcount = (int64_t*)(w + L.pcount);
+    B.n_pieces = p->n_pieces;
     B.rec = (unsigned long long*)(w + L.rec);
     B.n_items = p->n_items;
     B.total_slots = p->total_slots;
@@ -284,23 +291,29 @@ __global__ void __launch_bounds__(kBatchMaxThreads) k_batch_agg(const BatchK B) 
     }
 }
 
+// Emit runs in pieces of kPiece slots (one CTA each), so a query with a wide
+// key range is counted and written by many CTAs; pieces are ordered by query,
+// then slot, so the scan of piece counts keeps queries in order and keys
+// ascending within a query.
 __global__ void __launch_bounds__(kEmitBlock) k_batch_count(const BatchK B) {
     __shared__ int red[32];
-    const BQ Q = B.q[blockIdx.x];
+    const int64_t i = blockIdx.x;
+    const BQ& Q = B.q[B.piece_q[i]];
+    const int64_t s0 = B.piece_s0[i], s1 = s0 + kPiece < Q.n_slots ? s0 + kPiece : Q.n_slots;
     int c = 0;
-    for (int64_t s = threadIdx.x; s < Q.n_slots; s += blockDim.x) c += B.rec[(Q.acc_off + s) * B.W] != 0;
+    for (int64_t s = s0 + threadIdx.x; s < s1; s += blockDim.x) c += B.rec[(Q.acc_off + s) * B.W] != 0;
     int tot;
     block_excl_scan(c, &tot, red);
-    if (threadIdx.x == 0) B.qcount[blockIdx.x] = tot;
+    if (threadIdx.x == 0) B.pcount[i] = tot;
 }
 
 __global__ void __launch_bounds__(1024) k_batch_scan(const BatchK B, int64_t* d_total) {
     __shared__ long long part[1024];
-    const int64_t m = B.n_queries;
+    const int64_t m = B.n_pieces;
     const int64_t per = (m + blockDim.x - 1) / blockDim.x;
     const int64_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
     long long sum = 0;
-    for (int64_t i = b; i < e; i++) sum += B.qcount[i];
+    for (int64_t i = b; i < e; i++) sum += B.pcount[i];
     part[threadIdx.x] = sum;
     __syncthreads();
     for (int o = 1; o < (int)blockDim.x; o <<= 1) {
@@ -310,9 +323,9 @@ __global__ void __launch_bounds__(1024) k_batch_scan(const BatchK B, int64_t* d_
         __syncthreads();
     }
     long long run = threadIdx.x ? part[threadIdx.x - 1] : 0;
-    for (int64_t i = b; i < e; i++) { B.qoff[i] = run; run += B.qcount[i]; }
+    for (int64_t i = b; i < e; i++) { const long long c = B.pcount[i]; B.pcount[i] = run; run += c; }
     if (threadIdx.x == blockDim.x - 1) {
-        B.qoff[m] = part[blockDim.x - 1];
+        B.pcount[m] = part[blockDim.x - 1];
         // a key outside its query's [key_min, key_min + n_slots) range is
         // reported as a negative row count (the host maps it to an error)
         *d_total = *(volatile int32_t*)B.err ? -1 : part[blockDim.x - 1];
@@ -327,12 +340,14 @@ struct BOut {
 
 __global__ void __launch_bounds__(kEmitBlock) k_batch_emit(const BatchK B, const BOut O) {
     __shared__ int red[32];
-    const int q = blockIdx.x;
-    const BQ Q = B.q[q];
-    int64_t out = B.qoff[q];
-    for (int64_t s0 = 0; s0 < Q.n_slots; s0 += blockDim.x) {
+    const int64_t i = blockIdx.x;
+    const int q = B.piece_q[i];
+    const BQ& Q = B.q[q];
+    const int64_t p0 = B.piece_s0[i], p1 = p0 + kPiece < Q.n_slots ? p0 + kPiece : Q.n_slots;
+    int64_t out = B.pcount[i];
+    for (int64_t s0 = p0; s0 < p1; s0 += blockDim.x) {
         const int64_t s = s0 + threadIdx.x;
-        const unsigned long long* rec = s < Q.n_slots ? B.rec + (Q.acc_off + s) * B.W : nullptr;
+        const unsigned long long* rec = s < p1 ? B.rec + (Q.acc_off + s) * B.W : nullptr;
         const unsigned long long c = rec ? rec[0] : 0;
         int tot;
         const int pre = block_excl_scan(c ? 1 : 0, &tot, red);
@@ -414,6 +429,7 @@ extern "C" tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_
     p->smem_slots = (int32_t)((budget - 8) / (4 + 8 * (size_t)n_acc));
     p->smem_bytes = (int32_t)(((((size_t)p->smem_slots * 4) + 7) & ~(size_t)7) + (size_t)p->smem_slots * 8 * n_acc);
     p->val_f64 = d->n_queries > 0 && d->queries[0].val.type == T_F64;
+    int64_t pieces = 0;
     for (int i = 0; i < d->n_queries; i++) {
         const tdg_batch_query& q = d->queries[i];
         if (!is_int_class(q.key.type) || !elem_size(q.val.type, q.val.attrs)) return E_TYPE;
@@ -425,17 +441,22 @@ extern "C" tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_
         const int64_t t = query_tile(q, p);
         p->n_items += (q.nrows + t - 1) / t;
         p->total_slots += q.n_slots;
+        pieces += (q.n_slots + kPiece - 1) / kPiece;
     }
-    if (p->n_items > INT32_MAX) return E_RANGE;
-    p->ws_bytes = blayout(p->n_queries, p->n_items, p->total_slots, p->words).total;
+    if (p->n_items > INT32_MAX || pieces > INT32_MAX) return E_RANGE;
+    p->n_pieces = (int32_t)pieces;
+    p->ws_bytes = blayout(p->n_queries, p->n_items, p->total_slots, p->words, p->n_pieces).total;
     return E_OK;
 }
 
 extern "C" tdg_status tdg_batch_prepare(const tdg_batch_desc* d, const tdg_batch_plan* p, void* ws, void* stream) {
     if (!d || !p || !ws) return E_TYPE;
-    const BLayout L = blayout(p->n_queries, p->n_items, p->total_slots, p->words);
+    const BLayout L = blayout(p->n_queries, p->n_items, p->total_slots, p->words, p->n_pieces);
     std::vector<BQ> qs((size_t)p->n_queries);
     std::vector<int32_t> item_q((size_t)p->n_items);
+    std::vector<int32_t> piece_q((size_t)p->n_pieces);
+    std::vector<int64_t> piece_s0((size_t)p->n_pieces);
+    int64_t piece = 0;
     int64_t acc = 0, item = 0;
     for (int i = 0; i < p->n_queries; i++) {
         const tdg_batch_query& q = d->queries[i];
@@ -449,8 +470,12 @@ extern "C" tdg_status tdg_batch_prepare(const tdg_batch_desc* d, const tdg_batch
         for (int64_t t = 0; t < tiles; t++) item_q[(size_t)(item + t)] = i;
         item += tiles;
         acc += q.n_slots;
+        for (int64_t s0 = 0; s0 < q.n_slots && piece < p->n_pieces; s0 += kPiece, piece++) {
+            piece_q[(size_t)piece] = i;
+            piece_s0[(size_t)piece] = s0;
+        }
     }
-    if (item != p->n_items || acc != p->total_slots) return E_RANGE;
+    if (item != p->n_items || acc != p->total_slots || piece != p->n_pieces) return E_RANGE;
     if (p->smem_bytes > 48 * 1024 &&
         cudaFuncSetAttribute((const void*)k_batch_agg, cudaFuncAttributeMaxDynamicSharedMemorySize, p->smem_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -461,6 +486,8 @@ extern "C" tdg_status tdg_batch_prepare(const tdg_batch_desc* d, const tdg_batch
     if (cudaMemsetAsync(w + L.hdr, 0, 256, s) != cudaSuccess ||
         (p->n_queries && cudaMemcpyAsync(w + L.q, qs.data(), qs.size() * sizeof(BQ), cudaMemcpyHostToDevice, s) != cudaSuccess) ||
         (p->n_items && cudaMemcpyAsync(w + L.item_q, item_q.data(), item_q.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+        (p->n_pieces && cudaMemcpyAsync(w + L.piece_q, piece_q.data(), piece_q.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) ||
+        (p->n_pieces && cudaMemcpyAsync(w + L.piece_s0, piece_s0.data(), piece_s0.size() * 8, cudaMemcpyHostToDevice, s) != cudaSuccess) ||
         cudaStreamSynchronize(s) != cudaSuccess) {
         cudaGetLastError();
         return E_IO;
@@ -506,9 +533,9 @@ extern "C" tdg_status tdg_batch_run(const tdg_batch_plan* p, void* ws, const tdg
     O.key = out->key;
     for (int a = 0; a < p->n_aggs; a++) O.aggs[a] = out->aggs[a];
     if (p->n_queries > 0) {
-        (note_launch(), k_batch_count<<<(unsigned)p->n_queries, kEmitBlock, 0, s>>>(B));
+        (note_launch(), k_batch_count<<<(unsigned)p->n_pieces, kEmitBlock, 0, s>>>(B));
         (note_launch(), k_batch_scan<<<1, 1024, 0, s>>>(B, out->d_n_rows));
-        (note_launch(), k_batch_emit<<<(unsigned)p->n_queries, kEmitBlock, 0, s>>>(B, O));
+        (note_launch(), k_batch_emit<<<(unsigned)p->n_pieces, kEmitBlock, 0, s>>>(B, O));
     } else {
         cudaMemsetAsync(out->d_n_rows, 0, 8, s);
     }
