@@ -571,6 +571,100 @@ __device__ __forceinline__ void ld_pair(const tdg_col& c, int64_t r, int64_t n, 
     }
 }
 
+// One tile of the vector form: every column the rows need is loaded up front,
+// then each row's slot comes either from the join's payload map (MAP: the
+// probe key indexes it) or from a single group key (slot = key - key_min),
+// and the rows aggregate into the shared-memory accumulators.
+template <int NT, int NV, bool MAP>
+__device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, const Pred& P, const VecAgg& A,
+                                         const tdg_col& kcol, int64_t kmin, int64_t n_map,
+                                         const uint32_t* __restrict__ map, int64_t n, int64_t base) {
+    int64_t row[4];
+    long long fk[4], tv[NT > 0 ? NT : 1][4], vv[1][4];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const int64_t r = base + (int64_t)j * 2 * kThreads + 2 * threadIdx.x;
+        row[2 * j] = r;
+        row[2 * j + 1] = r + 1;
+        ld_pair(kcol, r, n, fk[2 * j], fk[2 * j + 1]);
+#pragma unroll
+        for (int t = 0; t < NT; t++) ld_pair(P.t[t].col, r, n, tv[t][2 * j], tv[t][2 * j + 1]);
+#pragma unroll
+        for (int c = 0; c < NV; c++) ld_pair(A.vc[c], r, n, vv[c][2 * j], vv[c][2 * j + 1]);
+    }
+    int64_t slot[4];
+    bool ok[4];
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        bool m = row[i] < n;
+#pragma unroll
+        for (int t = 0; t < NT; t++) {
+            const Term& T = P.t[t];
+            bool b;
+            if (T.f) {
+                const double v = __longlong_as_double(tv[t][i]);
+                b = (v >= __longlong_as_double(T.lo)) & (v <= __longlong_as_double(T.hi));
+            } else {
+                b = (tv[t][i] >= T.lo) & (tv[t][i] <= T.hi);
+            }
+            m = m && (b != (bool)T.neg);
+        }
+        const int64_t k = fk[i] - kmin;
+        if (MAP) {
+            const bool in = m && k >= 0 && k < n_map;
+            const uint32_t pl = in ? __ldg(map + k) : 0xFFFFFFFFu;
+            ok[i] = pl != 0xFFFFFFFFu;
+            slot[i] = pl;
+        } else {
+            const bool in = k >= 0 && k < n_map;
+            if (m && !in) set_err(G.err, E_DOMAIN);
+            ok[i] = m && in;
+            slot[i] = k;
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 4; i++) if (ok[i]) atomicAdd(&V.cnt[slot[i]], 1u);
+    for (int a = 0; a < G.na; a++) {
+        const int kind = G.kind[a];
+        if (kind == K_COUNT || NV == 0) continue;
+        unsigned long long* acc = V.acc + (int64_t)G.ai[a] * V.cap;
+        const long long (&w)[4] = vv[0];
+        switch (kind) {
+            case K_SUM_F:
+#pragma unroll
+                for (int i = 0; i < 4; i++) if (ok[i]) atomicAdd((double*)(acc + slot[i]), __longlong_as_double(w[i]));
+                break;
+            case K_SUM_I:
+#pragma unroll
+                for (int i = 0; i < 4; i++) if (ok[i]) atomicAdd(acc + slot[i], (unsigned long long)w[i]);
+                break;
+            case K_MIN_I:
+#pragma unroll
+                for (int i = 0; i < 4; i++) if (ok[i]) atomicMin((long long*)(acc + slot[i]), w[i]);
+                break;
+            case K_MAX_I:
+#pragma unroll
+                for (int i = 0; i < 4; i++) if (ok[i]) atomicMax((long long*)(acc + slot[i]), w[i]);
+                break;
+            case K_MIN_F:
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const double v = __longlong_as_double(w[i]);
+                    if (ok[i] && v == v) atomicMin((long long*)(acc + slot[i]), f2ord(v));
+                }
+                break;
+            case K_MAX_F:
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    const double v = __longlong_as_double(w[i]);
+                    if (ok[i] && v == v) atomicMax((long long*)(acc + slot[i]), f2ord(v));
+                }
+                break;
+            default: break;
+        }
+    }
+}
+
 template <int NT, int NV>
 __global__ void __launch_bounds__(kThreads, TDG_MINB) k_probe_vec(const GroupK G, const Pred P, const VecAgg A,
                                                                   const tdg_col lkey, int64_t kmin, int64_t n_map,
@@ -581,83 +675,22 @@ __global__ void __launch_bounds__(kThreads, TDG_MINB) k_probe_vec(const GroupK G
     for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
         const int64_t nb = base + (int64_t)gridDim.x * tile;
         prefetch_rows(G.pf, nb, nb + tile < n ? nb + tile : n);
-        int64_t row[4];
-        long long fk[4], tv[NT > 0 ? NT : 1][4], vv[1][4];
-#pragma unroll
-        for (int j = 0; j < 2; j++) {
-            const int64_t r = base + (int64_t)j * 2 * kThreads + 2 * threadIdx.x;
-            row[2 * j] = r;
-            row[2 * j + 1] = r + 1;
-            ld_pair(lkey, r, n, fk[2 * j], fk[2 * j + 1]);
-#pragma unroll
-            for (int t = 0; t < NT; t++) ld_pair(P.t[t].col, r, n, tv[t][2 * j], tv[t][2 * j + 1]);
-#pragma unroll
-            for (int c = 0; c < NV; c++) ld_pair(A.vc[c], r, n, vv[c][2 * j], vv[c][2 * j + 1]);
-        }
-        int64_t slot[4];
-        bool ok[4];
-#pragma unroll
-        for (int i = 0; i < 4; i++) {
-            bool m = row[i] < n;
-#pragma unroll
-            for (int t = 0; t < NT; t++) {
-                const Term& T = P.t[t];
-                bool b;
-                if (T.f) {
-                    const double v = __longlong_as_double(tv[t][i]);
-                    b = (v >= __longlong_as_double(T.lo)) & (v <= __longlong_as_double(T.hi));
-                } else {
-                    b = (tv[t][i] >= T.lo) & (tv[t][i] <= T.hi);
-                }
-                m = m && (b != (bool)T.neg);
-            }
-            const int64_t k = fk[i] - kmin;
-            const bool in = m && k >= 0 && k < n_map;
-            const uint32_t pl = in ? __ldg(map + k) : 0xFFFFFFFFu;
-            ok[i] = pl != 0xFFFFFFFFu;
-            slot[i] = pl;
-        }
-#pragma unroll
-        for (int i = 0; i < 4; i++) if (ok[i]) atomicAdd(&V.cnt[slot[i]], 1u);
-        for (int a = 0; a < G.na; a++) {
-            const int kind = G.kind[a];
-            if (kind == K_COUNT || NV == 0) continue;
-            unsigned long long* acc = V.acc + (int64_t)G.ai[a] * V.cap;
-            const long long (&w)[4] = vv[0];
-            switch (kind) {
-                case K_SUM_F:
-#pragma unroll
-                    for (int i = 0; i < 4; i++) if (ok[i]) atomicAdd((double*)(acc + slot[i]), __longlong_as_double(w[i]));
-                    break;
-                case K_SUM_I:
-#pragma unroll
-                    for (int i = 0; i < 4; i++) if (ok[i]) atomicAdd(acc + slot[i], (unsigned long long)w[i]);
-                    break;
-                case K_MIN_I:
-#pragma unroll
-                    for (int i = 0; i < 4; i++) if (ok[i]) atomicMin((long long*)(acc + slot[i]), w[i]);
-                    break;
-                case K_MAX_I:
-#pragma unroll
-                    for (int i = 0; i < 4; i++) if (ok[i]) atomicMax((long long*)(acc + slot[i]), w[i]);
-                    break;
-                case K_MIN_F:
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const double v = __longlong_as_double(w[i]);
-                        if (ok[i] && v == v) atomicMin((long long*)(acc + slot[i]), f2ord(v));
-                    }
-                    break;
-                case K_MAX_F:
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        const double v = __longlong_as_double(w[i]);
-                        if (ok[i] && v == v) atomicMax((long long*)(acc + slot[i]), f2ord(v));
-                    }
-                    break;
-                default: break;
-            }
-        }
+        vec_tile<NT, NV, true>(G, V, P, A, lkey, kmin, n_map, map, n, base);
+    }
+    smem_flush<0>(G, V);
+}
+
+// The same for a plain group-by with one key and shared-memory accumulators.
+template <int NT, int NV>
+__global__ void __launch_bounds__(kThreads, TDG_MINB) k_group_vec(const GroupK G, const Pred P, const VecAgg A,
+                                                                  int64_t n) {
+    extern __shared__ unsigned long long sm[];
+    const SmemView V = smem_setup<0>(G, sm);
+    const int64_t tile = (int64_t)kThreads * 4;
+    for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
+        const int64_t nb = base + (int64_t)gridDim.x * tile;
+        prefetch_rows(G.pf, nb, nb + tile < n ? nb + tile : n);
+        vec_tile<NT, NV, false>(G, V, P, A, G.key[0], G.kmin[0], G.krange[0], nullptr, n, base);
     }
     smem_flush<0>(G, V);
 }
@@ -1098,6 +1131,54 @@ static void set_prefetch(GroupK& G, const Pred& P, const tdg_expr& prog, int pk,
         if (G.kind[a] != K_COUNT && !G.in[a].side) pf_add(G.pf, G.in[a]);
 }
 
+// Value columns of the vector form: at most one distinct column, 16-byte
+// aligned, shared by every non-COUNT aggregate; false when they need more.
+static bool vec_aggs(const GroupK& G, VecAgg& A, int& nv) {
+    memset(&A, 0, sizeof(A));
+    nv = 0;
+    for (int a = 0; a < G.na; a++) {
+        A.vi[a] = -1;
+        if (G.kind[a] == K_COUNT) continue;
+        int c = 0;
+        while (c < nv && A.vc[c].data != G.in[a].data) c++;
+        if (c == nv) {
+            if (nv == 1 || !aligned16(G.in[a].data)) return false;
+            A.vc[nv++] = G.in[a];
+        }
+        A.vi[a] = c;
+    }
+    return true;
+}
+
+// Predicate terms of the vector form: the range form (or none), at most two
+// terms, aligned columns, and no more than two columns loaded besides the key.
+static bool vec_terms(int pk, const Pred& P, int nv, int* nt) {
+    if (P.sel || !(pk == 0 || (pk == 1 && P.n <= 2))) return false;
+    *nt = pk == 1 ? P.n : 0;
+    for (int t = 0; t < *nt; t++) if (!aligned16(P.t[t].col.data)) return false;
+    return *nt + nv <= 2;                       // larger shapes exceed the register budget
+}
+
+// Plain group-by with one 8-byte key and shared-memory accumulators in the
+// vector form; false when the shape does not qualify.
+static bool launch_group_vec(const GroupK& G, const Pred& P, int pk, int64_t n, cudaStream_t s, tdg_status* st) {
+    if (G.nk != 1 || G.key[0].type == T_F64 || !aligned16(G.key[0].data)) return false;
+    VecAgg A;
+    int nv, nt;
+    if (!vec_aggs(G, A, nv) || !vec_terms(pk, P, nv, &nt)) return false;
+    const size_t smem = smem_full_bytes(G.S, G.n_acc);
+#define TDG_GV(NTV, NVV)                                                                                \
+    if (nt == NTV && nv == NVV) {                                                                       \
+        const int g = grid_for((const void*)k_group_vec<NTV, NVV>, kThreads, smem, (n + 3) / 4);       \
+        (note_launch(), k_group_vec<NTV, NVV><<<g, kThreads, smem, s>>>(G, P, A, n));                   \
+        *st = launch_status();                                                                          \
+        return true;                                                                                    \
+    }
+    TDG_GV(0, 0) TDG_GV(0, 1) TDG_GV(1, 0) TDG_GV(1, 1) TDG_GV(2, 0)
+#undef TDG_GV
+    return false;
+}
+
 template <bool JOIN>
 static tdg_status dispatch(int pk, const GroupK& G0, bool smem, const Pred& P, const tdg_expr& prog,
                            const JoinK& J, int64_t n, cudaStream_t s, EventTimer& tm) {
@@ -1113,6 +1194,7 @@ static tdg_status dispatch(int pk, const GroupK& G0, bool smem, const Pred& P, c
     }
     const bool w8 = pk != 2 && group_w8(G, P, JOIN ? &J : nullptr);
     tm.start(s);
+    if (!JOIN && mode == 0 && w8 && n > 0 && launch_group_vec(G, P, pk, n, s, &st)) { tm.stop(s); return st; }
 #define TDG_CASE(PKV, MV, W) \
     if (pk == PKV && mode == MV && w8 == W) { st = launch_main<PKV, MV, JOIN, W>(G, P, prog, J, n, s); tm.stop(s); return st; }
     TDG_CASE(0, 0, true) TDG_CASE(0, 1, true) TDG_CASE(0, 2, true)
@@ -1172,24 +1254,10 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     tm.start(s);
     // the vector form, when the shape and the alignment allow it
     VecAgg A;
-    memset(&A, 0, sizeof(A));
-    int nv = 0;
-    bool vec = sm && w8 && (pk == 0 || (pk == 1 && P.n <= 2)) && !P.sel && aligned16(J->lkeys[0].data);
+    int nv = 0, nt = 0;
+    bool vec = sm && w8 && aligned16(J->lkeys[0].data);
     for (int k = 0; k < G.nk && vec; k++) vec = G.key[k].side == 1;
-    for (int t = 0; pk == 1 && t < P.n && vec; t++) vec = aligned16(P.t[t].col.data);
-    for (int a = 0; a < G.na && vec; a++) {
-        A.vi[a] = -1;
-        if (G.kind[a] == K_COUNT) continue;
-        int c = 0;
-        while (c < nv && A.vc[c].data != G.in[a].data) c++;
-        if (c == nv) {
-            if (nv == 1 || !aligned16(G.in[a].data)) { vec = false; break; }   // one value column
-            A.vc[nv++] = G.in[a];
-        }
-        A.vi[a] = c;
-    }
-    const int nt = pk == 1 ? P.n : 0;
-    if (nt + nv > 2) vec = false;               // larger shapes exceed the register budget
+    vec = vec && vec_aggs(G, A, nv) && vec_terms(pk, P, nv, &nt);
     bool launched = false;
 #define TDG_PV(NTV, NVV)                                                                                  \
     if (vec && !launched && nt == NTV && nv == NVV) {                                                     \

@@ -1,0 +1,105 @@
+"""The plain group-by's vector form (one 8-byte key, shared-memory
+accumulators, every column read with 16-byte loads) and its fallbacks: odd
+row counts (the last pair is half full), negative key ranges, a table view
+starting at an odd row (columns not 16-byte aligned: the general kernel
+runs), no filter, one and two filter terms, COUNT only and F64 / I64
+SUM, MIN and MAX -- each against the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+from gpu_pipelines import const
+from teide_b200 import serve
+from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(n, seed, lo=0, span=64):
+    r = np.random.default_rng(seed)
+    return {"flag": r.integers(0, 4, n, dtype=np.int64),
+            "region": r.integers(lo, lo + span, n, dtype=np.int64),
+            "amount": r.random(n) * 1000.0,
+            "qty": r.integers(-500, 500, n, dtype=np.int64)}
+
+
+def _run(td, tbl, preds, aggs):
+    g = td.graph(tbl)
+    try:
+        p = None
+        for c, op, k in preds:
+            q = g.op(op, g.scan(c), const(g, k))
+            p = q if p is None else g.op("and", p, q)
+        f = (lambda v: v) if p is None else (lambda v: g.filter(v, p))
+        r = g.execute(g.group([f(g.scan("region"))], [a for a, _ in aggs], [f(g.scan(n)) for _, n in aggs]),
+                      optimize=True)
+    finally:
+        g.free()
+    out = td.table_dict(r)
+    td.release(r)
+    return out
+
+
+def _want(d, preds, aggs):
+    m = np.ones(len(d["region"]), bool)
+    for c, op, k in preds:
+        m &= oracle.compare(op, d[c], k)
+    return oracle.group({"region": d["region"][m]},
+                        [(op, n, None if op == OP_COUNT else d[n][m]) for op, n in aggs])
+
+
+def _same(got, want):
+    assert list(got) == list(want)
+    for k in want:
+        if want[k].dtype.kind == "f":
+            assert np.allclose(got[k], want[k], rtol=1e-12, atol=1e-9), k
+        else:
+            assert np.array_equal(got[k], want[k]), k
+
+
+CASES = [
+    ([("flag", "eq", 0)], [(OP_SUM, "amount")]),
+    ([], [(OP_COUNT, "amount")]),
+    ([], [(OP_SUM, "amount"), (OP_MAX, "amount"), (OP_MIN, "amount")]),
+    ([("flag", "eq", 1), ("qty", "lt", 100)], [(OP_COUNT, "qty")]),
+    ([("qty", "ge", -20), ("qty", "le", 300)], [(OP_SUM, "qty"), (OP_MIN, "qty"), (OP_MAX, "qty")]),
+    ([("amount", "gt", 250.0)], [(OP_SUM, "qty"), (OP_COUNT, "qty"), (OP_AVG, "qty")]),
+    ([("flag", "ne", 2)], [(OP_SUM, "amount"), (OP_AVG, "amount"), (OP_COUNT, "amount")]),
+]
+
+
+@pytest.mark.parametrize("preds,aggs", CASES)
+@pytest.mark.parametrize("n,lo", [(400_001, 0), (400_000, -37), (3, 5)])
+def test_vector_group_shapes(gpu, preds, aggs, n, lo):
+    d = _data(n, seed=91 + n % 7, lo=lo)
+    t = gpu.table(d)
+    try:
+        _same(_run(gpu, t, preds, aggs), _want(d, preds, aggs))
+    finally:
+        gpu.release(t)
+
+
+def test_unaligned_view_falls_back(gpu):
+    d = _data(300_000, seed=92)
+    t = gpu.table(d)
+    view = serve.table_slice(gpu, t, 1, 250_001)          # starts 8 bytes into each column
+    try:
+        preds, aggs = CASES[0]
+        sub = {k: v[1:250_002] for k, v in d.items()}
+        _same(_run(gpu, view, preds, aggs), _want(sub, preds, aggs))
+    finally:
+        gpu.release(view)
+        gpu.release(t)
+
+
+def test_wide_key_range_takes_other_kernels(gpu):
+    """A key range too wide for shared memory takes the global-array or hash
+    kernel (hash groups come back in slot order, so rows compare sorted)."""
+    d = _data(500_000, seed=93, lo=-1_000_000, span=2_000_000)
+    t = gpu.table(d)
+    try:
+        preds, aggs = CASES[0]
+        _same(oracle.canonical(_run(gpu, t, preds, aggs), by=["region"]),
+              oracle.canonical(_want(d, preds, aggs), by=["region"]))
+    finally:
+        gpu.release(t)
