@@ -665,7 +665,8 @@ def main():
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": profile_traffic(prof),
                      "kernel": {"join_group": "k_probe_vec (fused probe + aggregate)",
-                                "group_radix": "k_group",
+                                "group_radix": "k_group_vec + k_part_agg (hot slots in shared memory, cold rows "
+                                               "partitioned by slot range and aggregated per partition)",
                                 "readme_group": "k_group_vec (one key, 16-byte column loads)"}[args.workload],
                      "bytes_per_launch": main_bytes,
                      "mean_launch_ms": mean_main, "peak_source": peak_kind,

@@ -14,7 +14,15 @@
 //   MODE 0  every slot privatized per CTA in shared memory (32-bit counts,
 //           8-byte accumulators), merged into the global records once per CTA;
 //   MODE 1  direct array in global memory;
-//   MODE 2  hash table in global memory.
+//   MODE 2  hash table in global memory;
+//   MODE 3  direct array in global memory, one key, partitioned: hot slots
+//           aggregate in shared memory as in MODE 1, every other row becomes
+//           an entry (slot, values) of its slot range's partition, and a
+//           second pass aggregates each partition in shared memory and merges
+//           it into the records -- the partitioned aggregation of
+//           exec.c:6406-6667 with shared memory as the per-partition table,
+//           so cold rows cost streaming writes and reads instead of random or
+//           contended global atomics.
 // Global accumulators are slot-major records [count, acc_0, acc_1, ...] so
 // one row's updates touch at most two 32-byte sectors.  In MODES 1 and 2 a
 // sampling pass finds the slots that take a large share of the rows (Zipf
@@ -53,8 +61,39 @@ constexpr int64_t kSampleRows = (int64_t)1 << 18;
 constexpr int64_t kSampleCap = (int64_t)1 << 19;
 constexpr uint32_t kHotMin = 8;               // sampled hits that make a slot hot
 constexpr int64_t kSampleMinRows = (int64_t)1 << 22;
+constexpr int kHotHist = 1024;                // sampled-count histogram buckets (hot threshold)
+// MODE 3 (partitioned cold rows)
+constexpr int64_t kPartMinRows = (int64_t)1 << 20;   // smaller inputs keep MODE 1
+constexpr size_t kPartSmem = 96 * 1024;       // a partition's shared-memory table
+constexpr int kPartThreads = 512;
+constexpr int64_t kPartItem = 16384;          // entries per aggregation work item
+constexpr int kPartRegions = 1024;            // partitions below this are split into stripes
+constexpr int kPartMaxStripes = 64;
+constexpr uint32_t kPartMargin = 32;          // entries every region holds beyond its estimate
 
 enum : int32_t { K_COUNT = 0, K_SUM_I, K_SUM_F, K_MIN_I, K_MAX_I, K_MIN_F, K_MAX_F };
+
+// MODE 3: partition p holds slots [p << shift, (p + 1) << shift); its rows go
+// to `stripes` regions (region r = p * stripes + stripe, the stripe chosen by
+// the CTA) so that small partition counts do not serialize on one counter.
+// Region r holds cap[r] entries from base[r]: e_slot[e] and the values
+// e_val[j][e].  fill[r] counts reservations and may pass cap[r]; rows beyond
+// it update the global records directly.
+struct PartK {
+    int32_t shift, stripes;
+    int32_t ne, pad;              // values per entry
+    int64_t P, R;                 // partitions, regions
+    int64_t cap_total;            // entries the buffers hold
+    uint32_t* est;                // [P] sampled cold rows per partition
+    uint32_t* fill;               // [R]
+    uint32_t* cap;                // [R]
+    int64_t* base;                // [R]
+    int64_t* item_start;          // [R + 1] aggregation work items per region, prefix
+    int32_t* item_region;         // [R + cap_total / kPartItem + 1] region of each work item
+    uint32_t* item_next;          // work-item counter
+    uint32_t* e_slot;
+    unsigned long long* e_val[2];
+};
 
 struct GroupK {
     int32_t nk, na, method, n_acc;
@@ -74,7 +113,10 @@ struct GroupK {
     int64_t* sample_keys;
     uint32_t* sample_cnt;
     int64_t* hot;                 // hot slot list
-    int32_t* hot_n;
+    int32_t* hot_n;               // [0] hot slots, [1] sampled-count threshold; hot_hist follows
+    uint32_t* hot_hist;           // [kHotHist] sampled slots per count
+    int64_t sample_rows;          // rows the sample drew
+    PartK pk;                     // MODE 3 buffers (pk.P == 0: not planned)
     PfCols pf;                    // streamed columns the main kernels prefetch into L2
 };
 
@@ -462,11 +504,54 @@ __global__ void __launch_bounds__(kThreads) k_sample(const GroupK G, const Pred 
     }
 }
 
-__global__ void __launch_bounds__(kThreads) k_select_hot(const GroupK G) {
+// Histogram of the sampled slots by how often they were drawn.
+__global__ void __launch_bounds__(kThreads) k_hot_hist(const GroupK G) {
+    __shared__ uint32_t h[kHotHist];
+    for (int i = threadIdx.x; i < kHotHist; i += blockDim.x) h[i] = 0;
+    __syncthreads();
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < kSampleCap; e += (int64_t)gridDim.x * blockDim.x) {
-        if (G.sample_keys[e] == -1 || G.sample_cnt[e] < kHotMin) continue;
-        const int i = atomicAdd(G.hot_n, 1);
-        if (i < kHotMax) G.hot[i] = G.sample_keys[e];
+        if (G.sample_keys[e] == -1) continue;
+        const uint32_t c = G.sample_cnt[e];
+        atomicAdd(&h[c < (uint32_t)kHotHist ? c : kHotHist - 1], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kHotHist; i += blockDim.x) if (h[i]) atomicAdd(&G.hot_hist[i], h[i]);
+}
+
+// The hot threshold: the smallest count (at least kHotMin) whose slots --
+// every slot drawn at least that often -- fit one CTA's cache, so the cache
+// holds the most frequent slots.  hot_n[1] = kHotHist: no slot is hot.
+__global__ void __launch_bounds__(kHotHist) k_hot_threshold(const GroupK G) {
+    __shared__ uint32_t sfx[kHotHist];                 // slots drawn at least c times
+    const int c = threadIdx.x;
+    sfx[c] = G.hot_hist[c];
+    __syncthreads();
+    for (int off = 1; off < kHotHist; off <<= 1) {
+        const uint32_t v = c + off < kHotHist ? sfx[c + off] : 0u;
+        __syncthreads();
+        sfx[c] += v;
+        __syncthreads();
+    }
+    if (c == 0) G.hot_n[1] = kHotHist;
+    __syncthreads();
+    const uint32_t cap = (uint32_t)G.hot_cap;
+    if (c >= (int)kHotMin && sfx[c] <= cap && (c == (int)kHotMin || sfx[c - 1] > cap)) G.hot_n[1] = c;
+}
+
+// Slots at or above the threshold become the hot list; with MODE 3 planned,
+// every other sampled slot's draws count toward its partition's estimate.
+__global__ void __launch_bounds__(kThreads) k_select_hot(const GroupK G) {
+    const uint32_t t = (uint32_t)G.hot_n[1];
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < kSampleCap; e += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = G.sample_keys[e];
+        if (k == -1) continue;
+        const uint32_t c = G.sample_cnt[e] < (uint32_t)kHotHist ? G.sample_cnt[e] : kHotHist - 1;
+        if (c >= t) {
+            const int i = atomicAdd(G.hot_n, 1);
+            if (i < kHotMax) G.hot[i] = k;
+        } else if (G.pk.P) {
+            atomicAdd(&G.pk.est[k >> G.pk.shift], G.sample_cnt[e]);
+        }
     }
 }
 
@@ -547,16 +632,24 @@ __global__ void __launch_bounds__(kThreads, TDG_MINB) k_payload_probe(const Grou
     if (MODE == 0 || V.n_hot) smem_flush<MODE>(G, V);
 }
 
-// Vector form of k_payload_probe for its common shape (8-byte columns
-// aligned to 16 bytes, at most two predicate terms and one aggregate input
-// column between them, every group key on the build side, shared-memory
-// accumulators).  Each thread owns two pairs of adjacent rows and loads every
-// column it needs for them up front with 16-byte loads -- nothing waits for
-// the predicate or the join -- so the only dependent step left is the map
-// gather: two memory round trips per tile instead of four.
+// The vector form.  For the common shapes (8-byte columns aligned to 16
+// bytes, at most two predicate terms, at most two distinct columns read
+// besides the key -- a column that is both filtered and aggregated is read
+// once) each thread owns two pairs of adjacent rows and loads every column it
+// needs for them up front with 16-byte loads: nothing waits for the
+// predicate, so a tile costs one memory round trip (two for the join probe,
+// whose map gather depends on the key).  It serves
+//   k_probe_vec        the fused join probe (slot from the payload map);
+//   k_group_vec<0>     a one-key group-by with shared-memory accumulators;
+//   k_group_vec<1>     a one-key group-by over the global record array, with
+//                      the CTA's cache of sampled hot slots in shared memory.
 struct VecAgg {
-    int32_t vi[TDG_MAX_AGGS];    // aggregate -> value column index (-1: COUNT)
-    tdg_col vc[1];
+    int32_t vi[TDG_MAX_AGGS];    // aggregate -> loaded column (-1: COUNT)
+    int32_t ti[kMaxTerms];       // predicate term -> loaded column
+    int32_t ne;                  // MODE 3 values per entry
+    int32_t ec[2];               // MODE 3 entry value j -> loaded column
+    int32_t ve[TDG_MAX_AGGS];    // aggregate -> entry value (-1: COUNT)
+    tdg_col vc[2];               // the distinct columns read besides the key
 };
 
 __device__ __forceinline__ void ld_pair(const tdg_col& c, int64_t r, int64_t n, long long& a, long long& b) {
@@ -571,16 +664,45 @@ __device__ __forceinline__ void ld_pair(const tdg_col& c, int64_t r, int64_t n, 
     }
 }
 
-// One tile of the vector form: every column the rows need is loaded up front,
-// then each row's slot comes either from the join's payload map (MAP: the
-// probe key indexes it) or from a single group key (slot = key - key_min),
-// and the rows aggregate into the shared-memory accumulators.
-template <int NT, int NV, bool MAP>
+// Reductions on the shared window by address: always the shared-memory
+// atomic unit, whatever the compiler can prove about a pointer.
+__device__ __forceinline__ uint32_t sh_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void sh_add_u32(uint32_t a, uint32_t v) {
+    asm volatile("red.shared.add.u32 [%0], %1;" :: "r"(a), "r"(v) : "memory");
+}
+__device__ __forceinline__ void sh_add_u64(uint32_t a, unsigned long long v) {
+    asm volatile("red.shared.add.u64 [%0], %1;" :: "r"(a), "l"(v) : "memory");
+}
+__device__ __forceinline__ void sh_add_f64(uint32_t a, double v) {
+    asm volatile("red.shared.add.f64 [%0], %1;" :: "r"(a), "d"(v) : "memory");
+}
+__device__ __forceinline__ void sh_min_s64(uint32_t a, long long v) {
+    asm volatile("red.shared.min.s64 [%0], %1;" :: "r"(a), "l"(v) : "memory");
+}
+__device__ __forceinline__ void sh_max_s64(uint32_t a, long long v) {
+    asm volatile("red.shared.max.s64 [%0], %1;" :: "r"(a), "l"(v) : "memory");
+}
+__device__ __forceinline__ long long sh_ld_s64(uint32_t a) {
+    long long v;
+    asm volatile("ld.shared.s64 %0, [%1];" : "=l"(v) : "r"(a) : "memory");
+    return v;
+}
+
+template <int NC>
+__device__ __forceinline__ long long vec_pick(const long long (&cv)[NC > 0 ? NC : 1][4], int c, int i) {
+    return (NC > 1 && c == 1) ? cv[NC > 1 ? 1 : 0][i] : cv[0][i];
+}
+
+// One tile of 4 * kThreads rows.  MAP: the key indexes the join's payload
+// map, whose entry is the slot; otherwise slot = key - key_min.  MODE 0:
+// every slot has shared-memory accumulators; MODE 1: hot slots do, the rest
+// update the global records.
+template <int NT, int NC, int MODE, bool MAP>
 __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, const Pred& P, const VecAgg& A,
                                          const tdg_col& kcol, int64_t kmin, int64_t n_map,
                                          const uint32_t* __restrict__ map, int64_t n, int64_t base) {
     int64_t row[4];
-    long long fk[4], tv[NT > 0 ? NT : 1][4], vv[1][4];
+    long long fk[4], cv[NC > 0 ? NC : 1][4];
 #pragma unroll
     for (int j = 0; j < 2; j++) {
         const int64_t r = base + (int64_t)j * 2 * kThreads + 2 * threadIdx.x;
@@ -588,11 +710,10 @@ __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, con
         row[2 * j + 1] = r + 1;
         ld_pair(kcol, r, n, fk[2 * j], fk[2 * j + 1]);
 #pragma unroll
-        for (int t = 0; t < NT; t++) ld_pair(P.t[t].col, r, n, tv[t][2 * j], tv[t][2 * j + 1]);
-#pragma unroll
-        for (int c = 0; c < NV; c++) ld_pair(A.vc[c], r, n, vv[c][2 * j], vv[c][2 * j + 1]);
+        for (int c = 0; c < NC; c++) ld_pair(A.vc[c], r, n, cv[c][2 * j], cv[c][2 * j + 1]);
     }
     int64_t slot[4];
+    int hidx[4];
     bool ok[4];
 #pragma unroll
     for (int i = 0; i < 4; i++) {
@@ -600,12 +721,13 @@ __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, con
 #pragma unroll
         for (int t = 0; t < NT; t++) {
             const Term& T = P.t[t];
+            const long long x = vec_pick<NC>(cv, A.ti[t], i);
             bool b;
             if (T.f) {
-                const double v = __longlong_as_double(tv[t][i]);
+                const double v = __longlong_as_double(x);
                 b = (v >= __longlong_as_double(T.lo)) & (v <= __longlong_as_double(T.hi));
             } else {
-                b = (tv[t][i] >= T.lo) & (tv[t][i] <= T.hi);
+                b = (x >= T.lo) & (x <= T.hi);
             }
             m = m && (b != (bool)T.neg);
         }
@@ -621,51 +743,124 @@ __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, con
             ok[i] = m && in;
             slot[i] = k;
         }
+        hidx[i] = MODE == 0 ? (int)slot[i] : -1;
+        if (MODE != 0 && ok[i]) {
+            if (V.n_hot) hidx[i] = hot_find(V, slot[i]);
+            // a cold record's line is fetched now, so the four rows' DRAM
+            // round trips overlap
+            if (MODE == 1 && hidx[i] < 0)
+                asm volatile("{\n\t.reg .u64 g;\n\tcvta.to.global.u64 g, %0;\n\tprefetch.global.L2 [g];\n\t}"
+                             :: "l"(grec(G, slot[i])));
+        }
     }
+    if (MODE == 3) {
+        // cold rows become entries of their region; the lanes of a warp that
+        // share a region reserve their places with one atomic
+        const PartK& K = G.pk;
+        const unsigned lane = threadIdx.x & 31;
+        const uint32_t stripe = blockIdx.x & (uint32_t)(K.stripes - 1);
 #pragma unroll
-    for (int i = 0; i < 4; i++) if (ok[i]) atomicAdd(&V.cnt[slot[i]], 1u);
+        for (int i = 0; i < 4; i++) {
+            const bool cold = ok[i] && hidx[i] < 0;
+            const unsigned act = __ballot_sync(0xffffffffu, cold);
+            if (!cold) continue;
+            const uint32_t r = (uint32_t)(slot[i] >> K.shift) * (uint32_t)K.stripes + stripe;
+            const unsigned peers = __match_any_sync(act, r);
+            const int leader = __ffs(peers) - 1;
+            uint32_t pos = 0, cap = 0;
+            long long base = 0;
+            if ((int)lane == leader) {
+                pos = atomicAdd(&K.fill[r], (uint32_t)__popc(peers));
+                cap = K.cap[r];
+                base = K.base[r];
+            }
+            pos = __shfl_sync(peers, pos, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+            cap = __shfl_sync(peers, cap, leader);
+            base = __shfl_sync(peers, base, leader);
+            if (pos < cap) {
+                const int64_t e = base + pos;
+                K.e_slot[e] = (uint32_t)slot[i];
+#pragma unroll
+                for (int j = 0; j < 2; j++)
+                    if (j < K.ne) K.e_val[j][e] = (unsigned long long)vec_pick<NC>(cv, A.ec[j], i);
+                ok[i] = false;              // the partition pass aggregates it
+            }
+        }
+    }
+    // hot (shared-memory) and cold (global-record) updates are separate call
+    // sites; a MIN/MAX reads the shared extreme first, which stops moving
+    // after a slot's first rows, so most of those atomics are skipped
+    const uint32_t scnt = sh_addr(V.cnt);
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+        if (!ok[i]) continue;
+        if (MODE == 0 || hidx[i] >= 0) sh_add_u32(scnt + 4u * (uint32_t)hidx[i], 1u);
+        else atomicAdd(grec(G, slot[i]), 1ULL);
+    }
     for (int a = 0; a < G.na; a++) {
         const int kind = G.kind[a];
-        if (kind == K_COUNT || NV == 0) continue;
-        unsigned long long* acc = V.acc + (int64_t)G.ai[a] * V.cap;
-        const long long (&w)[4] = vv[0];
+        if (kind == K_COUNT || NC == 0) continue;
+        const int ai = G.ai[a];
+        const uint32_t sacc = sh_addr(V.acc + (int64_t)ai * V.cap);
+        const int c = A.vi[a];
+        long long w[4];
+        bool on[4];
+        const bool fl = kind == K_MIN_F || kind == K_MAX_F;
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            w[i] = vec_pick<NC>(cv, c, i);
+            on[i] = ok[i];
+            if (fl) {
+                const double d = __longlong_as_double(w[i]);
+                on[i] = ok[i] && d == d;               // MIN/MAX of F64 skip NaN
+                w[i] = f2ord(d);
+            }
+        }
+#define TDG_HOT(i) (MODE == 0 || hidx[i] >= 0)
+#define TDG_SA(i) (sacc + 8u * (uint32_t)hidx[i])
+#define TDG_GA(i) (grec(G, slot[i]) + 1 + ai)
         switch (kind) {
             case K_SUM_F:
 #pragma unroll
-                for (int i = 0; i < 4; i++) if (ok[i]) atomicAdd((double*)(acc + slot[i]), __longlong_as_double(w[i]));
+                for (int i = 0; i < 4; i++) {
+                    if (!on[i]) continue;
+                    if (TDG_HOT(i)) sh_add_f64(TDG_SA(i), __longlong_as_double(w[i]));
+                    else atomicAdd((double*)TDG_GA(i), __longlong_as_double(w[i]));
+                }
                 break;
             case K_SUM_I:
 #pragma unroll
-                for (int i = 0; i < 4; i++) if (ok[i]) atomicAdd(acc + slot[i], (unsigned long long)w[i]);
-                break;
-            case K_MIN_I:
-#pragma unroll
-                for (int i = 0; i < 4; i++) if (ok[i]) atomicMin((long long*)(acc + slot[i]), w[i]);
-                break;
-            case K_MAX_I:
-#pragma unroll
-                for (int i = 0; i < 4; i++) if (ok[i]) atomicMax((long long*)(acc + slot[i]), w[i]);
-                break;
-            case K_MIN_F:
-#pragma unroll
                 for (int i = 0; i < 4; i++) {
-                    const double v = __longlong_as_double(w[i]);
-                    if (ok[i] && v == v) atomicMin((long long*)(acc + slot[i]), f2ord(v));
+                    if (!on[i]) continue;
+                    if (TDG_HOT(i)) sh_add_u64(TDG_SA(i), (unsigned long long)w[i]);
+                    else atomicAdd(TDG_GA(i), (unsigned long long)w[i]);
                 }
                 break;
-            case K_MAX_F:
+            case K_MIN_I: case K_MIN_F:
 #pragma unroll
                 for (int i = 0; i < 4; i++) {
-                    const double v = __longlong_as_double(w[i]);
-                    if (ok[i] && v == v) atomicMax((long long*)(acc + slot[i]), f2ord(v));
+                    if (!on[i]) continue;
+                    if (TDG_HOT(i)) { if (w[i] < sh_ld_s64(TDG_SA(i))) sh_min_s64(TDG_SA(i), w[i]); }
+                    else upd_min<true>(TDG_GA(i), w[i]);
+                }
+                break;
+            case K_MAX_I: case K_MAX_F:
+#pragma unroll
+                for (int i = 0; i < 4; i++) {
+                    if (!on[i]) continue;
+                    if (TDG_HOT(i)) { if (w[i] > sh_ld_s64(TDG_SA(i))) sh_max_s64(TDG_SA(i), w[i]); }
+                    else upd_max<true>(TDG_GA(i), w[i]);
                 }
                 break;
             default: break;
         }
+#undef TDG_HOT
+#undef TDG_SA
+#undef TDG_GA
     }
 }
 
-template <int NT, int NV>
+template <int NT, int NC>
 __global__ void __launch_bounds__(kThreads, TDG_MINB) k_probe_vec(const GroupK G, const Pred P, const VecAgg A,
                                                                   const tdg_col lkey, int64_t kmin, int64_t n_map,
                                                                   const uint32_t* __restrict__ map, int64_t n) {
@@ -675,24 +870,226 @@ __global__ void __launch_bounds__(kThreads, TDG_MINB) k_probe_vec(const GroupK G
     for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
         const int64_t nb = base + (int64_t)gridDim.x * tile;
         prefetch_rows(G.pf, nb, nb + tile < n ? nb + tile : n);
-        vec_tile<NT, NV, true>(G, V, P, A, lkey, kmin, n_map, map, n, base);
+        vec_tile<NT, NC, 0, true>(G, V, P, A, lkey, kmin, n_map, map, n, base);
     }
     smem_flush<0>(G, V);
 }
 
-// The same for a plain group-by with one key and shared-memory accumulators.
-template <int NT, int NV>
-__global__ void __launch_bounds__(kThreads, TDG_MINB) k_group_vec(const GroupK G, const Pred P, const VecAgg A,
-                                                                  int64_t n) {
+// MODE 1 holds fewer CTAs per SM (the hot cache's shared memory), so it may
+// use more registers.
+constexpr int kVecHotMinBlocks = 3;
+
+template <int NT, int NC, int MODE>
+__global__ void __launch_bounds__(kThreads, MODE == 0 ? TDG_MINB : kVecHotMinBlocks)
+k_group_vec(const GroupK G, const Pred P, const VecAgg A, int64_t n) {
     extern __shared__ unsigned long long sm[];
-    const SmemView V = smem_setup<0>(G, sm);
+    const SmemView V = smem_setup<MODE>(G, sm);
     const int64_t tile = (int64_t)kThreads * 4;
     for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
         const int64_t nb = base + (int64_t)gridDim.x * tile;
         prefetch_rows(G.pf, nb, nb + tile < n ? nb + tile : n);
-        vec_tile<NT, NV, false>(G, V, P, A, G.key[0], G.kmin[0], G.krange[0], nullptr, n, base);
+        vec_tile<NT, NC, MODE, false>(G, V, P, A, G.key[0], G.kmin[0], G.krange[0], nullptr, n, base);
     }
-    smem_flush<0>(G, V);
+    if (MODE == 0 || V.n_hot) smem_flush<MODE>(G, V);
+}
+
+// ---- MODE 3: partitioned cold rows -----------------------------------------------
+
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        double w = threadIdx.x < (blockDim.x >> 5) ? sh[threadIdx.x] : 0.0;
+        for (int o = 16; o; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
+        if (threadIdx.x == 0) sh[32] = w;
+    }
+    __syncthreads();
+    const double r = sh[32];
+    __syncthreads();
+    return r;
+}
+
+// Exclusive prefix of v[0, m) into out[0, m] (out[m] = total), one CTA.
+__device__ void block_scan_i64(const uint32_t* v, int64_t m, int64_t* out, long long* part) {
+    const int64_t per = (m + blockDim.x - 1) / blockDim.x;
+    const int64_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
+    long long sum = 0;
+    for (int64_t i = b; i < e; i++) sum += v[i];
+    part[threadIdx.x] = sum;
+    __syncthreads();
+    for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+        const long long add = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0;
+        __syncthreads();
+        part[threadIdx.x] += add;
+        __syncthreads();
+    }
+    long long run = threadIdx.x ? part[threadIdx.x - 1] : 0;
+    for (int64_t i = b; i < e; i++) { out[i] = run; run += v[i]; }
+    if (threadIdx.x == blockDim.x - 1) out[m] = part[blockDim.x - 1];
+    __syncthreads();
+}
+
+// Region capacities from the sampled estimates: 1.5x the partition's own
+// estimate plus half the mean (so a partition the sample under-counted still
+// gets room), scaled from the sampled rows to the input, shared by its
+// stripes, plus a margin -- shrunk to the entry buffers when they would not
+// fit.  Bases are the prefix of the capacities; fills and the work counter
+// start at zero.
+__global__ void __launch_bounds__(1024) k_part_plan(const GroupK G, int64_t n, int64_t m_rows) {
+    const PartK& K = G.pk;
+    __shared__ double sh[33];
+    __shared__ long long part[1024];
+    double s = 0;
+    for (int64_t p = threadIdx.x; p < K.P; p += blockDim.x) s += K.est[p];
+    const double mean = block_sum(s, sh) / (double)K.P;
+    const double scale = (double)n / (double)(m_rows > 0 ? m_rows : 1) / (double)K.stripes;
+    double tot = 0;
+    for (int64_t r = threadIdx.x; r < K.R; r += blockDim.x) {
+        double c = (1.5 * K.est[r / K.stripes] + 0.5 * mean) * scale + kPartMargin;
+        if (c > 2.0e9) c = 2.0e9;
+        K.cap[r] = (uint32_t)c;
+        tot += (double)(uint32_t)c;
+    }
+    const double total = block_sum(tot, sh);
+    if (total > (double)K.cap_total) {
+        // R entries of slack: the truncations can never round the sum past the buffers
+        const double room = (double)K.cap_total - (double)K.R;
+        const double f = room > 0 ? room / total : 0.0;
+        for (int64_t r = threadIdx.x; r < K.R; r += blockDim.x) K.cap[r] = (uint32_t)((double)K.cap[r] * f);
+    }
+    __syncthreads();
+    block_scan_i64(K.cap, K.R, K.base, part);
+    for (int64_t r = threadIdx.x; r < K.R; r += blockDim.x) K.fill[r] = 0;
+    if (threadIdx.x == 0) *K.item_next = 0;
+}
+
+// Work items of the partition pass: ceil(entries / kPartItem) per region.
+__global__ void __launch_bounds__(1024) k_part_items(const GroupK G) {
+    const PartK& K = G.pk;
+    __shared__ long long part[1024];
+    // the capacities are no longer needed: reuse them for the item counts
+    // after the fills are clamped
+    for (int64_t r = threadIdx.x; r < K.R; r += blockDim.x) {
+        const uint32_t f = K.fill[r] < K.cap[r] ? K.fill[r] : K.cap[r];
+        K.fill[r] = f;
+        K.cap[r] = (uint32_t)((f + kPartItem - 1) / kPartItem);
+    }
+    __syncthreads();
+    block_scan_i64(K.cap, K.R, K.item_start, part);
+    for (int64_t r = threadIdx.x; r < K.R; r += blockDim.x)
+        for (int64_t i = K.item_start[r]; i < K.item_start[r + 1]; i++) K.item_region[i] = (int32_t)r;
+}
+
+// The partition pass: each work item aggregates up to kPartItem entries of
+// one region in a shared-memory table of the partition's slots, then merges
+// the table into the global records -- with plain read-modify-writes when
+// the item is its partition's only one, with atomics otherwise.  Every
+// thread loads four entries before it aggregates them.
+__global__ void __launch_bounds__(kPartThreads) k_part_agg(const GroupK G, const VecAgg A) {
+    extern __shared__ unsigned long long sm[];
+    __shared__ long long s_item;
+    const PartK& K = G.pk;
+    const int64_t PS = (int64_t)1 << K.shift;
+    uint32_t* cnt = (uint32_t*)sm;
+    unsigned long long* acc = sm + ((PS * 4 + 7) >> 3);
+    const uint32_t scnt = sh_addr(cnt), sacc = sh_addr(acc);
+    const int64_t n_items = K.item_start[K.R];
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (long long)atomicAdd(K.item_next, 1u);
+        __syncthreads();
+        const int64_t item = s_item;
+        if (item >= n_items) break;
+        const int64_t r = K.item_region[item], k = item - K.item_start[r];
+        const int64_t p = r / K.stripes, slot0 = p << K.shift;
+        const int64_t f = K.fill[r];
+        const int64_t e0 = K.base[r] + k * kPartItem;
+        const int64_t e1 = K.base[r] + ((k + 1) * kPartItem < f ? (k + 1) * kPartItem : f);
+        const bool sole = K.stripes == 1 && K.item_start[r + 1] - K.item_start[r] == 1;
+        for (int64_t i = threadIdx.x; i < PS; i += blockDim.x) cnt[i] = 0;
+        for (int a = 0; a < G.na; a++) {
+            if (G.ai[a] < 0) continue;
+            const unsigned long long init = acc_init_kind(G.kind[a]);
+            for (int64_t i = threadIdx.x; i < PS; i += blockDim.x) acc[(int64_t)G.ai[a] * PS + i] = init;
+        }
+        __syncthreads();
+        for (int64_t eb = e0; eb < e1; eb += 4 * (int64_t)blockDim.x) {
+            uint32_t ls[4];
+            long long v[2][4];
+            bool in[4];
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+                const int64_t e = eb + u * (int64_t)blockDim.x + threadIdx.x;
+                in[u] = e < e1;
+                ls[u] = in[u] ? (uint32_t)((int64_t)__ldcs(K.e_slot + e) - slot0) : 0u;
+                v[0][u] = in[u] && K.ne > 0 ? (long long)__ldcs(K.e_val[0] + e) : 0;
+                v[1][u] = in[u] && K.ne > 1 ? (long long)__ldcs(K.e_val[1] + e) : 0;
+            }
+#pragma unroll
+            for (int u = 0; u < 4; u++) if (in[u]) sh_add_u32(scnt + 4u * ls[u], 1u);
+            for (int a = 0; a < G.na; a++) {
+                const int kind = G.kind[a];
+                if (kind == K_COUNT) continue;
+                const uint32_t sa = sacc + 8u * (uint32_t)(G.ai[a] * PS);
+                const bool second = A.ve[a] == 1;
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (!in[u]) continue;
+                    long long w = second ? v[1][u] : v[0][u];
+                    const uint32_t t = sa + 8u * ls[u];
+                    switch (kind) {
+                        case K_SUM_F: sh_add_f64(t, __longlong_as_double(w)); break;
+                        case K_SUM_I: sh_add_u64(t, (unsigned long long)w); break;
+                        case K_MIN_I: if (w < sh_ld_s64(t)) sh_min_s64(t, w); break;
+                        case K_MAX_I: if (w > sh_ld_s64(t)) sh_max_s64(t, w); break;
+                        case K_MIN_F: {
+                            const double d = __longlong_as_double(w);
+                            w = f2ord(d);
+                            if (d == d && w < sh_ld_s64(t)) sh_min_s64(t, w);
+                            break;
+                        }
+                        case K_MAX_F: {
+                            const double d = __longlong_as_double(w);
+                            w = f2ord(d);
+                            if (d == d && w > sh_ld_s64(t)) sh_max_s64(t, w);
+                            break;
+                        }
+                        default: break;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        const int64_t n_ls = G.S - slot0 < PS ? G.S - slot0 : PS;
+        for (int64_t i = threadIdx.x; i < n_ls; i += blockDim.x) {
+            const uint32_t c = cnt[i];
+            if (!c) continue;
+            unsigned long long* rec = grec(G, slot0 + i);
+            if (sole) {
+                rec[0] += c;
+                for (int a = 0; a < G.na; a++) {
+                    const int ai = G.ai[a];
+                    if (ai < 0) continue;
+                    const unsigned long long x = acc[(int64_t)ai * PS + i];
+                    unsigned long long& y = rec[1 + ai];
+                    switch (G.kind[a]) {
+                        case K_SUM_I: y += x; break;
+                        case K_SUM_F: y = (unsigned long long)__double_as_longlong(
+                                          __longlong_as_double((long long)y) + __longlong_as_double((long long)x));
+                                      break;
+                        case K_MIN_I: case K_MIN_F: if ((long long)x < (long long)y) y = x; break;
+                        case K_MAX_I: case K_MAX_F: if ((long long)x > (long long)y) y = x; break;
+                        default: break;
+                    }
+                }
+            } else {
+                atomicAdd(rec, (unsigned long long)c);
+                for (int a = 0; a < G.na; a++)
+                    if (G.ai[a] >= 0) merge(rec + 1 + G.ai[a], G.kind[a], acc[(int64_t)G.ai[a] * PS + i]);
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // Full outer join: build rows that no probe row matched enter the group-by
@@ -805,7 +1202,7 @@ __global__ void __launch_bounds__(kThreads) k_emit(const GroupK G, const OutK O,
 
 // Small group-bys (S <= kSmallEmit slots): one CTA counts, scans and emits in
 // slot order in a single launch.
-constexpr int64_t kSmallEmit = 65536;
+constexpr int64_t kSmallEmit = 8192;
 
 __device__ __forceinline__ void emit_one(const GroupK& G, const OutK& O, int64_t s, const unsigned long long* r,
                                          unsigned long long c, int64_t o) {
@@ -889,7 +1286,73 @@ static Layout layout_of(int64_t S, int n_acc, int nk, int method, bool sampled) 
     L.sample_keys = o; o += sampled ? al((size_t)kSampleCap * 8) : 0;
     L.sample_cnt = o; o += sampled ? al((size_t)kSampleCap * 4) : 0;
     L.hot = o; o += sampled ? al((size_t)kHotMax * 8) : 0;
-    L.hot_n = o; o += sampled ? 256 : 0;
+    L.hot_n = o; o += sampled ? al(256 + (size_t)kHotHist * 4) : 0;   // hot_n, threshold, then hot_hist
+    L.total = o;
+    return L;
+}
+
+// ---- MODE 3 planning ----
+// Distinct aggregate input columns (-1 when an input is not 8 bytes wide or
+// there are more than two).
+static int part_values(const tdg_group_desc* d) {
+    const void* seen[2] = {nullptr, nullptr};
+    int ne = 0;
+    for (int a = 0; a < d->n_aggs; a++) {
+        if (d->aggs[a].op == A_COUNT) continue;
+        if (elem_size(d->aggs[a].in.type, d->aggs[a].in.attrs) != 8) return -1;
+        int j = 0;
+        while (j < ne && seen[j] != d->aggs[a].in.data) j++;
+        if (j < ne) continue;
+        if (ne == 2) return -1;
+        seen[ne++] = d->aggs[a].in.data;
+    }
+    return ne;
+}
+
+static bool wants_partition(const tdg_group_desc* d, int method, bool smem, int64_t S, int64_t nrows) {
+    return method == TDG_GROUP_DIRECT && !smem && nrows >= kPartMinRows && d->n_keys == 1 &&
+           is_int_class(d->keys[0].type) && elem_size(d->keys[0].type, d->keys[0].attrs) == 8 &&
+           S < ((int64_t)1 << 32) && part_values(d) >= 0;
+}
+
+static bool wants_sampling(int method, bool smem, int64_t S, int64_t nrows);
+
+static bool group_sampled(const tdg_group_desc* d, int method, bool smem, int64_t S, int64_t nrows) {
+    return wants_sampling(method, smem, S, nrows) || wants_partition(d, method, smem, S, nrows);
+}
+
+struct PartLayout {
+    PartK k;                      // dimensions; pointers are offsets from the section start
+    size_t est, fill, cap, base, item_start, item_region, item_next, e_slot, e_val[2], total;
+};
+
+// The MODE 3 section, placed after the rest of the workspace.  A partition
+// spans the slots whose shared-memory table (32-bit count, 8-byte
+// accumulators) fits kPartSmem; the entry buffers hold one entry per input row.
+static PartLayout part_layout(const tdg_group_desc* d, int64_t S, int n_acc, int64_t nrows) {
+    PartLayout L;
+    memset(&L, 0, sizeof(L));
+    const size_t per = 4 + 8 * (size_t)n_acc;
+    int shift = 0;
+    while (((size_t)2 << shift) * per <= kPartSmem) shift++;
+    L.k.shift = shift;
+    L.k.P = (S + ((int64_t)1 << shift) - 1) >> shift;
+    int st = 1;
+    while (st < kPartMaxStripes && L.k.P * st * 2 <= kPartRegions) st <<= 1;
+    L.k.stripes = st;
+    L.k.R = L.k.P * st;
+    L.k.ne = part_values(d);
+    L.k.cap_total = nrows;
+    size_t o = 0;
+    L.est = o; o += al((size_t)L.k.P * 4);
+    L.fill = o; o += al((size_t)L.k.R * 4);
+    L.cap = o; o += al((size_t)L.k.R * 4);
+    L.base = o; o += al((size_t)L.k.R * 8);
+    L.item_start = o; o += al((size_t)(L.k.R + 1) * 8);
+    L.item_region = o; o += al((size_t)(L.k.R + nrows / kPartItem + 1) * 4);
+    L.item_next = o; o += 256;
+    L.e_slot = o; o += al((size_t)nrows * 4);
+    for (int j = 0; j < L.k.ne; j++) { L.e_val[j] = o; o += al((size_t)nrows * 8); }
     L.total = o;
     return L;
 }
@@ -966,8 +1429,10 @@ static tdg_status plan_group(const tdg_group_desc* d, int64_t nrows_bound, int64
         p->n_slots = next_pow2(bound * 2 > 1024 ? bound * 2 : 1024);
     }
     p->max_groups = p->n_slots;
-    const bool sampled = wants_sampling(p->method, p->smem != 0, p->n_slots, nrows_bound);
+    const bool sampled = group_sampled(d, p->method, p->smem != 0, p->n_slots, nrows_bound);
     p->ws_bytes = layout_of(p->n_slots, n_acc, d->n_keys, p->method, sampled).total;
+    if (wants_partition(d, p->method, p->smem != 0, p->n_slots, nrows_bound))
+        p->ws_bytes += part_layout(d, p->n_slots, n_acc, nrows_bound).total;
     return E_OK;
 }
 
@@ -985,7 +1450,7 @@ static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws
     GroupK G;
     memset(&G, 0, sizeof(G));
     const int n_acc = count_acc(d);
-    const bool sampled = wants_sampling(p->method, p->smem != 0, p->n_slots, nrows_bound);
+    const bool sampled = group_sampled(d, p->method, p->smem != 0, p->n_slots, nrows_bound);
     const Layout L = layout_of(p->n_slots, n_acc, d->n_keys, p->method, sampled);
     char* w = (char*)ws;
     G.nk = d->n_keys;
@@ -1026,8 +1491,23 @@ static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws
         G.sample_cnt = (uint32_t*)(w + L.sample_cnt);
         G.hot = (int64_t*)(w + L.hot);
         G.hot_n = (int32_t*)(w + L.hot_n);
+        G.hot_hist = (uint32_t*)(w + L.hot_n + 256);
         int cap = (int)((kSmemMax - (size_t)kHotMap * 6 - 8) / (4 + 8 * (size_t)n_acc));
         G.hot_cap = cap < kHotMax ? cap : kHotMax;
+    }
+    if (wants_partition(d, p->method, p->smem != 0, p->n_slots, nrows_bound)) {
+        const PartLayout PL = part_layout(d, p->n_slots, n_acc, nrows_bound);
+        char* b = w + L.total;
+        G.pk = PL.k;
+        G.pk.est = (uint32_t*)(b + PL.est);
+        G.pk.fill = (uint32_t*)(b + PL.fill);
+        G.pk.cap = (uint32_t*)(b + PL.cap);
+        G.pk.base = (int64_t*)(b + PL.base);
+        G.pk.item_start = (int64_t*)(b + PL.item_start);
+        G.pk.item_region = (int32_t*)(b + PL.item_region);
+        G.pk.item_next = (uint32_t*)(b + PL.item_next);
+        G.pk.e_slot = (uint32_t*)(b + PL.e_slot);
+        for (int j = 0; j < PL.k.ne; j++) G.pk.e_val[j] = (unsigned long long*)(b + PL.e_val[j]);
     }
     return G;
 }
@@ -1039,8 +1519,9 @@ static tdg_status prepare(const GroupK& G, cudaStream_t s) {
     if (G.hot_cap) {
         cudaMemsetAsync(G.sample_keys, 0xFF, (size_t)kSampleCap * 8, s);
         cudaMemsetAsync(G.sample_cnt, 0, (size_t)kSampleCap * 4, s);
-        cudaMemsetAsync(G.hot_n, 0, 4, s);
+        cudaMemsetAsync(G.hot_n, 0, 256 + (size_t)kHotHist * 4, s);
     }
+    if (G.pk.P) cudaMemsetAsync(G.pk.est, 0, (size_t)G.pk.P * 4, s);
     return launch_status();
 }
 
@@ -1112,6 +1593,8 @@ static tdg_status launch_sample(const GroupK& G, const Pred& P, const tdg_expr& 
     const int g = grid_for((const void*)k_sample<PK, MODE, JOIN>, kThreads, 0, m_rows);
     (note_launch(), k_sample<PK, MODE, JOIN><<<g, kThreads, 0, s>>>(G, P, prog, J, n, step, m_rows));
     const int g2 = grid_for((const void*)k_select_hot, kThreads, 0, kSampleCap);
+    (note_launch(), k_hot_hist<<<g2, kThreads, 0, s>>>(G));
+    (note_launch(), k_hot_threshold<<<1, kHotHist, 0, s>>>(G));
     (note_launch(), k_select_hot<<<g2, kThreads, 0, s>>>(G));
     return launch_status();
 }
@@ -1131,52 +1614,82 @@ static void set_prefetch(GroupK& G, const Pred& P, const tdg_expr& prog, int pk,
         if (G.kind[a] != K_COUNT && !G.in[a].side) pf_add(G.pf, G.in[a]);
 }
 
-// Value columns of the vector form: at most one distinct column, 16-byte
-// aligned, shared by every non-COUNT aggregate; false when they need more.
-static bool vec_aggs(const GroupK& G, VecAgg& A, int& nv) {
+// Columns of the vector form: the predicate's terms (the range form, at most
+// two) and the aggregates' inputs, at most two distinct columns between them,
+// each 16-byte aligned.  False when the shape needs more.
+static int vec_col(VecAgg& A, int& nc, const tdg_col& c) {
+    for (int i = 0; i < nc; i++) if (A.vc[i].data == c.data) return i;
+    if (nc == 2 || !aligned16(c.data)) return -1;
+    A.vc[nc] = c;
+    return nc++;
+}
+
+static bool vec_plan(const GroupK& G, int pk, const Pred& P, VecAgg& A, int* nt, int* nc) {
     memset(&A, 0, sizeof(A));
-    nv = 0;
+    *nt = 0;
+    *nc = 0;
+    if (P.sel || !(pk == 0 || (pk == 1 && P.n <= 2))) return false;
+    *nt = pk == 1 ? P.n : 0;
+    for (int t = 0; t < *nt; t++)
+        if ((A.ti[t] = vec_col(A, *nc, P.t[t].col)) < 0) return false;
     for (int a = 0; a < G.na; a++) {
         A.vi[a] = -1;
+        A.ve[a] = -1;
         if (G.kind[a] == K_COUNT) continue;
-        int c = 0;
-        while (c < nv && A.vc[c].data != G.in[a].data) c++;
-        if (c == nv) {
-            if (nv == 1 || !aligned16(G.in[a].data)) return false;
-            A.vc[nv++] = G.in[a];
-        }
-        A.vi[a] = c;
+        if ((A.vi[a] = vec_col(A, *nc, G.in[a])) < 0) return false;
+        int j = 0;
+        while (j < A.ne && A.ec[j] != A.vi[a]) j++;
+        if (j == A.ne) A.ec[A.ne++] = A.vi[a];
+        A.ve[a] = j;
     }
     return true;
 }
 
-// Predicate terms of the vector form: the range form (or none), at most two
-// terms, aligned columns, and no more than two columns loaded besides the key.
-static bool vec_terms(int pk, const Pred& P, int nv, int* nt) {
-    if (P.sel || !(pk == 0 || (pk == 1 && P.n <= 2))) return false;
-    *nt = pk == 1 ? P.n : 0;
-    for (int t = 0; t < *nt; t++) if (!aligned16(P.t[t].col.data)) return false;
-    return *nt + nv <= 2;                       // larger shapes exceed the register budget
-}
-
-// Plain group-by with one 8-byte key and shared-memory accumulators in the
-// vector form; false when the shape does not qualify.
-static bool launch_group_vec(const GroupK& G, const Pred& P, int pk, int64_t n, cudaStream_t s, tdg_status* st) {
+// Plain group-by with one 8-byte key in the vector form (MODE 0: shared-memory
+// accumulators; MODE 1: global records and the hot cache; MODE 3 when its
+// buffers are planned: MODE 1 with the cold rows partitioned); false when the
+// shape does not qualify.
+static bool launch_group_vec(const GroupK& G, const Pred& P, int pk, int mode, int64_t n, cudaStream_t s,
+                             tdg_status* st) {
     if (G.nk != 1 || G.key[0].type == T_F64 || !aligned16(G.key[0].data)) return false;
     VecAgg A;
-    int nv, nt;
-    if (!vec_aggs(G, A, nv) || !vec_terms(pk, P, nv, &nt)) return false;
-    const size_t smem = smem_full_bytes(G.S, G.n_acc);
-#define TDG_GV(NTV, NVV)                                                                                \
-    if (nt == NTV && nv == NVV) {                                                                       \
-        const int g = grid_for((const void*)k_group_vec<NTV, NVV>, kThreads, smem, (n + 3) / 4);       \
-        (note_launch(), k_group_vec<NTV, NVV><<<g, kThreads, smem, s>>>(G, P, A, n));                   \
-        *st = launch_status();                                                                          \
-        return true;                                                                                    \
+    int nt, nc;
+    if (!vec_plan(G, pk, P, A, &nt, &nc)) return false;
+    if (mode == 1 && G.pk.P && G.hot_cap && A.ne <= G.pk.ne) mode = 3;
+    const size_t smem = mode == 0 ? smem_full_bytes(G.S, G.n_acc) : (G.hot_cap ? smem_hot_bytes(G.hot_cap, G.n_acc) : 0);
+    if (mode == 3) {
+        const int64_t m_rows = n < kSampleRows ? n : kSampleRows;
+        (note_launch(), k_part_plan<<<1, 1024, 0, s>>>(G, n, m_rows));
     }
-    TDG_GV(0, 0) TDG_GV(0, 1) TDG_GV(1, 0) TDG_GV(1, 1) TDG_GV(2, 0)
+    bool launched = false;
+#define TDG_GV(NTV, NCV, MV)                                                                            \
+    if (!launched && nt == NTV && nc == NCV && mode == MV) {                                            \
+        const int g = grid_for((const void*)k_group_vec<NTV, NCV, MV>, kThreads, smem, (n + 3) / 4);   \
+        (note_launch(), k_group_vec<NTV, NCV, MV><<<g, kThreads, smem, s>>>(G, P, A, n));               \
+        launched = true;                                                                                \
+    }
+    TDG_GV(0, 0, 0) TDG_GV(0, 1, 0) TDG_GV(0, 2, 0) TDG_GV(1, 1, 0) TDG_GV(1, 2, 0) TDG_GV(2, 1, 0) TDG_GV(2, 2, 0)
+    TDG_GV(0, 0, 1) TDG_GV(0, 1, 1) TDG_GV(0, 2, 1) TDG_GV(1, 1, 1) TDG_GV(1, 2, 1) TDG_GV(2, 1, 1) TDG_GV(2, 2, 1)
+    TDG_GV(0, 0, 3) TDG_GV(0, 1, 3) TDG_GV(0, 2, 3) TDG_GV(1, 1, 3) TDG_GV(1, 2, 3) TDG_GV(2, 1, 3) TDG_GV(2, 2, 3)
 #undef TDG_GV
-    return false;
+    if (!launched) {
+        // k_part_plan ran for nothing: harmless, the fallback kernel does not read its buffers
+        return false;
+    }
+    if (mode == 3) {
+        (note_launch(), k_part_items<<<1, 1024, 0, s>>>(G));
+        const int64_t PS = (int64_t)1 << G.pk.shift;
+        const size_t smb = smem_full_bytes(PS, G.n_acc);
+        if (cudaFuncSetAttribute((const void*)k_part_agg, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smb) !=
+            cudaSuccess) {
+            *st = launch_status();
+            return true;
+        }
+        const int g = grid_for((const void*)k_part_agg, kPartThreads, smb, (int64_t)1 << 40);
+        (note_launch(), k_part_agg<<<g, kPartThreads, smb, s>>>(G, A));
+    }
+    *st = launch_status();
+    return true;
 }
 
 template <bool JOIN>
@@ -1194,7 +1707,7 @@ static tdg_status dispatch(int pk, const GroupK& G0, bool smem, const Pred& P, c
     }
     const bool w8 = pk != 2 && group_w8(G, P, JOIN ? &J : nullptr);
     tm.start(s);
-    if (!JOIN && mode == 0 && w8 && n > 0 && launch_group_vec(G, P, pk, n, s, &st)) { tm.stop(s); return st; }
+    if (!JOIN && mode != 2 && w8 && n > 0 && launch_group_vec(G, P, pk, mode, n, s, &st)) { tm.stop(s); return st; }
 #define TDG_CASE(PKV, MV, W) \
     if (pk == PKV && mode == MV && w8 == W) { st = launch_main<PKV, MV, JOIN, W>(G, P, prog, J, n, s); tm.stop(s); return st; }
     TDG_CASE(0, 0, true) TDG_CASE(0, 1, true) TDG_CASE(0, 2, true)
@@ -1254,19 +1767,19 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     tm.start(s);
     // the vector form, when the shape and the alignment allow it
     VecAgg A;
-    int nv = 0, nt = 0;
+    int nc = 0, nt = 0;
     bool vec = sm && w8 && aligned16(J->lkeys[0].data);
     for (int k = 0; k < G.nk && vec; k++) vec = G.key[k].side == 1;
-    vec = vec && vec_aggs(G, A, nv) && vec_terms(pk, P, nv, &nt);
+    vec = vec && vec_plan(G, pk, P, A, &nt, &nc);
     bool launched = false;
-#define TDG_PV(NTV, NVV)                                                                                  \
-    if (vec && !launched && nt == NTV && nv == NVV) {                                                     \
-        const int g = grid_for((const void*)k_probe_vec<NTV, NVV>, kThreads, smem, (n_left + 3) / 4);    \
-        (note_launch(), k_probe_vec<NTV, NVV><<<g, kThreads, smem, s>>>(G, P, A, J->lkeys[0], J->kmin,    \
+#define TDG_PV(NTV, NCV)                                                                                  \
+    if (vec && !launched && nt == NTV && nc == NCV) {                                                     \
+        const int g = grid_for((const void*)k_probe_vec<NTV, NCV>, kThreads, smem, (n_left + 3) / 4);    \
+        (note_launch(), k_probe_vec<NTV, NCV><<<g, kThreads, smem, s>>>(G, P, A, J->lkeys[0], J->kmin,    \
                                                                          J->n_slots, (const uint32_t*)map, n_left)); \
         launched = true;                                                                                  \
     }
-    TDG_PV(0, 0) TDG_PV(0, 1) TDG_PV(1, 0) TDG_PV(1, 1) TDG_PV(2, 0)
+    TDG_PV(0, 0) TDG_PV(0, 1) TDG_PV(0, 2) TDG_PV(1, 1) TDG_PV(1, 2) TDG_PV(2, 1) TDG_PV(2, 2)
 #undef TDG_PV
 #define TDG_PL(PKV, SMV, PT, W)                                                                         \
     if (!launched && pk == PKV && sm == SMV && narrow == (sizeof(PT) == 2) && w8 == W) {                \

@@ -1,9 +1,9 @@
-"""The plain group-by's vector form (one 8-byte key, shared-memory
-accumulators, every column read with 16-byte loads) and its fallbacks: odd
-row counts (the last pair is half full), negative key ranges, a table view
-starting at an odd row (columns not 16-byte aligned: the general kernel
-runs), no filter, one and two filter terms, COUNT only and F64 / I64
-SUM, MIN and MAX -- each against the oracle."""
+"""The plain group-by's vector form (one 8-byte key, every column read with
+16-byte loads; shared-memory accumulators or the global record array) and
+its fallbacks: odd row counts (the last pair is half full), negative key
+ranges, a table view starting at an odd row (columns not 16-byte aligned:
+the general kernel runs), no filter, one and two filter terms, COUNT only
+and F64 / I64 SUM, MIN and MAX -- each against the oracle."""
 import numpy as np
 import pytest
 
@@ -69,9 +69,13 @@ CASES = [
 
 
 @pytest.mark.parametrize("preds,aggs", CASES)
-@pytest.mark.parametrize("n,lo", [(400_001, 0), (400_000, -37), (3, 5)])
-def test_vector_group_shapes(gpu, preds, aggs, n, lo):
-    d = _data(n, seed=91 + n % 7, lo=lo)
+@pytest.mark.parametrize("n,lo,span", [(400_001, 0, 64), (400_000, -37, 64), (3, 5, 64),
+                                       (400_001, -50_000, 150_000)])
+def test_vector_group_shapes(gpu, preds, aggs, n, lo, span):
+    """span 64: shared-memory accumulators; span 150000: the global record
+    array (a direct array too large for shared memory, too few rows to sample
+    hot slots)."""
+    d = _data(n, seed=91 + n % 7, lo=lo, span=span)
     t = gpu.table(d)
     try:
         _same(_run(gpu, t, preds, aggs), _want(d, preds, aggs))
@@ -101,5 +105,57 @@ def test_wide_key_range_takes_other_kernels(gpu):
         preds, aggs = CASES[0]
         _same(oracle.canonical(_run(gpu, t, preds, aggs), by=["region"]),
               oracle.canonical(_want(d, preds, aggs), by=["region"]))
+    finally:
+        gpu.release(t)
+
+
+AGGS5 = [(OP_COUNT, "qty"), (OP_SUM, "qty"), (OP_MIN, "qty"), (OP_MAX, "qty"), (OP_AVG, "amount")]
+
+
+@pytest.mark.parametrize("preds,aggs", [
+    ([("flag", "ne", 3)], AGGS5),
+    ([], [(OP_COUNT, "qty")]),
+    ([("qty", "gt", 0)], [(OP_SUM, "amount"), (OP_MIN, "amount"), (OP_MAX, "amount")]),
+])
+@pytest.mark.parametrize("n,lo,span", [(1_500_001, -9_000, 16_384), (1_200_000, 0, 1_000_000)])
+def test_partitioned_shapes(gpu, preds, aggs, n, lo, span):
+    """At least 2^20 rows over a direct array too large for shared memory:
+    hot slots in shared memory, every other row an entry of its slot range's
+    partition, then the partition pass (few partitions split into stripes,
+    or many partitions with one owner each)."""
+    d = _data(n, seed=94 + n % 5, lo=lo, span=span)
+    t = gpu.table(d)
+    try:
+        _same(_run(gpu, t, preds, aggs), _want(d, preds, aggs))
+    finally:
+        gpu.release(t)
+
+
+def test_partitioned_zipf_keys(gpu):
+    """Skewed keys: the hot cache takes the head, the partitions the tail."""
+    from teide_b200 import workloads
+    c = workloads.config2(n=2_000_000, seed=95, nkeys=1 << 16)
+    d = {"region": c["key"], "qty": c["v1"], "amount": c["v2"], "flag": (c["v1"] & 3)}
+    t = gpu.table(d)
+    try:
+        preds = [("flag", "ne", 1)]
+        _same(_run(gpu, t, preds, AGGS5), _want(d, preds, AGGS5))
+    finally:
+        gpu.release(t)
+
+
+def test_partition_overflow_falls_back_to_atomics(gpu):
+    """The sample reads every 4th row; keys that differ between sampled and
+    unsampled rows make one key range's estimate far too small, so most of
+    its rows overflow their regions and update the records directly."""
+    n = 1_200_000
+    r = np.random.default_rng(96)
+    i = np.arange(n)
+    key = np.where(i % 4 == 0, r.integers(0, 8192, n), r.integers(8192, 40_000, n)).astype(np.int64)
+    d = {"flag": r.integers(0, 4, n, dtype=np.int64), "region": key,
+         "amount": r.random(n) * 1000.0, "qty": r.integers(-500, 500, n, dtype=np.int64)}
+    t = gpu.table(d)
+    try:
+        _same(_run(gpu, t, [], AGGS5), _want(d, [], AGGS5))
     finally:
         gpu.release(t)
