@@ -643,12 +643,15 @@ __global__ void __launch_bounds__(kThreads, TDG_MINB) k_payload_probe(const Grou
 //   k_group_vec<0>     a one-key group-by with shared-memory accumulators;
 //   k_group_vec<1>     a one-key group-by over the global record array, with
 //                      the CTA's cache of sampled hot slots in shared memory.
+// Column choices are bit masks (bit k set: the second column), so kernels
+// never index a parameter array at run time -- that would copy the struct
+// to local memory.
 struct VecAgg {
-    int32_t vi[TDG_MAX_AGGS];    // aggregate -> loaded column (-1: COUNT)
-    int32_t ti[kMaxTerms];       // predicate term -> loaded column
-    int32_t ne;                  // MODE 3 values per entry
-    int32_t ec[2];               // MODE 3 entry value j -> loaded column
-    int32_t ve[TDG_MAX_AGGS];    // aggregate -> entry value (-1: COUNT)
+    uint32_t vsel;               // bit a: aggregate a reads the second loaded column
+    uint32_t tsel;               // bit t: predicate term t reads the second loaded column
+    uint32_t esel;               // bit j: MODE 3 entry value j is the second loaded column
+    uint32_t asel;               // bit a: aggregate a reads MODE 3 entry value 1
+    int32_t ne, pad;             // MODE 3 values per entry
     tdg_col vc[2];               // the distinct columns read besides the key
 };
 
@@ -688,9 +691,15 @@ __device__ __forceinline__ long long sh_ld_s64(uint32_t a) {
     return v;
 }
 
+// Column c of row i.  The two candidates pass through an empty asm first, so
+// the choice is a register select: folded into an indexed load it would put
+// the whole column array in local memory.
 template <int NC>
 __device__ __forceinline__ long long vec_pick(const long long (&cv)[NC > 0 ? NC : 1][4], int c, int i) {
-    return (NC > 1 && c == 1) ? cv[NC > 1 ? 1 : 0][i] : cv[0][i];
+    if (NC < 2) return cv[0][i];
+    long long a = cv[0][i], b = cv[NC > 1 ? 1 : 0][i];
+    asm("" : "+l"(a), "+l"(b));
+    return c == 1 ? b : a;
 }
 
 // One tile of 4 * kThreads rows.  MAP: the key indexes the join's payload
@@ -721,7 +730,7 @@ __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, con
 #pragma unroll
         for (int t = 0; t < NT; t++) {
             const Term& T = P.t[t];
-            const long long x = vec_pick<NC>(cv, A.ti[t], i);
+            const long long x = vec_pick<NC>(cv, (A.tsel >> t) & 1, i);
             bool b;
             if (T.f) {
                 const double v = __longlong_as_double(x);
@@ -782,7 +791,7 @@ __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, con
                 K.e_slot[e] = (uint32_t)slot[i];
 #pragma unroll
                 for (int j = 0; j < 2; j++)
-                    if (j < K.ne) K.e_val[j][e] = (unsigned long long)vec_pick<NC>(cv, A.ec[j], i);
+                    if (j < K.ne) K.e_val[j][e] = (unsigned long long)vec_pick<NC>(cv, (A.esel >> j) & 1, i);
                 ok[i] = false;              // the partition pass aggregates it
             }
         }
@@ -802,7 +811,7 @@ __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, con
         if (kind == K_COUNT || NC == 0) continue;
         const int ai = G.ai[a];
         const uint32_t sacc = sh_addr(V.acc + (int64_t)ai * V.cap);
-        const int c = A.vi[a];
+        const int c = (A.vsel >> a) & 1;
         long long w[4];
         bool on[4];
         const bool fl = kind == K_MIN_F || kind == K_MAX_F;
@@ -1031,11 +1040,13 @@ __global__ void __launch_bounds__(kPartThreads) k_part_agg(const GroupK G, const
                 const int kind = G.kind[a];
                 if (kind == K_COUNT) continue;
                 const uint32_t sa = sacc + 8u * (uint32_t)(G.ai[a] * PS);
-                const bool second = A.ve[a] == 1;
+                const bool second = (A.asel >> a) & 1;
 #pragma unroll
                 for (int u = 0; u < 4; u++) {
                     if (!in[u]) continue;
-                    long long w = second ? v[1][u] : v[0][u];
+                    long long w0 = v[0][u], w1 = v[1][u];
+                    asm("" : "+l"(w0), "+l"(w1));     // a register select, not an indexed load
+                    long long w = second ? w1 : w0;
                     const uint32_t t = sa + 8u * ls[u];
                     switch (kind) {
                         case K_SUM_F: sh_add_f64(t, __longlong_as_double(w)); break;
@@ -1630,17 +1641,25 @@ static bool vec_plan(const GroupK& G, int pk, const Pred& P, VecAgg& A, int* nt,
     *nc = 0;
     if (P.sel || !(pk == 0 || (pk == 1 && P.n <= 2))) return false;
     *nt = pk == 1 ? P.n : 0;
-    for (int t = 0; t < *nt; t++)
-        if ((A.ti[t] = vec_col(A, *nc, P.t[t].col)) < 0) return false;
+    for (int t = 0; t < *nt; t++) {
+        const int c = vec_col(A, *nc, P.t[t].col);
+        if (c < 0) return false;
+        A.tsel |= (uint32_t)c << t;
+    }
+    int ec[2] = {-1, -1};
     for (int a = 0; a < G.na; a++) {
-        A.vi[a] = -1;
-        A.ve[a] = -1;
         if (G.kind[a] == K_COUNT) continue;
-        if ((A.vi[a] = vec_col(A, *nc, G.in[a])) < 0) return false;
+        const int c = vec_col(A, *nc, G.in[a]);
+        if (c < 0) return false;
+        A.vsel |= (uint32_t)c << a;
         int j = 0;
-        while (j < A.ne && A.ec[j] != A.vi[a]) j++;
-        if (j == A.ne) A.ec[A.ne++] = A.vi[a];
-        A.ve[a] = j;
+        while (j < A.ne && ec[j] != c) j++;
+        if (j == A.ne) {
+            ec[j] = c;
+            A.esel |= (uint32_t)c << j;
+            A.ne++;
+        }
+        A.asel |= (uint32_t)j << a;
     }
     return true;
 }
