@@ -70,6 +70,7 @@ constexpr int64_t kPartItem = 16384;          // entries per aggregation work it
 constexpr int kPartRegions = 1024;            // partitions below this are split into stripes
 constexpr int kPartMaxStripes = 64;
 constexpr uint32_t kPartMargin = 32;          // entries every region holds beyond its estimate
+constexpr int64_t kPartDense = 4;             // entries per slot below which an item skips the table
 
 enum : int32_t { K_COUNT = 0, K_SUM_I, K_SUM_F, K_MIN_I, K_MAX_I, K_MIN_F, K_MAX_F };
 
@@ -104,6 +105,7 @@ struct GroupK {
     int32_t op[TDG_MAX_AGGS];
     int32_t kind[TDG_MAX_AGGS];   // K_*
     int32_t ai[TDG_MAX_AGGS];     // accumulator index, -1 for COUNT
+    int32_t akind[TDG_MAX_AGGS];  // K_* of each accumulator
     tdg_col in[TDG_MAX_AGGS];
     int64_t S;
     unsigned long long* rec;      // S * W words
@@ -1004,17 +1006,46 @@ __global__ void __launch_bounds__(kPartThreads) k_part_agg(const GroupK G, const
     unsigned long long* acc = sm + ((PS * 4 + 7) >> 3);
     const uint32_t scnt = sh_addr(cnt), sacc = sh_addr(acc);
     const int64_t n_items = K.item_start[K.R];
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(K.item_next, 1u);
+    __syncthreads();
     for (;;) {
-        if (threadIdx.x == 0) s_item = (long long)atomicAdd(K.item_next, 1u);
-        __syncthreads();
         const int64_t item = s_item;
         if (item >= n_items) break;
+        // the next item is claimed now; its index is published after this one
+        long long next = 0;
+        if (threadIdx.x == 0) next = (long long)atomicAdd(K.item_next, 1u);
         const int64_t r = K.item_region[item], k = item - K.item_start[r];
         const int64_t p = r / K.stripes, slot0 = p << K.shift;
         const int64_t f = K.fill[r];
         const int64_t e0 = K.base[r] + k * kPartItem;
         const int64_t e1 = K.base[r] + ((k + 1) * kPartItem < f ? (k + 1) * kPartItem : f);
         const bool sole = K.stripes == 1 && K.item_start[r + 1] - K.item_start[r] == 1;
+        if (e1 - e0 < PS * kPartDense) {
+            // sparse: a table would cost more to clear and merge than the
+            // entries themselves; they update the records directly, which
+            // this item's partition keeps in L2 meanwhile
+            for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+                unsigned long long* rec = grec(G, (int64_t)__ldcs(K.e_slot + e));
+                const long long v0 = K.ne > 0 ? (long long)__ldcs(K.e_val[0] + e) : 0;
+                const long long v1 = K.ne > 1 ? (long long)__ldcs(K.e_val[1] + e) : 0;
+                atomicAdd(rec, 1ULL);
+                for (int a = 0; a < G.na; a++) {
+                    const int kind = G.kind[a];
+                    if (kind == K_COUNT) continue;
+                    long long w = ((A.asel >> a) & 1) ? v1 : v0;
+                    if (kind == K_MIN_F || kind == K_MAX_F) {
+                        const double d = __longlong_as_double(w);
+                        if (d != d) continue;
+                        w = f2ord(d);
+                    }
+                    merge(rec + 1 + G.ai[a], kind, (unsigned long long)w);
+                }
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) s_item = next;
+            __syncthreads();
+            continue;
+        }
         for (int64_t i = threadIdx.x; i < PS; i += blockDim.x) cnt[i] = 0;
         for (int a = 0; a < G.na; a++) {
             if (G.ai[a] < 0) continue;
@@ -1077,28 +1108,36 @@ __global__ void __launch_bounds__(kPartThreads) k_part_agg(const GroupK G, const
             if (!c) continue;
             unsigned long long* rec = grec(G, slot0 + i);
             if (sole) {
-                rec[0] += c;
-                for (int a = 0; a < G.na; a++) {
-                    const int ai = G.ai[a];
-                    if (ai < 0) continue;
-                    const unsigned long long x = acc[(int64_t)ai * PS + i];
-                    unsigned long long& y = rec[1 + ai];
-                    switch (G.kind[a]) {
-                        case K_SUM_I: y += x; break;
-                        case K_SUM_F: y = (unsigned long long)__double_as_longlong(
-                                          __longlong_as_double((long long)y) + __longlong_as_double((long long)x));
+                // every word of the record is read before any is combined, so
+                // a record costs one memory round trip
+                unsigned long long y[TDG_MAX_AGGS + 1];
+#pragma unroll
+                for (int w = 0; w <= TDG_MAX_AGGS; w++) if (w <= G.n_acc) y[w] = rec[w];
+                y[0] += c;
+#pragma unroll
+                for (int w = 1; w <= TDG_MAX_AGGS; w++) {
+                    if (w > G.n_acc) break;
+                    const unsigned long long x = acc[(int64_t)(w - 1) * PS + i];
+                    switch (G.akind[w - 1]) {
+                        case K_SUM_I: y[w] += x; break;
+                        case K_SUM_F: y[w] = (unsigned long long)__double_as_longlong(
+                                          __longlong_as_double((long long)y[w]) + __longlong_as_double((long long)x));
                                       break;
-                        case K_MIN_I: case K_MIN_F: if ((long long)x < (long long)y) y = x; break;
-                        case K_MAX_I: case K_MAX_F: if ((long long)x > (long long)y) y = x; break;
+                        case K_MIN_I: case K_MIN_F: if ((long long)x < (long long)y[w]) y[w] = x; break;
+                        case K_MAX_I: case K_MAX_F: if ((long long)x > (long long)y[w]) y[w] = x; break;
                         default: break;
                     }
                 }
+#pragma unroll
+                for (int w = 0; w <= TDG_MAX_AGGS; w++) if (w <= G.n_acc) rec[w] = y[w];
             } else {
                 atomicAdd(rec, (unsigned long long)c);
                 for (int a = 0; a < G.na; a++)
                     if (G.ai[a] >= 0) merge(rec + 1 + G.ai[a], G.kind[a], acc[(int64_t)G.ai[a] * PS + i]);
             }
         }
+        __syncthreads();
+        if (threadIdx.x == 0) s_item = next;
         __syncthreads();
     }
 }
@@ -1488,7 +1527,10 @@ static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws
         G.in[a] = d->aggs[a].in;
         G.kind[a] = kind_of(d->aggs[a]);
         G.ai[a] = G.op[a] == A_COUNT ? -1 : ai++;
-        if (G.ai[a] >= 0) G.finit[1 + G.ai[a]] = acc_init_kind(G.kind[a]);
+        if (G.ai[a] >= 0) {
+            G.finit[1 + G.ai[a]] = acc_init_kind(G.kind[a]);
+            G.akind[G.ai[a]] = G.kind[a];
+        }
     }
     if (p->method == TDG_GROUP_HASH) {
         G.ht.state = (uint32_t*)(w + L.state);

@@ -117,12 +117,14 @@ AGGS5 = [(OP_COUNT, "qty"), (OP_SUM, "qty"), (OP_MIN, "qty"), (OP_MAX, "qty"), (
     ([], [(OP_COUNT, "qty")]),
     ([("qty", "gt", 0)], [(OP_SUM, "amount"), (OP_MIN, "amount"), (OP_MAX, "amount")]),
 ])
-@pytest.mark.parametrize("n,lo,span", [(1_500_001, -9_000, 16_384), (1_200_000, 0, 1_000_000)])
+@pytest.mark.parametrize("n,lo,span", [(1_500_001, -9_000, 16_384), (1_200_000, 0, 1_000_000),
+                                       (2_000_001, 100, 4_096)])
 def test_partitioned_shapes(gpu, preds, aggs, n, lo, span):
     """At least 2^20 rows over a direct array too large for shared memory:
     hot slots in shared memory, every other row an entry of its slot range's
     partition, then the partition pass (few partitions split into stripes,
-    or many partitions with one owner each)."""
+    or many partitions with one owner each; sparse partitions update the
+    records directly, dense ones -- span 4096 -- through a shared table)."""
     d = _data(n, seed=94 + n % 5, lo=lo, span=span)
     t = gpu.table(d)
     try:
