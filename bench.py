@@ -649,8 +649,8 @@ def main():
     hbm, peak_kind = peaks()
     mean_main = sum(main_ms) / len(main_ms) if main_ms else 0.0
     achieved = main_bytes / (mean_main / 1e3) / 1e9 if mean_main > 0 else None
-    prof = {"join_group": "k_probe_vec_join_group.md", "group_radix": "k_group_group_radix.md",
-            "readme_group": "k_group_readme_group.md"}[args.workload]
+    prof = {"join_group": "k_probe_vec_join_group.md", "group_radix": "k_group_vec_part_agg_group_radix.md",
+            "readme_group": "k_group_vec_readme_group.md"}[args.workload]
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,

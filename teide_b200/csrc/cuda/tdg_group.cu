@@ -1024,21 +1024,34 @@ __global__ void __launch_bounds__(kPartThreads) k_part_agg(const GroupK G, const
             // sparse: a table would cost more to clear and merge than the
             // entries themselves; they update the records directly, which
             // this item's partition keeps in L2 meanwhile
-            for (int64_t e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
-                unsigned long long* rec = grec(G, (int64_t)__ldcs(K.e_slot + e));
-                const long long v0 = K.ne > 0 ? (long long)__ldcs(K.e_val[0] + e) : 0;
-                const long long v1 = K.ne > 1 ? (long long)__ldcs(K.e_val[1] + e) : 0;
-                atomicAdd(rec, 1ULL);
-                for (int a = 0; a < G.na; a++) {
-                    const int kind = G.kind[a];
-                    if (kind == K_COUNT) continue;
-                    long long w = ((A.asel >> a) & 1) ? v1 : v0;
-                    if (kind == K_MIN_F || kind == K_MAX_F) {
-                        const double d = __longlong_as_double(w);
-                        if (d != d) continue;
-                        w = f2ord(d);
+            for (int64_t eb = e0; eb < e1; eb += 4 * (int64_t)blockDim.x) {
+                int64_t sl[4];
+                long long v0[4], v1[4];
+#pragma unroll
+                for (int u = 0; u < 4; u++) {           // four entries' loads in flight together
+                    const int64_t e = eb + u * (int64_t)blockDim.x + threadIdx.x;
+                    sl[u] = e < e1 ? (int64_t)__ldcs(K.e_slot + e) : -1;
+                    v0[u] = e < e1 && K.ne > 0 ? (long long)__ldcs(K.e_val[0] + e) : 0;
+                    v1[u] = e < e1 && K.ne > 1 ? (long long)__ldcs(K.e_val[1] + e) : 0;
+                }
+#pragma unroll
+                for (int u = 0; u < 4; u++) {
+                    if (sl[u] < 0) continue;
+                    unsigned long long* rec = grec(G, sl[u]);
+                    atomicAdd(rec, 1ULL);
+                    for (int a = 0; a < G.na; a++) {
+                        const int kind = G.kind[a];
+                        if (kind == K_COUNT) continue;
+                        long long w0 = v0[u], w1 = v1[u];
+                        asm("" : "+l"(w0), "+l"(w1));     // a register select, not an indexed load
+                        long long w = ((A.asel >> a) & 1) ? w1 : w0;
+                        if (kind == K_MIN_F || kind == K_MAX_F) {
+                            const double d = __longlong_as_double(w);
+                            if (d != d) continue;
+                            w = f2ord(d);
+                        }
+                        merge(rec + 1 + G.ai[a], kind, (unsigned long long)w);
                     }
-                    merge(rec + 1 + G.ai[a], kind, (unsigned long long)w);
                 }
             }
             __syncthreads();
