@@ -55,7 +55,7 @@ constexpr int kEmitChunk = kThreads * 32;
 constexpr size_t kSmemMax = 48 * 1024;
 constexpr int64_t kDirectMaxSlots = (int64_t)1 << 26;
 constexpr int kHotMap = 2048;                 // shared hot-slot map entries (power of 2)
-constexpr int kHotMapBits = 11;
+constexpr int kHotBuckets = kHotMap / 4;       // the map is probed four entries (16 bytes) at a time
 constexpr int kHotMax = 1024;                 // at most this many hot slots
 constexpr int64_t kSampleRows = (int64_t)1 << 18;
 constexpr int64_t kSampleCap = (int64_t)1 << 19;
@@ -279,13 +279,32 @@ __host__ __device__ inline size_t smem_hot_bytes(int hot_cap, int n_acc) {
            (size_t)hot_cap * 8 * n_acc;
 }
 
+// Bucket of a hot slot: the MurmurHash3 32-bit finalizer, so structured key
+// sets (strided or multiplicative ones) spread evenly -- a warp waits for its
+// longest probe, so clustering costs far more than its average suggests.
+__host__ __device__ __forceinline__ uint32_t hot_bucket(int64_t slot) {
+    uint32_t x = (uint32_t)slot;
+    x ^= x >> 16;
+    x *= 0x85ebca6bu;
+    x ^= x >> 13;
+    x *= 0xc2b2ae35u;
+    x ^= x >> 16;
+    return x & (kHotBuckets - 1);
+}
+
+// Linear probing over the map in bucket order, a key inserted from the start
+// of its bucket: one 16-byte load answers a lookup unless the bucket is full.
 __device__ __forceinline__ int hot_find(const SmemView& V, int64_t slot) {
-    uint32_t h = ((uint32_t)slot * 2654435761u) >> (32 - kHotMapBits);
-    for (int p = 0; p < kHotMap; p++) {
-        const int32_t k = V.map_key[h];
-        if (k == (int32_t)slot) return V.map_idx[h];
-        if (k == -1) return -1;
-        h = (h + 1) & (kHotMap - 1);
+    const int32_t key = (int32_t)slot;
+    uint32_t b = hot_bucket(slot);
+    for (int t = 0; t < kHotBuckets; t++) {
+        const int4 k = *reinterpret_cast<const int4*>(V.map_key + 4 * b);
+        if (k.x == key) return V.map_idx[4 * b];
+        if (k.y == key) return V.map_idx[4 * b + 1];
+        if (k.z == key) return V.map_idx[4 * b + 2];
+        if (k.w == key) return V.map_idx[4 * b + 3];
+        if ((k.x == -1) | (k.y == -1) | (k.z == -1) | (k.w == -1)) return -1;
+        b = (b + 1) & (kHotBuckets - 1);
     }
     return -1;
 }
@@ -316,7 +335,7 @@ __device__ SmemView smem_setup(const GroupK& G, unsigned long long* sm) {
         __syncthreads();
         for (int h = threadIdx.x; h < V.n_hot; h += blockDim.x) {
             const int32_t slot = (int32_t)G.hot[h];
-            uint32_t p = ((uint32_t)slot * 2654435761u) >> (32 - kHotMapBits);
+            uint32_t p = 4 * hot_bucket(slot);
             for (int t = 0; t < kHotMap; t++) {
                 if (atomicCAS(&V.map_key[p], -1, slot) == -1) { V.map_idx[p] = (int16_t)h; break; }
                 p = (p + 1) & (kHotMap - 1);
