@@ -348,14 +348,16 @@ def serve_main(args, td, L, rank, world, local, barrier, max_over_ranks):
     serve.build(td, reqs, tg, tb, tp)
     alg = sum(24 * r.n + (16 * 10_000_000 if r.kind == "join" else 0) for r in reqs)
     warm = reqs[:min(len(reqs), 32)]
-    out = {}
+    out, launches = {}, {}
     clk = Clocks(local).__enter__()
     tc0 = time.monotonic()
     for name, slots in (("served", args.slots), ("one_at_a_time", 1)):
         with serve.Server(td, slots=slots) as srv:
             serve.run_closed(srv, warm)                      # warm-up: caches, pinned result blocks
             barrier()
+            l0 = L.tdg_launch_count()
             lat, makespan, _ = serve.run_open_loop(srv, reqs)
+            launches[name] = int(L.tdg_launch_count() - l0)
             closed = serve.run_closed(srv, reqs)
             st = srv.stats()
         out[name] = {"qps": len(reqs) / makespan, "p50_ms": float(np.percentile(lat, 50) * 1e3),
@@ -396,7 +398,7 @@ def serve_main(args, td, L, rank, world, local, barrier, max_over_ranks):
                      "traffic": None, "kernel": "whole served pipeline (closed loop)", "peak_source": peak_kind},
         "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": None,
                 "note": "tables are resident by design; results are host td_t tables"},
-        "gpu_launches": None,
+        "gpu_launches": launches.get("served"),
         "clocks": clk.summary(tc0, tc1),
         "cpu_baseline": cpu,
     }

@@ -106,7 +106,7 @@ td_t*        td_server_wait(td_server_t* s, int64_t ticket, td_server_timing_t* 
 void         td_server_stats(td_server_t* s, td_server_stats_t* out);
 void         td_server_free(td_server_t* s);
 /* Device bytes a query may need beyond resident columns: uploads of columns
- * that are not resident plus a per-row scratch bound (64 bytes per row of the
+ * that are not resident plus a per-row scratch bound (128 bytes per row of the
  * largest input table, 16 per row of the others). */
 size_t       td_server_estimate(td_graph_t* g, td_op_t* root);
 

@@ -228,8 +228,10 @@ size_t td_server_estimate(td_graph_t* g, td_op_t* root) {
         td_op_ext_t* x = g->ext_nodes[i];
         if (x && x->base.opcode == OP_CONST) est_table(x->literal, seen, &n_seen, &upload, &rows_max, &rows_sum);
     }
-    /* columns not resident are uploaded; scratch (group records, join map,
-     * selections, compacted copies) is bounded by 64 bytes per row of the
-     * largest input and 16 per row of the others */
-    return upload + (size_t)rows_max * 64 + (size_t)(rows_sum - rows_max) * 16 + ((size_t)1 << 20);
+    /* columns not resident are uploaded; scratch (group records -- a direct
+     * array holds at most two slots per row, 80 bytes at five words -- the
+     * partitioned group-by's 20-byte entries, join map, selections, compacted
+     * copies) is bounded by 128 bytes per row of the largest input and 16 per
+     * row of the others */
+    return upload + (size_t)rows_max * 128 + (size_t)(rows_sum - rows_max) * 16 + ((size_t)8 << 20);
 }

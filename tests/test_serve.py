@@ -83,6 +83,6 @@ def test_estimate_counts_uploads(td):
     tbl, gs = _graphs(td, 1)
     g, root = gs[0]
     est = td.lib.td_server_estimate(g.g, root)
-    assert est >= 100 * 16 + 100 * 64                   # both columns uploaded + scratch bound
+    assert est >= 100 * 16 + 100 * 128                  # both columns uploaded + scratch bound
     g.free()
     td.release(tbl)
