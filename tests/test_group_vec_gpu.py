@@ -161,3 +161,23 @@ def test_partition_overflow_falls_back_to_atomics(gpu):
         _same(_run(gpu, t, [], AGGS5), _want(d, [], AGGS5))
     finally:
         gpu.release(t)
+
+
+def test_partition_long_runs(gpu):
+    """About 2000 warm keys of ~400 rows each, more than the hot cache holds,
+    over a sparse 1M-key range: the warm keys left out of the cache put long
+    runs of one slot in otherwise sparse partitions, which then update the
+    records directly instead of sorting their entries."""
+    r = np.random.default_rng(97)
+    n_warm, n_flat = 800_000, 400_000
+    warm = r.choice(1_000_000, 2000, replace=False)
+    key = np.concatenate([warm[r.integers(0, 2000, n_warm)], r.integers(0, 1_000_000, n_flat)]).astype(np.int64)
+    r.shuffle(key)
+    n = len(key)
+    d = {"flag": r.integers(0, 4, n, dtype=np.int64), "region": key,
+         "amount": r.standard_normal(n), "qty": r.integers(-10**12, 10**12, n, dtype=np.int64)}
+    t = gpu.table(d)
+    try:
+        _same(_run(gpu, t, [("flag", "ne", 3)], AGGS5), _want(d, [("flag", "ne", 3)], AGGS5))
+    finally:
+        gpu.release(t)
