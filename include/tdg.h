@@ -254,6 +254,33 @@ tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_plan* jplan
                               const tdg_group_desc* g, const tdg_group_plan* gplan, void* gws,
                               const tdg_group_out* out, void* stream);
 
+/* ---- sort ------------------------------------------------------------------------
+ * tdg_sort_perm: the stable permutation that orders n rows by keys[0..n_keys)
+ * (keys[0] most significant).  Replaces exec_sort (exec.c:3370-3862) for
+ * Teide's radix key types: I64, TIMESTAMP, I32, DATE, TIME, F64 and SYM.
+ * Each key is encoded as radix_encode_fn does (exec.c:2739-2840): DESC
+ * complements the code (equal keys keep their row order), F64 follows IEEE
+ * order with -0.0 before +0.0 and NaN first or last by nulls_first, and SYM
+ * sorts by sym_rank[id], a device array holding the rank of each intern id's
+ * string (build_enum_rank, exec.c:2876-2975).  perm receives n int64 row
+ * indices; ws is tdg_sort_ws_bytes(n) device bytes.  The stream is
+ * synchronized once per key (the key's range sets how many digits to sort).
+ * Other key types return TD_ERR_NYI.
+ * tdg_gather: out[i] = in[perm[i]] for i < n_out, for any element width. */
+#define TDG_MAX_SORT_KEYS 16
+
+typedef struct tdg_sort_key {
+    tdg_col         col;
+    const uint32_t* sym_rank;     /* SYM keys: rank by string of every intern id; NULL otherwise */
+    uint8_t         desc;
+    uint8_t         nulls_first;
+    uint8_t         pad[6];
+} tdg_sort_key;
+
+size_t     tdg_sort_ws_bytes(int64_t n);
+tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, int64_t n, void* ws, int64_t* perm, void* stream);
+tdg_status tdg_gather(const tdg_col* in, const int64_t* perm, int64_t n_out, void* out, void* stream);
+
 /* ---- batched group-by ------------------------------------------------------------
  * Many independent group-bys of one shape -- one integer key column with a
  * known range, aggregates over one value column -- run as ONE persistent

@@ -26,7 +26,11 @@ Semantics restated here, with the lines they follow:
   * join: every (left, right) pair with equal keys (join_keys_eq,
     exec.c:7754-7768); output = all left columns then right non-key columns
     (exec.c:8635-8655); LEFT keeps unmatched left rows, FULL also unmatched
-    right rows, with the missing side zero-filled (gather_fn, exec.c:1910-1939).
+    right rows, with the missing side zero-filled (gather_fn, exec.c:1910-1939);
+  * sort: every key encoded as an order-preserving u64 (radix_encode_fn,
+    exec.c:2739-2840) and the rows ordered stably by the keys, the first key
+    most significant (radix_sort_run, exec.c:2647-2737 keeps equal keys in row
+    order); SYM keys order by their strings (build_enum_rank, exec.c:2876-2975).
 """
 from __future__ import annotations
 
@@ -218,3 +222,42 @@ def canonical(d: dict, by=None) -> dict:
         keys.append(v.view(np.int64) if v.dtype == np.float64 else v)
     order = np.lexsort(keys[::-1])
     return {k: np.asarray(v)[order] for k, v in d.items()}
+
+
+def sort_code(values, desc=False, nulls_first=None, kind=None):
+    """The u64 code radix_encode_fn (exec.c:2739-2840) gives each value:
+    integers flip the sign bit (I32 / DATE / TIME at 32 bits), F64 maps to
+    IEEE order (-0.0 before +0.0) with NaN smallest or largest by nulls_first
+    (default: DESC), strings (SYM) to the rank of their bytes among the
+    distinct strings, and DESC complements the code."""
+    nf = desc if nulls_first is None else nulls_first
+    v = np.asarray(values)
+    if kind == "sym" or v.dtype.kind in ("O", "U", "S"):
+        b = [x.encode() if isinstance(x, str) else bytes(x) for x in v]
+        uniq = sorted(set(b))
+        rank = {x: i for i, x in enumerate(uniq)}
+        e = np.array([rank[x] for x in b], dtype=np.uint64)
+    elif v.dtype == np.float64:
+        bits = v.view(np.uint64)
+        mask = (np.uint64(0) - (bits >> np.uint64(63))) | np.uint64(1 << 63)
+        e = bits ^ mask
+        nan_e = np.uint64(0) if (bool(nf) ^ bool(desc)) else np.uint64(0xFFFFFFFFFFFFFFFF)
+        e = np.where(np.isnan(v), (~nan_e) if desc else nan_e, e).astype(np.uint64)
+        return e if not desc else np.where(np.isnan(v), e, ~e)
+    elif v.dtype.itemsize == 4:
+        e = (v.astype(np.int32).view(np.uint32) ^ np.uint32(1 << 31)).astype(np.uint64)
+    else:
+        e = v.astype(np.int64).view(np.uint64) ^ np.uint64(1 << 63)
+    return ~e if desc else e
+
+
+def sort(cols: dict, keys, limit=None) -> dict:
+    """Rows of `cols` ordered by keys [(name, desc, nulls_first)] (stable,
+    first key most significant), cut to the first `limit` rows when given.
+    A SYM key column is passed as its strings."""
+    n = len(next(iter(cols.values()))) if cols else 0
+    codes = [sort_code(cols[name], desc, nf) for name, desc, nf in keys]
+    order = np.lexsort(codes[::-1]) if codes else np.arange(n)
+    if limit is not None:
+        order = order[:limit]
+    return {k: np.asarray(v)[order] for k, v in cols.items()}

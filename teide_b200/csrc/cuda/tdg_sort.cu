@@ -1,0 +1,303 @@
+// Sort: the permutation that orders a table's rows by up to 16 keys, and the
+// gather that applies it to a column.
+//
+// Replaces exec_sort (Teide src/ops/exec.c:3370-3862) for its radix-sortable
+// key types.  Teide encodes every key as an order-preserving u64
+// (radix_encode_fn, exec.c:2739-2840) and sorts the encoded keys with an
+// 8-pass LSD radix sort carrying row indices (radix_sort_run, exec.c:2647-
+// 2737); several keys are bit-packed into one composite when their ranges
+// fit 64 bits.  Here each key is encoded the same way, the keys are applied
+// from the last to the first with a stable LSD radix sort (8-bit digits), and
+// the result -- stable, so equal keys keep their row order -- is the order
+// Teide's radix path produces.  Only the digits that differ are sorted: the
+// key range (max - min of the encoded keys) sets the number of passes.
+//
+// One pass over n keys: a per-tile digit histogram, a prefix over
+// (digit, tile), and a stable scatter in which every tile ranks its rows 256
+// at a time with warp match masks, so rows of equal digit keep their order.
+#include "tdg_common.cuh"
+#include <string.h>
+
+namespace tdg {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortRounds = 16;                           // 256-row rounds per tile
+constexpr int64_t kSortTile = (int64_t)kSortThreads * kSortRounds;
+constexpr int kSortWarps = kSortThreads / 32;
+
+// The order-preserving key of one row (radix_encode_fn, exec.c:2739-2800):
+// integers flip the sign bit, F64 flips every bit of negatives and the sign
+// of the rest (IEEE order, -0.0 before +0.0), NaN is the smallest or largest
+// key by nulls_first, SYM reads the rank of its string, DESC complements.
+__device__ __forceinline__ uint64_t sort_encode(const tdg_sort_key& K, int64_t r) {
+    const tdg_col& c = K.col;
+    uint64_t e;
+    switch (c.type) {
+        case T_I64: case T_TIMESTAMP:
+            e = (uint64_t)((const long long*)c.data)[r] ^ (1ULL << 63);
+            break;
+        case T_I32: case T_DATE: case T_TIME:
+            e = (uint64_t)((uint32_t)((const int*)c.data)[r] ^ (1u << 31));
+            break;
+        case T_F64: {
+            const uint64_t b = (uint64_t)__double_as_longlong(((const double*)c.data)[r]);
+            if ((b & 0x7FF0000000000000ULL) == 0x7FF0000000000000ULL && (b & 0x000FFFFFFFFFFFFFULL)) {
+                const uint64_t nan_e = (K.nulls_first ^ K.desc) ? 0ULL : ~0ULL;
+                return K.desc ? ~nan_e : nan_e;
+            }
+            e = b ^ ((0ULL - (b >> 63)) | (1ULL << 63));
+            break;
+        }
+        case T_SYM: {
+            const int w = elem_size(c.type, c.attrs);
+            uint32_t id;
+            if (w == 1) id = ((const uint8_t*)c.data)[r];
+            else if (w == 2) id = ((const uint16_t*)c.data)[r];
+            else if (w == 4) id = ((const uint32_t*)c.data)[r];
+            else id = (uint32_t)((const long long*)c.data)[r];
+            e = K.sym_rank[id];
+            break;
+        }
+        default:
+            e = 0;
+            break;
+    }
+    return K.desc ? ~e : e;
+}
+
+// keys[i] = encoded key of row perm[i]; folds the min and max into mm[0..1].
+__global__ void __launch_bounds__(kThreads) k_sort_encode(const tdg_sort_key K, const int64_t* __restrict__ perm,
+                                                          int64_t n, uint64_t* __restrict__ keys,
+                                                          unsigned long long* mm) {
+    unsigned long long lo = ~0ULL, hi = 0ULL;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint64_t e = sort_encode(K, perm[i]);
+        keys[i] = e;
+        lo = e < lo ? e : lo;
+        hi = e > hi ? e : hi;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long a = __shfl_xor_sync(0xffffffffu, lo, o);
+        const unsigned long long b = __shfl_xor_sync(0xffffffffu, hi, o);
+        lo = a < lo ? a : lo;
+        hi = b > hi ? b : hi;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(mm, lo);
+        atomicMax(mm + 1, hi);
+    }
+}
+
+__global__ void k_sort_iota(int64_t* __restrict__ perm, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        perm[i] = i;
+}
+
+__global__ void k_sort_mm_init(unsigned long long* mm) { mm[0] = ~0ULL; mm[1] = 0ULL; }
+
+// hist[d * n_tiles + tile]: rows of the tile whose digit ((key - kmin) >> shift) & 255 is d.
+__global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint64_t* __restrict__ keys, int64_t n,
+                                                             uint64_t kmin, int shift, uint32_t* __restrict__ hist,
+                                                             int64_t n_tiles) {
+    __shared__ uint32_t h[256];
+    h[threadIdx.x] = 0;
+    __syncthreads();
+    const int64_t t0 = blockIdx.x * kSortTile;
+    for (int q = 0; q < kSortRounds; q++) {
+        const int64_t i = t0 + (int64_t)q * kSortThreads + threadIdx.x;
+        if (i < n) atomicAdd(&h[((keys[i] - kmin) >> shift) & 255], 1u);
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * n_tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// In-place exclusive prefix of a[0, m) (m <= 2^32 rows in total), one CTA.
+__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* a, int64_t m) {
+    __shared__ uint32_t part[1024];
+    const int64_t per = (m + blockDim.x - 1) / blockDim.x;
+    const int64_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
+    uint32_t s = 0;
+    for (int64_t i = b; i < e; i++) s += a[i];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int off = 1; off < (int)blockDim.x; off <<= 1) {
+        const uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part[threadIdx.x] += v;
+        __syncthreads();
+    }
+    uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
+    for (int64_t i = b; i < e; i++) {
+        const uint32_t v = a[i];
+        a[i] = run;
+        run += v;
+    }
+}
+
+// The stable scatter of one pass.  A tile's rows go 256 at a time; within a
+// round a row's place is the tile's running offset for its digit, plus the
+// rows of that digit in lower warps, plus its rank among its warp's lanes of
+// the same digit (match mask).
+__global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const uint64_t* __restrict__ kin,
+                                                                const int64_t* __restrict__ vin,
+                                                                uint64_t* __restrict__ kout, int64_t* __restrict__ vout,
+                                                                int64_t n, uint64_t kmin, int shift,
+                                                                const uint32_t* __restrict__ offs, int64_t n_tiles) {
+    __shared__ uint32_t base[256];
+    __shared__ uint32_t wc[kSortWarps][256];
+    base[threadIdx.x] = offs[(int64_t)threadIdx.x * n_tiles + blockIdx.x];
+    for (int w = 0; w < kSortWarps; w++) wc[w][threadIdx.x] = 0;
+    __syncthreads();
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned lt = (1u << lane) - 1u;
+    const int64_t t0 = blockIdx.x * kSortTile;
+    for (int q = 0; q < kSortRounds; q++) {
+        const int64_t i = t0 + (int64_t)q * kSortThreads + threadIdx.x;
+        const bool in = i < n;
+        uint64_t k = 0;
+        int64_t v = 0;
+        uint32_t d = 256;                          // rows past the end share a digit of their own
+        if (in) {
+            k = kin[i];
+            v = vin[i];
+            d = (uint32_t)(((k - kmin) >> shift) & 255);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t cnt = (uint32_t)__popc(peers), rank = (uint32_t)__popc(peers & lt);
+        const bool leader = (peers & lt) == 0;
+        if (in && leader) wc[warp][d] = cnt;
+        __syncthreads();
+        if (in) {
+            uint32_t pos = base[d] + rank;
+            for (unsigned w = 0; w < warp; w++) pos += wc[w][d];
+            kout[pos] = k;
+            vout[pos] = v;
+        }
+        __syncthreads();
+        if (in && leader) {
+            atomicAdd(&base[d], cnt);
+            wc[warp][d] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+template <typename T>
+__global__ void k_gather(const T* __restrict__ in, const int64_t* __restrict__ perm, int64_t n, T* __restrict__ out) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = in[perm[i]];
+}
+
+static bool sortable(const tdg_sort_key& k) {
+    switch (k.col.type) {
+        case T_I64: case T_TIMESTAMP: case T_I32: case T_DATE: case T_TIME: case T_F64: return true;
+        case T_SYM: return k.sym_rank != nullptr;
+        default: return false;
+    }
+}
+
+struct SortWs {
+    uint64_t* ka;
+    uint64_t* kb;
+    int64_t* va;
+    int64_t* vb;
+    uint32_t* hist;
+    unsigned long long* mm;
+};
+
+static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// Two page-locked words per host thread for the key range read-back (the
+// copy is asynchronous); pageable memory when allocation is not allowed.
+static unsigned long long* pinned_pair() {
+    static thread_local unsigned long long* w = nullptr;
+    if (no_alloc()) return nullptr;
+    if (!w && cudaMallocHost((void**)&w, 16) != cudaSuccess) { cudaGetLastError(); w = nullptr; }
+    return w;
+}
+
+static SortWs sort_ws(void* ws, int64_t n) {
+    SortWs W;
+    char* p = (char*)ws;
+    const size_t kb = al256((size_t)n * 8);
+    const int64_t n_tiles = (n + kSortTile - 1) / kSortTile;
+    W.ka = (uint64_t*)p; p += kb;
+    W.kb = (uint64_t*)p; p += kb;
+    W.va = (int64_t*)p; p += kb;
+    W.vb = (int64_t*)p; p += kb;
+    W.hist = (uint32_t*)p; p += al256((size_t)n_tiles * 256 * 4);
+    W.mm = (unsigned long long*)p;
+    return W;
+}
+
+}  // namespace tdg
+
+using namespace tdg;
+
+extern "C" size_t tdg_sort_ws_bytes(int64_t n) {
+    if (n < 0) n = 0;
+    const int64_t n_tiles = (n + kSortTile - 1) / kSortTile;
+    return 4 * al256((size_t)n * 8) + al256((size_t)n_tiles * 256 * 4) + 256;
+}
+
+extern "C" tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, int64_t n, void* ws, int64_t* perm,
+                                    void* stream) {
+    if ((n_keys > 0 && !keys) || n_keys < 0 || n_keys > TDG_MAX_SORT_KEYS || n < 0) return E_RANGE;
+    if (n > (int64_t)UINT32_MAX) return E_RANGE;                     // 32-bit positions in the scatter
+    for (int k = 0; k < n_keys; k++) if (!sortable(keys[k])) return E_NYI;
+    if (n == 0) return E_OK;
+    if (!ws || !perm) return E_RANGE;
+    cudaStream_t s = (cudaStream_t)stream;
+    SortWs W = sort_ws(ws, n);
+    const int64_t n_tiles = (n + kSortTile - 1) / kSortTile;
+    const int g = grid_for((const void*)k_sort_iota, kThreads, 0, n);
+    (note_launch(), k_sort_iota<<<g, kThreads, 0, s>>>(W.va, n));
+    int64_t* cur = W.va;
+    int64_t* alt = W.vb;
+    unsigned long long* mmh = pinned_pair();
+    unsigned long long mm_local[2];
+    tdg_status st = E_OK;
+    // the last key first: a stable sort by each earlier key keeps the later ones' order within ties
+    for (int k = n_keys - 1; k >= 0 && !st; k--) {
+        (note_launch(), k_sort_mm_init<<<1, 1, 0, s>>>(W.mm));
+        const int ge = grid_for((const void*)k_sort_encode, kThreads, 0, n);
+        (note_launch(), k_sort_encode<<<ge, kThreads, 0, s>>>(keys[k], cur, n, W.ka, W.mm));
+        unsigned long long* mm = mmh ? mmh : mm_local;
+        if (cudaMemcpyAsync(mm, W.mm, 16, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) { st = launch_status(); if (!st) st = E_IO; break; }
+        const uint64_t kmin = mm[0], range = mm[1] - mm[0];
+        int bits = 0;
+        while (bits < 64 && (range >> bits) != 0) bits++;
+        uint64_t* kc = W.ka;
+        uint64_t* kd = W.kb;
+        for (int shift = 0; shift < bits; shift += 8) {
+            (note_launch(), k_sort_hist<<<(unsigned)n_tiles, kSortThreads, 0, s>>>(kc, n, kmin, shift, W.hist, n_tiles));
+            (note_launch(), k_sort_scan<<<1, 1024, 0, s>>>(W.hist, n_tiles * 256));
+            (note_launch(), k_sort_scatter<<<(unsigned)n_tiles, kSortThreads, 0, s>>>(kc, cur, kd, alt, n, kmin, shift,
+                                                                                     W.hist, n_tiles));
+            uint64_t* tk = kc; kc = kd; kd = tk;
+            int64_t* tv = cur; cur = alt; alt = tv;
+        }
+        st = launch_status();
+    }
+    if (!st && cudaMemcpyAsync(perm, cur, (size_t)n * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess) st = E_IO;
+    if (!st) st = launch_status();
+    return st;
+}
+
+extern "C" tdg_status tdg_gather(const tdg_col* in, const int64_t* perm, int64_t n_out, void* out, void* stream) {
+    if (!in || n_out < 0) return E_RANGE;
+    if (n_out == 0) return E_OK;
+    if (!in->data || !perm || !out) return E_RANGE;
+    cudaStream_t s = (cudaStream_t)stream;
+    const int w = elem_size(in->type, in->attrs);
+    const int g = grid_for((const void*)k_gather<long long>, kThreads, 0, n_out);
+    switch (w) {
+        case 1: (note_launch(), k_gather<uint8_t><<<g, kThreads, 0, s>>>((const uint8_t*)in->data, perm, n_out, (uint8_t*)out)); break;
+        case 2: (note_launch(), k_gather<uint16_t><<<g, kThreads, 0, s>>>((const uint16_t*)in->data, perm, n_out, (uint16_t*)out)); break;
+        case 4: (note_launch(), k_gather<uint32_t><<<g, kThreads, 0, s>>>((const uint32_t*)in->data, perm, n_out, (uint32_t*)out)); break;
+        case 8: (note_launch(), k_gather<unsigned long long><<<g, kThreads, 0, s>>>((const unsigned long long*)in->data, perm, n_out, (unsigned long long*)out)); break;
+        default: return E_TYPE;
+    }
+    return launch_status();
+}

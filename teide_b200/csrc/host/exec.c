@@ -892,6 +892,155 @@ static td_t* exec_group_node(ex_t* x, td_op_t* op) {
 }
 
 /* Evaluate op; sets *out (retained value) and returns its obj or an error. */
+/* ---- sort ------------------------------------------------------------------------------- */
+
+typedef struct { const char* p; uint32_t len; uint32_t id; } symstr_t;
+
+static int symstr_cmp(const void* a, const void* b) {
+    const symstr_t* x = a;
+    const symstr_t* y = b;
+    const uint32_t ml = x->len < y->len ? x->len : y->len;
+    int c = ml ? memcmp(x->p, y->p, ml) : 0;
+    if (!c) c = (x->len > y->len) - (x->len < y->len);
+    if (!c) c = (x->id > y->id) - (x->id < y->id);
+    return c;
+}
+
+static uint32_t sym_id_at(td_t* col, int64_t i) {
+    const void* d = td_data(col);
+    switch (td_sym_elem_size(col->type, col->attrs)) {
+        case 1: return ((const uint8_t*)d)[i];
+        case 2: return ((const uint16_t*)d)[i];
+        case 4: return ((const uint32_t*)d)[i];
+        default: return (uint32_t)((const int64_t*)d)[i];
+    }
+}
+
+/* Rank of every intern id up to the column's largest, by its string: the
+ * bytes of the shorter length, then the length (build_enum_rank,
+ * exec.c:2876-2975); returned as a device array. */
+static const uint32_t* sym_rank_dev(ex_t* x, td_t* col) {
+    uint32_t max_id = 0;
+    for (int64_t i = 0; i < col->len; i++) {
+        const uint32_t v = sym_id_at(col, i);
+        if (v > max_id) max_id = v;
+    }
+    if (max_id >= UINT32_MAX - 1) return NULL;
+    const uint32_t n_ids = max_id + 1;
+    symstr_t* s = malloc((size_t)n_ids * sizeof(symstr_t));
+    uint32_t* rank = malloc((size_t)n_ids * sizeof(uint32_t));
+    uint32_t* d = rank ? tdb_dev_alloc(&x->c, (size_t)n_ids * sizeof(uint32_t)) : NULL;
+    if (!s || !rank || !d) { free(s); free(rank); return NULL; }
+    for (uint32_t i = 0; i < n_ids; i++) {
+        td_t* str = td_sym_str((int64_t)i);
+        s[i].p = str ? td_str_ptr(str) : NULL;
+        s[i].len = str ? (uint32_t)td_str_len(str) : 0;
+        s[i].id = i;
+    }
+    qsort(s, n_ids, sizeof(symstr_t), symstr_cmp);
+    for (uint32_t i = 0; i < n_ids; i++) rank[s[i].id] = i;
+    int st = tdb_h2d(&x->c, d, rank, (size_t)n_ids * sizeof(uint32_t));
+    free(s);
+    free(rank);
+    return st ? NULL : d;
+}
+
+/* Sort a table by the node's key columns on the device and keep the first
+ * `limit` rows (all when limit < 0): exec_sort (exec.c:3370-3862), with
+ * HEAD(SORT) as in exec.c:11895-11917.  Keys are column scans of the sorted
+ * table; the table's columns that came from an earlier step of this query
+ * are still on the device, so only host-born columns are uploaded. */
+static td_t* exec_sort_node(ex_t* x, td_op_t* sop, int64_t limit) {
+    td_graph_t* g = x->g;
+    td_op_ext_t* ext = tdb_find_ext(g, sop->id);
+    if (!ext || ext->sort.n_cols > TDG_MAX_SORT_KEYS) return TD_ERR_PTR(TD_ERR_NYI);
+    val_t in;
+    td_t* r = exec_value(x, sop->inputs[0], &in);
+    if (TD_IS_ERR(r)) return r;
+    td_t* tbl = materialize(x, &in);
+    vfree(&in);
+    if (TD_IS_ERR(tbl)) return tbl;
+    if (tbl->type != TD_TABLE) { td_release(tbl); return TD_ERR_PTR(TD_ERR_TYPE); }
+    const int64_t n = td_table_nrows(tbl);
+    const int64_t n_out = limit >= 0 && limit < n ? limit : n;
+    const int nk = ext->sort.n_cols;
+    tdg_sort_key keys[TDG_MAX_SORT_KEYS];
+    td_t* res = NULL;
+    int st = 0;
+    for (int k = 0; k < nk && !st; k++) {
+        td_op_ext_t* ke = tdb_find_ext(g, ext->sort.columns[k]->id);
+        if (!ke || ke->base.opcode != OP_SCAN) { st = TD_ERR_NYI; break; }
+        td_t* col = td_table_get_col(tbl, ke->sym);
+        if (!col) { st = TD_ERR_SCHEMA; break; }
+        tdb_devcol d;
+        st = tdb_col_device(&x->c, col, 0, &d);
+        if (st) break;
+        memset(&keys[k], 0, sizeof(keys[k]));
+        keys[k].col.data = d.dptr;
+        keys[k].col.type = d.type;
+        keys[k].col.attrs = d.attrs;
+        keys[k].desc = ext->sort.desc ? ext->sort.desc[k] : 0;
+        keys[k].nulls_first = ext->sort.nulls_first ? ext->sort.nulls_first[k] : keys[k].desc;
+        if (d.type == TD_SYM && !(keys[k].sym_rank = sym_rank_dev(x, col))) st = TD_ERR_OOM;
+    }
+    void* ws = st ? NULL : tdb_dev_alloc(&x->c, tdg_sort_ws_bytes(n));
+    int64_t* perm = st ? NULL : tdb_dev_alloc(&x->c, (size_t)(n ? n : 1) * 8);
+    if (!st && (!ws || !perm)) st = TD_ERR_OOM;
+    if (!st) st = CALL(tdg_sort_perm(keys, nk, n, ws, perm, x->c.stream));
+    tdg_col cols[MAX_TCOLS];
+    int nc = 0;
+    if (!st) {
+        nc = table_dev_cols(x, tbl, cols, MAX_TCOLS);
+        if (nc < 0) st = -nc;
+    }
+    if (!st) {
+        res = td_table_new(nc);
+        if (!res || TD_IS_ERR(res)) { st = res ? TD_ERR_CODE(res) : TD_ERR_OOM; res = NULL; }
+    }
+    for (int j = 0; j < nc && !st; j++) {
+        void* out = tdb_dev_alloc(&x->c, (size_t)(n_out ? n_out : 1) * td_sym_elem_size(cols[j].type, cols[j].attrs));
+        if (!out) { st = TD_ERR_OOM; break; }
+        st = CALL(tdg_gather(&cols[j], perm, n_out, out, x->c.stream));
+        if (st) break;
+        td_t* col = fetch_vec_q(x, out, cols[j].type, cols[j].attrs, n_out, 1);
+        if (TD_IS_ERR(col)) { st = TD_ERR_CODE(col); break; }
+        td_t* t2 = td_table_add_col(res, td_table_col_name(tbl, j), col);
+        td_release(col);
+        if (TD_IS_ERR(t2)) { st = TD_ERR_CODE(t2); break; }
+        res = t2;
+    }
+    int st2 = tdb_ctx_sync(&x->c);                 /* the queued copies land before anything is returned or freed */
+    if (!st) st = st2;
+    td_release(tbl);
+    if (st) {
+        if (res) td_release(res);
+        return TD_ERR_PTR(st);
+    }
+    return res;
+}
+
+/* The first m elements of a vector, as a new vector with inline data. */
+static td_t* vec_prefix(td_t* v, int64_t m) {
+    td_t* c = vec_like(v->type, v->attrs, m);
+    if (!c || TD_IS_ERR(c)) return c ? c : TD_ERR_PTR(TD_ERR_OOM);
+    if (m) memcpy(td_data(c), td_data(v), (size_t)m * td_sym_elem_size(v->type, v->attrs));
+    return c;
+}
+
+/* HEAD of anything but a sort: the first n rows, copied. */
+static td_t* head_rows(td_t* v, int64_t limit) {
+    if (v->type != TD_TABLE) return vec_prefix(v, limit < v->len ? limit : v->len);
+    const int64_t n = td_table_nrows(v), m = limit < n ? limit : n;
+    td_t* out = td_table_new(td_table_ncols(v));
+    for (int64_t j = 0; j < td_table_ncols(v) && out && !TD_IS_ERR(out); j++) {
+        td_t* s = vec_prefix(td_table_get_col_idx(v, j), m);
+        if (TD_IS_ERR(s)) { td_release(out); return s; }
+        out = td_table_add_col(out, td_table_col_name(v, j), s);
+        td_release(s);
+    }
+    return out ? out : TD_ERR_PTR(TD_ERR_OOM);
+}
+
 static td_t* exec_value(ex_t* x, td_op_t* op, val_t* out) {
     *out = vnone();
     if (!op) return TD_ERR_PTR(TD_ERR_NYI);
@@ -977,6 +1126,34 @@ static td_t* exec_value(ex_t* x, td_op_t* op, val_t* out) {
             }
             vfree(&lv);
             vfree(&rv);
+            if (TD_IS_ERR(res)) return res;
+            out->obj = res;
+            return res;
+        }
+        case OP_SORT: {
+            td_t* res = exec_sort_node(x, op, -1);
+            if (TD_IS_ERR(res)) return res;
+            out->obj = res;
+            return res;
+        }
+        case OP_HEAD: {
+            td_op_ext_t* he = tdb_find_ext(g, op->id);
+            int64_t limit = he ? he->sym : 10;
+            if (limit < 0) limit = 0;
+            td_op_t* child = op->inputs[0];
+            td_t* res;
+            if (child && child->opcode == OP_SORT) {
+                res = exec_sort_node(x, child, limit);
+            } else {
+                val_t in;
+                td_t* r = exec_value(x, child, &in);
+                if (TD_IS_ERR(r)) return r;
+                td_t* v = materialize(x, &in);
+                vfree(&in);
+                if (TD_IS_ERR(v)) return v;
+                res = head_rows(v, limit);
+                td_release(v);
+            }
             if (TD_IS_ERR(res)) return res;
             out->obj = res;
             return res;

@@ -285,6 +285,48 @@ td_op_t* td_group(td_graph_t* g, td_op_t** keys, uint8_t n_keys,
     return publish(g, e);
 }
 
+/* Sort node (graph.c:620-663 of Teide): key columns, DESC flags and
+ * nulls-first flags stored after the ext node; nulls_first defaults to DESC
+ * (NULLS LAST ascending, NULLS FIRST descending). */
+td_op_t* td_sort_op(td_graph_t* g, td_op_t* table_node, td_op_t** keys, uint8_t* descs, uint8_t* nulls_first,
+                    uint8_t n_cols) {
+    uint32_t ti = table_node->id, kid[256];
+    for (int i = 0; i < n_cols; i++) kid[i] = keys[i]->id;
+    size_t ksz = (size_t)n_cols * sizeof(td_op_t*);
+    td_op_ext_t* e = new_ext(g, ksz + 2 * (size_t)n_cols);
+    if (!e) return NULL;
+    char* trail = (char*)(e + 1);
+    e->base.opcode = OP_SORT;
+    e->base.arity = 1;
+    e->base.inputs[0] = &g->nodes[ti];
+    e->base.out_type = TD_TABLE;
+    e->base.est_rows = g->nodes[ti].est_rows;
+    e->sort.columns = (td_op_t**)trail;
+    for (int i = 0; i < n_cols; i++) e->sort.columns[i] = &g->nodes[kid[i]];
+    e->sort.desc = (uint8_t*)(trail + ksz);
+    e->sort.nulls_first = (uint8_t*)(trail + ksz + n_cols);
+    for (int i = 0; i < n_cols; i++) {
+        e->sort.desc[i] = descs ? descs[i] : 0;
+        e->sort.nulls_first[i] = nulls_first ? nulls_first[i] : e->sort.desc[i];
+    }
+    e->sort.n_cols = n_cols;
+    return publish(g, e);
+}
+
+/* First n rows (graph.c:906-922 of Teide): n is kept in the ext node's sym. */
+td_op_t* td_head(td_graph_t* g, td_op_t* input, int64_t n) {
+    uint32_t ii = input->id;
+    td_op_ext_t* e = new_ext(g, 0);
+    if (!e) return NULL;
+    e->base.opcode = OP_HEAD;
+    e->base.arity = 1;
+    e->base.inputs[0] = &g->nodes[ii];
+    e->base.out_type = g->nodes[ii].out_type;
+    e->base.est_rows = (uint32_t)n;
+    e->sym = n;
+    return publish(g, e);
+}
+
 td_op_t* td_distinct(td_graph_t* g, td_op_t** keys, uint8_t n_keys) {
     return td_group(g, keys, n_keys, NULL, NULL, 0);
 }

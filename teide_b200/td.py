@@ -85,6 +85,8 @@ class Td:
             "td_sel_new": (P, [C.c_int64]), "td_sel_from_pred": (P, [P]),
             "td_sel_and": (P, [P, P]), "td_sel_recompute": (None, [P]),
             "td_cancel": (None, []),
+            "td_sort_op": (P, [P, P, P, P, P, C.c_uint8]),
+            "td_head": (P, [P, P, C.c_int64]),
         }
         for name in ("td_eq", "td_ne", "td_lt", "td_le", "td_gt", "td_ge", "td_and", "td_or",
                      "td_add", "td_sub", "td_mul", "td_div", "td_mod", "td_min2", "td_max2"):
@@ -276,6 +278,18 @@ class Graph:
         LK = (P * n)(*lkeys)
         RK = (P * n)(*rkeys)
         return self._ok(self.L.td_join(self.g, left, LK, right, RK, n, join_type), "join")
+
+    def sort(self, table_node, keys, descs=None, nulls_first=None):
+        """td_sort_op: rows of table_node ordered by the key columns (scans);
+        nulls_first None keeps Teide's default (DESC flags)."""
+        n = len(keys)
+        K = (P * max(n, 1))(*keys)
+        D = (C.c_uint8 * max(n, 1))(*(descs or [0] * n))
+        NF = (C.c_uint8 * max(n, 1))(*nulls_first) if nulls_first is not None else None
+        return self._ok(self.L.td_sort_op(self.g, table_node, K, D, NF, n), "sort")
+
+    def head(self, inp, n):
+        return self._ok(self.L.td_head(self.g, inp, int(n)), "head")
 
     def execute(self, root, optimize=True):
         if optimize:
