@@ -15,8 +15,9 @@ data; inputs (2.56 GB) are larger than L2, so no flush is needed between steps.
          (24 B per probe row: fk, qty, price) / its CUDA-event duration
 
 Other workloads (--workload): "group_radix" (200M rows, Zipf keys over 2^24,
-filter v1 > 0, COUNT/SUM/MIN/MAX/AVG) and "readme_group" (10M rows, filter
-flag == 0, group by region, SUM(amount)).
+filter v1 > 0, COUNT/SUM/MIN/MAX/AVG), "group_sort" (the same group-by with its
+5.9M groups sorted by v1_sum descending: td_sort_op over the group node) and
+"readme_group" (10M rows, filter flag == 0, group by region, SUM(amount)).
 
 --impl reference runs Teide's own CPU engine (compiled from its sources into
 oracle/_ref/) on a bounded sample of the same workload per step, with every
@@ -117,7 +118,7 @@ def make_tables(td, workload, rank, device, scale=1.0):
         b, p = workloads.config3(n_probe=int(100_000_000 * scale), seed=3 + 1000 * rank, device=device)
         bt, pt = td.table(b), td.table(p)
         return {"build": bt, "probe": pt}, len(p["fk"]), 16 * len(b["pk"]) + 24 * len(p["fk"]), 24 * len(p["fk"])
-    if workload == "group_radix":
+    if workload in ("group_radix", "group_sort"):
         c = workloads.config2(n=int(200_000_000 * scale), seed=2 + 1000 * rank, device=device)
         t = td.table(c)
         return {"t": t}, len(c["key"]), 24 * len(c["key"]), 24 * len(c["key"])
@@ -129,10 +130,12 @@ def make_tables(td, workload, rank, device, scale=1.0):
 def run_query(td, workload, tabs, world=1):
     """One step.  With several ranks every rank runs its shard and the partial
     groups are merged across ranks (teide_b200.shard) inside the step."""
-    from gpu_pipelines import fused_join_group, readme_group
+    from gpu_pipelines import fused_join_group, group_sorted, readme_group
     from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
     if world > 1:
         from teide_b200 import shard
+        if workload == "group_sort":
+            raise SystemExit("group_sort runs on one GPU (the sharded merge returns unsorted groups)")
         if workload == "join_group":
             return shard.sharded_join_group(td, tabs["build"], tabs["probe"], ("qty", "gt", 10), "fk", "pk",
                                             ["cat"], [(OP_SUM, "price"), (OP_COUNT, "price")])
@@ -147,6 +150,10 @@ def run_query(td, workload, tabs, world=1):
         return readme_group(td, tabs["t"], ("v1", "gt", 0), ["key"],
                             [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")],
                             as_dict=False)
+    if workload == "group_sort":
+        return group_sorted(td, tabs["t"], ("v1", "gt", 0), ["key"],
+                            [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")],
+                            "v1_sum", desc=True, as_dict=False)
     return readme_group(td, tabs["t"], ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")], as_dict=False)
 
 
@@ -461,7 +468,7 @@ def serve_reference(td):
 def reference_sample(workload, scale_rows):
     """Teide's CPU engine on a bounded sample of the workload: returns
     (seconds per query, rows per query, description)."""
-    from gpu_pipelines import join_then_group, two_graph_group
+    from gpu_pipelines import join_then_group, two_graph_group, two_graph_group_sorted
     from teide_b200 import workloads
     from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM, Td
     td = Td(REF_LIB)
@@ -487,6 +494,15 @@ def reference_sample(workload, scale_rows):
             two_graph_group(td, t, ("v1", "gt", 0), ["key"],
                             [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")])
         desc = f"{scale_rows / 1e6:g}M of 200M rows per query"
+    elif workload == "group_sort":
+        c = workloads.config2(n=scale_rows, seed=32)
+        t = td.table(c)
+
+        def q():
+            two_graph_group_sorted(td, t, ("v1", "gt", 0), ["key"],
+                                   [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")],
+                                   "v1_sum", desc=True)
+        desc = f"{scale_rows / 1e6:g}M of 200M rows per query, group result sorted by v1_sum DESC"
     else:
         c = workloads.config1(n=scale_rows, seed=31)
         t = td.table(c)
@@ -503,8 +519,8 @@ def reference_arm(args):
     if not os.path.exists(REF_LIB):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libteide_ref.so not built"}))
         return
-    rows = {"join_group": 10_000_000, "group_radix": 20_000_000, "readme_group": 10_000_000,
-            "batch": BATCH_REF_QUERIES, "serve": SERVE_REF_REQUESTS}[args.workload]
+    rows = {"join_group": 10_000_000, "group_radix": 20_000_000, "group_sort": 20_000_000,
+            "readme_group": 10_000_000, "batch": BATCH_REF_QUERIES, "serve": SERVE_REF_REQUESTS}[args.workload]
     td, q, desc = reference_sample(args.workload, rows)
     if args.workload == "serve":                 # q() reports its own query seconds
         for _ in range(min(args.warmup, 1)):
@@ -538,7 +554,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="teide_b200", choices=["teide_b200", "reference"])
-    ap.add_argument("--workload", default="join_group", choices=["join_group", "group_radix", "readme_group", "batch", "serve"])
+    ap.add_argument("--workload", default="join_group", choices=["join_group", "group_radix", "group_sort", "readme_group", "batch",
+                                                        "serve"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-table (upload) pass")
@@ -569,6 +586,7 @@ def main():
     L.tdg_set_timing.argtypes = [__import__("ctypes").c_int32]
     L.tdg_last_main_ms.restype = __import__("ctypes").c_float
     L.tdg_last_build_ms.restype = __import__("ctypes").c_float
+    L.tdg_last_sort_ms.restype = __import__("ctypes").c_float
     L.tdg_launch_count.restype = __import__("ctypes").c_uint64
     L.td_gpu_pin.argtypes = [__import__("ctypes").c_void_p]
     L.td_gpu_unpin.argtypes = [__import__("ctypes").c_void_p]
@@ -609,7 +627,7 @@ def main():
         run_query(td, args.workload, tabs, world)
     barrier()
     l0 = L.tdg_launch_count()
-    main_ms, build_ms = [], []
+    main_ms, build_ms, sort_ms = [], [], []
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     tc0 = time.monotonic()
     ev0.record()
@@ -617,6 +635,7 @@ def main():
         run_query(td, args.workload, tabs, world)
         main_ms.append(L.tdg_last_main_ms())
         build_ms.append(L.tdg_last_build_ms())
+        sort_ms.append(L.tdg_last_sort_ms())
     ev1.record()
     torch.cuda.synchronize()
     tc1 = time.monotonic()
@@ -652,6 +671,7 @@ def main():
     mean_main = sum(main_ms) / len(main_ms) if main_ms else 0.0
     achieved = main_bytes / (mean_main / 1e3) / 1e9 if mean_main > 0 else None
     prof = {"join_group": "k_probe_vec_join_group.md", "group_radix": "k_group_vec_part_agg_group_radix.md",
+            "group_sort": "k_group_vec_part_agg_group_radix.md",
             "readme_group": "k_group_vec_readme_group.md"}[args.workload]
     line = {
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
@@ -669,6 +689,7 @@ def main():
                      "kernel": {"join_group": "k_probe_vec (fused probe + aggregate)",
                                 "group_radix": "k_group_vec + k_part_agg (hot slots in shared memory, cold rows "
                                                "partitioned by slot range and aggregated per partition)",
+                                "group_sort": "k_group_vec + k_part_agg (the group-by; the sort is sort_ms)",
                                 "readme_group": "k_group_vec (one key, 16-byte column loads)"}[args.workload],
                      "bytes_per_launch": main_bytes,
                      "mean_launch_ms": mean_main, "peak_source": peak_kind,
@@ -679,8 +700,11 @@ def main():
         "clocks": clk.summary(tc0, tc1),
         "resident_h2d_bytes_per_step": int(s_res.h2d),
     }
+    if args.workload == "group_sort" and sort_ms:
+        line["sort_ms"] = sum(sort_ms) / len(sort_ms)      # tdg_sort_perm: the 5.9M-row permutation
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
-        rows_s = {"join_group": 10_000_000, "group_radix": 20_000_000, "readme_group": 10_000_000}[args.workload]
+        rows_s = {"join_group": 10_000_000, "group_radix": 20_000_000, "group_sort": 20_000_000,
+                  "readme_group": 10_000_000}[args.workload]
         rtd, q, desc = reference_sample(args.workload, rows_s)
         q()
         t0 = time.perf_counter()

@@ -356,13 +356,15 @@ int32_t tdg_device_sm_count(void);
  * kernel; the last durations are read back here in milliseconds.  Timing
  * adds no synchronization beyond the one each call already does, except in
  * tdg_batch_run, which waits for its aggregation kernel's end event (and
- * records nothing while its stream is being captured into a CUDA graph). */
+ * records nothing while its stream is being captured into a CUDA graph), and
+ * tdg_sort_perm, which waits for its end event. */
 void     tdg_set_timing(int32_t on);
 int32_t  tdg_timing_enabled(void);
 /* A host that replays captured tdg launches (a CUDA graph) counts them here. */
 void     tdg_count_launches(uint64_t n);
 float    tdg_last_main_ms(void);
 float    tdg_last_build_ms(void);
+float    tdg_last_sort_ms(void);    /* the last tdg_sort_perm (timing on), CUDA events */
 /* Kernels launched by this library since the process started. */
 uint64_t tdg_launch_count(void);
 

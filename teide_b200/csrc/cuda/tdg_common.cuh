@@ -360,6 +360,7 @@ struct EventTimer {
 bool timing_on();
 void set_last_main_ms(float ms);
 void set_last_build_ms(float ms);
+void set_last_sort_ms(float ms);
 
 // While alive, this thread's tdg calls record no timing events.
 // While alive, this thread's tdg calls make no allocating CUDA call (no

@@ -61,6 +61,8 @@ void note_launch(int n) { g_launches.fetch_add((unsigned long long)n, std::memor
 bool timing_on() { return g_timing.load(std::memory_order_relaxed) != 0 && t_timing_off == 0; }
 void set_last_main_ms(float ms) { g_main_ms.store(ms); }
 void set_last_build_ms(float ms) { g_build_ms.store(ms); }
+static std::atomic<float> g_sort_ms{0.f};
+void set_last_sort_ms(float ms) { g_sort_ms.store(ms); }
 
 void EventTimer::start(cudaStream_t s) {
     on = timing_on();
@@ -422,4 +424,5 @@ extern "C" int32_t tdg_timing_enabled(void) { return g_timing.load(); }
 extern "C" void tdg_count_launches(uint64_t n) { note_launch((int)n); }
 extern "C" float tdg_last_main_ms(void) { return g_main_ms.load(); }
 extern "C" float tdg_last_build_ms(void) { return g_build_ms.load(); }
+extern "C" float tdg_last_sort_ms(void) { return g_sort_ms.load(); }
 extern "C" uint64_t tdg_launch_count(void) { return g_launches.load(); }

@@ -13,7 +13,7 @@
 // key range (max - min of the encoded keys) sets the number of passes.
 //
 // One pass over n keys: a per-tile digit histogram, a prefix over
-// (digit, tile), and a stable scatter in which every tile ranks its rows 256
+// (digit, tile) in three coalesced steps, and a stable scatter in which every tile ranks its rows 256
 // at a time with warp match masks, so rows of equal digit keep their order.
 #include "tdg_common.cuh"
 #include <string.h>
@@ -111,26 +111,80 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_hist(const uint64_t* __re
     hist[(int64_t)threadIdx.x * n_tiles + blockIdx.x] = h[threadIdx.x];
 }
 
-// In-place exclusive prefix of a[0, m) (m <= 2^32 rows in total), one CTA.
-__global__ void __launch_bounds__(1024) k_sort_scan(uint32_t* a, int64_t m) {
-    __shared__ uint32_t part[1024];
-    const int64_t per = (m + blockDim.x - 1) / blockDim.x;
-    const int64_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
-    uint32_t s = 0;
-    for (int64_t i = b; i < e; i++) s += a[i];
-    part[threadIdx.x] = s;
+// In-place exclusive prefix of a[0, m) in three steps: every CTA sums a
+// segment of kScanSeg entries, one CTA scans those sums, and every CTA
+// rescans its segment from its offset -- coalesced, and all SMs take part.
+constexpr int kScanThreads = 1024;
+constexpr int kScanPer = 4;
+constexpr int64_t kScanSeg = (int64_t)kScanThreads * kScanPer;
+
+__device__ __forceinline__ uint32_t block_incl_scan(uint32_t x, uint32_t* wsum) {
+    const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+        if (lane >= (unsigned)o) x += y;
+    }
+    if (lane == 31) wsum[warp] = x;
     __syncthreads();
-    for (int off = 1; off < (int)blockDim.x; off <<= 1) {
-        const uint32_t v = threadIdx.x >= (unsigned)off ? part[threadIdx.x - off] : 0u;
-        __syncthreads();
-        part[threadIdx.x] += v;
+    if (warp == 0) {
+        uint32_t w = lane < (blockDim.x >> 5) ? wsum[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= (unsigned)o) w += y;
+        }
+        wsum[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t r = x + (warp ? wsum[warp - 1] : 0u);
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_sums(const uint32_t* __restrict__ a, int64_t m,
+                                                            uint32_t* __restrict__ sums) {
+    __shared__ uint32_t wsum[32];
+    const int64_t b = blockIdx.x * kScanSeg + (int64_t)threadIdx.x * kScanPer;
+    uint32_t t = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) t += b + k < m ? a[b + k] : 0u;
+    const uint32_t incl = block_incl_scan(t, wsum);
+    if (threadIdx.x == blockDim.x - 1) sums[blockIdx.x] = incl;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_top(uint32_t* sums, int64_t nb) {
+    __shared__ uint32_t wsum[32];
+    __shared__ uint32_t s_carry;
+    if (threadIdx.x == 0) s_carry = 0;
+    __syncthreads();
+    for (int64_t c = 0; c < nb; c += blockDim.x) {
+        const int64_t i = c + threadIdx.x;
+        const uint32_t v = i < nb ? sums[i] : 0u;
+        const uint32_t incl = block_incl_scan(v, wsum);
+        const uint32_t carry = s_carry;
+        if (i < nb) sums[i] = carry + incl - v;
+        __syncthreads();                                  // every thread has read the carry
+        if (threadIdx.x == blockDim.x - 1) s_carry = carry + incl;
         __syncthreads();
     }
-    uint32_t run = threadIdx.x ? part[threadIdx.x - 1] : 0u;
-    for (int64_t i = b; i < e; i++) {
-        const uint32_t v = a[i];
-        a[i] = run;
-        run += v;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_apply(uint32_t* __restrict__ a, int64_t m,
+                                                             const uint32_t* __restrict__ offs) {
+    __shared__ uint32_t wsum[32];
+    const int64_t b = blockIdx.x * kScanSeg + (int64_t)threadIdx.x * kScanPer;
+    uint32_t v[kScanPer], t = 0;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        v[k] = b + k < m ? a[b + k] : 0u;
+        t += v[k];
+    }
+    uint32_t run = offs[blockIdx.x] + block_incl_scan(t, wsum) - t;
+#pragma unroll
+    for (int k = 0; k < kScanPer; k++) {
+        if (b + k < m) a[b + k] = run;
+        run += v[k];
     }
 }
 
@@ -202,10 +256,12 @@ struct SortWs {
     int64_t* va;
     int64_t* vb;
     uint32_t* hist;
+    uint32_t* sums;
     unsigned long long* mm;
 };
 
 static size_t al256(size_t x) { return (x + 255) & ~(size_t)255; }
+static int64_t scan_blocks(int64_t n_tiles) { return (n_tiles * 256 + kScanSeg - 1) / kScanSeg; }
 
 // Two page-locked words per host thread for the key range read-back (the
 // copy is asynchronous); pageable memory when allocation is not allowed.
@@ -226,6 +282,7 @@ static SortWs sort_ws(void* ws, int64_t n) {
     W.va = (int64_t*)p; p += kb;
     W.vb = (int64_t*)p; p += kb;
     W.hist = (uint32_t*)p; p += al256((size_t)n_tiles * 256 * 4);
+    W.sums = (uint32_t*)p; p += al256((size_t)scan_blocks(n_tiles) * 4);
     W.mm = (unsigned long long*)p;
     return W;
 }
@@ -237,7 +294,7 @@ using namespace tdg;
 extern "C" size_t tdg_sort_ws_bytes(int64_t n) {
     if (n < 0) n = 0;
     const int64_t n_tiles = (n + kSortTile - 1) / kSortTile;
-    return 4 * al256((size_t)n * 8) + al256((size_t)n_tiles * 256 * 4) + 256;
+    return 4 * al256((size_t)n * 8) + al256((size_t)n_tiles * 256 * 4) + al256((size_t)scan_blocks(n_tiles) * 4) + 256;
 }
 
 extern "C" tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, int64_t n, void* ws, int64_t* perm,
@@ -248,6 +305,8 @@ extern "C" tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, in
     if (n == 0) return E_OK;
     if (!ws || !perm) return E_RANGE;
     cudaStream_t s = (cudaStream_t)stream;
+    EventTimer tm;
+    tm.start(s);
     SortWs W = sort_ws(ws, n);
     const int64_t n_tiles = (n + kSortTile - 1) / kSortTile;
     const int g = grid_for((const void*)k_sort_iota, kThreads, 0, n);
@@ -272,7 +331,10 @@ extern "C" tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, in
         uint64_t* kd = W.kb;
         for (int shift = 0; shift < bits; shift += 8) {
             (note_launch(), k_sort_hist<<<(unsigned)n_tiles, kSortThreads, 0, s>>>(kc, n, kmin, shift, W.hist, n_tiles));
-            (note_launch(), k_sort_scan<<<1, 1024, 0, s>>>(W.hist, n_tiles * 256));
+            const int64_t m = n_tiles * 256, nb = (m + kScanSeg - 1) / kScanSeg;
+            (note_launch(), k_scan_sums<<<(unsigned)nb, kScanThreads, 0, s>>>(W.hist, m, W.sums));
+            (note_launch(), k_scan_top<<<1, kScanThreads, 0, s>>>(W.sums, nb));
+            (note_launch(), k_scan_apply<<<(unsigned)nb, kScanThreads, 0, s>>>(W.hist, m, W.sums));
             (note_launch(), k_sort_scatter<<<(unsigned)n_tiles, kSortThreads, 0, s>>>(kc, cur, kd, alt, n, kmin, shift,
                                                                                      W.hist, n_tiles));
             uint64_t* tk = kc; kc = kd; kd = tk;
@@ -282,6 +344,12 @@ extern "C" tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, in
     }
     if (!st && cudaMemcpyAsync(perm, cur, (size_t)n * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess) st = E_IO;
     if (!st) st = launch_status();
+    tm.stop(s);
+    if (tm.on) {
+        if (!st && cudaStreamSynchronize(s) != cudaSuccess) st = E_IO;
+        const float ms = tm.ms();
+        if (!st) set_last_sort_ms(ms);
+    }
     return st;
 }
 

@@ -55,6 +55,7 @@ typedef struct {
 typedef struct {
     td_graph_t* g;
     tdb_ctx     c;
+    int         dev_only;      /* a group result that only a sort reads stays on the device */
 } ex_t;
 
 static val_t vnone(void) { val_t v; memset(&v, 0, sizeof(v)); return v; }
@@ -259,10 +260,14 @@ static td_t* vec_like(int8_t type, uint8_t attrs, int64_t n) {
 
 /* Copy n elements from the device into a new host vector.  With `deferred`
  * the copy is only queued: the caller synchronizes the stream (once for all
- * the columns of a result) before reading the vector. */
+ * the columns of a result) before reading the vector.  deferred == 2 marks a
+ * column the executor may leave on the device: while x->dev_only is set the
+ * vector is only the handle of its device copy (its host bytes are never
+ * written, and it does not outlive the query). */
 static td_t* fetch_vec_q(ex_t* x, const void* dptr, int8_t type, uint8_t attrs, int64_t n, int deferred) {
     td_t* v = vec_like(type, attrs, n);
     if (!v || TD_IS_ERR(v)) return v ? v : TD_ERR_PTR(TD_ERR_OOM);
+    if (deferred == 2 && x->dev_only && tdb_adopt_mirror(&x->c, v, (void*)dptr)) return v;
     size_t bytes = (size_t)n * td_sym_elem_size(type, attrs);
     if (bytes >= ((size_t)2 << 20)) tdb_pin_host(v);     /* heap-mapped block: DMA straight into it */
     int st = deferred ? tdb_d2h_async(&x->c, td_data(v), dptr, bytes) : tdb_d2h(&x->c, td_data(v), dptr, bytes);
@@ -577,7 +582,7 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
     memset(wide, 0, sizeof(wide));
     td_t* err = NULL;
     for (int k = 0; k < nk && !err; k++) {
-        cols[k] = fetch_vec_q(x, out.keys[k], keys[k].type, keys[k].attrs, ng, 1);
+        cols[k] = fetch_vec_q(x, out.keys[k], keys[k].type, keys[k].attrs, ng, 2);
         if (TD_IS_ERR(cols[k])) { err = cols[k]; cols[k] = NULL; }
     }
     for (int a = 0; a < na && !err; a++) {
@@ -590,7 +595,7 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
         td_t* v;
         if (td_sym_elem_size(ot, ins[a].attrs) == 8 || op == OP_AVG || op == OP_COUNT || op == OP_SUM) {
             int8_t vt = (ot == TD_F64 || op == OP_AVG) ? TD_F64 : (td_sym_elem_size(ot, ins[a].attrs) == 8 ? ot : TD_I64);
-            v = fetch_vec_q(x, out.aggs[a], vt, vt == TD_SYM ? ins[a].attrs : 0, ng, 1);
+            v = fetch_vec_q(x, out.aggs[a], vt, vt == TD_SYM ? ins[a].attrs : 0, ng, 2);
             if (!TD_IS_ERR(v)) cols[nk + a] = v;
         } else {
             /* MIN/MAX of a narrow integer column: int64 results, narrowed below */
@@ -955,7 +960,10 @@ static td_t* exec_sort_node(ex_t* x, td_op_t* sop, int64_t limit) {
     td_op_ext_t* ext = tdb_find_ext(g, sop->id);
     if (!ext || ext->sort.n_cols > TDG_MAX_SORT_KEYS) return TD_ERR_PTR(TD_ERR_NYI);
     val_t in;
+    const int dev_only = x->dev_only;
+    x->dev_only = sop->inputs[0] && sop->inputs[0]->opcode == OP_GROUP;   /* read only through its device copy */
     td_t* r = exec_value(x, sop->inputs[0], &in);
+    x->dev_only = dev_only;
     if (TD_IS_ERR(r)) return r;
     td_t* tbl = materialize(x, &in);
     vfree(&in);

@@ -593,17 +593,17 @@ int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
 /* Keep a device buffer this call produced as the resident mirror of the host
  * vector it was copied to: a later query over the result reads it from HBM.
  * The buffer leaves the call's transient list; it is freed with the host
- * vector (td_free) or by td_gpu_unpin. */
-void tdb_adopt_mirror(tdb_ctx* c, td_t* host, void* dptr) {
-    if (!host || TD_IS_ERR(host) || !dptr || getenv("TD_GPU_NO_RESULT_MIRROR")) return;
+ * vector (td_free) or by td_gpu_unpin.  Returns 1 when adopted. */
+int tdb_adopt_mirror(tdb_ctx* c, td_t* host, void* dptr) {
+    if (!host || TD_IS_ERR(host) || !dptr || getenv("TD_GPU_NO_RESULT_MIRROR")) return 0;
     int k = -1;
     for (int i = 0; i < c->n_tmp; i++) if (c->tmp[i] == dptr) { k = i; break; }
-    if (k < 0) return;
+    if (k < 0) return 0;
     pthread_mutex_lock(&mu);
     if (n_mir == cap_mir) {
         int ncap = cap_mir ? cap_mir * 2 : 64;
         mirror_t* nm = realloc(mirrors, (size_t)ncap * sizeof(mirror_t));
-        if (!nm) { pthread_mutex_unlock(&mu); return; }
+        if (!nm) { pthread_mutex_unlock(&mu); return 0; }
         mirrors = nm; cap_mir = ncap;
     }
     tdb_devcol dc;
@@ -613,6 +613,7 @@ void tdb_adopt_mirror(tdb_ctx* c, td_t* host, void* dptr) {
     mh_added_locked();
     pthread_mutex_unlock(&mu);
     c->tmp[k] = c->tmp[--c->n_tmp];
+    return 1;
 }
 
 td_err_t td_gpu_pin(td_t* tbl) {

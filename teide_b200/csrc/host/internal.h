@@ -96,7 +96,7 @@ void     tdb_reset_methods(void);
 int      tdb_d2h(tdb_ctx* c, void* host, const void* dev, size_t bytes);
 int      tdb_h2d(tdb_ctx* c, void* dev, const void* host, size_t bytes);
 void     tdb_mirror_forget(td_t* v);             /* host block freed or mutated */
-void     tdb_adopt_mirror(tdb_ctx* c, td_t* host, void* dptr);
+int     tdb_adopt_mirror(tdb_ctx* c, td_t* host, void* dptr);
 void     tdb_pin_host(td_t* v);                  /* page-lock a large host block */
 int      tdb_check_cancel(void);
 

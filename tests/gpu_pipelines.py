@@ -96,3 +96,42 @@ def f64_tolerance_ok(got, want, abs_sum, rel=1e-12):
 
 
 CONFIG3_AGGS = [(None, "price"), (OP_COUNT, "price")]
+
+
+def group_sorted(td, tbl, pred, keys, aggs, sort_col, desc=True, as_dict=True):
+    """One graph: README-form filter + group-by, its result sorted by
+    sort_col (td_sort_op over the group node)."""
+    g = td.graph(tbl)
+    try:
+        c, op, k = pred
+        p = g.op(op, g.scan(c), const(g, k))
+        ks = [g.filter(g.scan(name), p) for name in keys]
+        ins = [g.filter(g.scan(name), p) for _, name in aggs]
+        grp = g.group(ks, [a for a, _ in aggs], ins)
+        r = g.execute(g.sort(grp, [g.scan(sort_col)], [int(desc)]), optimize=True)
+    finally:
+        g.free()
+    return _result(td, r, as_dict)
+
+
+def two_graph_group_sorted(td, tbl, pred, keys, aggs, sort_col, desc=True):
+    """Filter graph -> compacted table -> group graph -> sort graph."""
+    g = td.graph(tbl)
+    try:
+        c, op, k = pred
+        t2 = g.execute(g.filter(g.const_table(tbl), g.op(op, g.scan(c), const(g, k))))
+    finally:
+        g.free()
+    g = td.graph(t2)
+    try:
+        grp = g.execute(g.group([g.scan(n) for n in keys], [a for a, _ in aggs], [g.scan(n) for _, n in aggs]))
+    finally:
+        g.free()
+    g = td.graph(grp)
+    try:
+        r = g.execute(g.sort(g.const_table(grp), [g.scan(sort_col)], [int(desc)]), optimize=False)
+    finally:
+        g.free()
+    td.release(grp)
+    td.release(t2)
+    td.release(r)

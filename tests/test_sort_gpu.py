@@ -44,3 +44,11 @@ def test_limit_beyond_rows_and_plain_head(gpu):
         assert np.array_equal(out["k"], d["k"][:2]) and np.array_equal(out["i"], d["i"][:2])
     finally:
         gpu.release(t)
+
+
+def test_sort_of_group_without_result_mirrors(gpu, monkeypatch):
+    """With result mirrors off the group result the sort reads is copied to
+    the host and uploaded again: same answer."""
+    monkeypatch.setenv("TD_GPU_NO_RESULT_MIRROR", "1")
+    got, want = sort_cases.sort_of_group(gpu)
+    sort_cases.same(got, want)
