@@ -127,6 +127,77 @@ def make_tables(td, workload, rank, device, scale=1.0):
     return {"t": t}, len(c["flag"]), 24 * len(c["flag"]), 24 * len(c["flag"])
 
 
+def splay_main(args, td, L, rank, world, local, barrier, max_over_ranks):
+    """A splayed table on local disk (the cfg 2 columns: key, v1, v2 at 50M
+    rows, 1.2 GB) read into HBM by td_gpu_splay_load each step: the column
+    files come from the page cache into page-locked blocks and are copied to
+    the device.  value = column bytes resident per second, whole job."""
+    import ctypes as C
+    import shutil
+    import tempfile
+    from teide_b200 import workloads
+    L.td_gpu_splay_load.restype = C.c_void_p
+    L.td_gpu_splay_load.argtypes = [C.c_char_p]
+    n = int(50_000_000 * args.scale)
+    c = workloads.config2(n=n, seed=2 + 1000 * rank, device="cuda")
+    bytes_ = sum(v.nbytes for v in c.values())
+    t = td.table(c)
+    del c
+    root = tempfile.mkdtemp(prefix="td_splay_")
+    dirp = os.path.join(root, "t").encode()
+    try:
+        if L.td_splay_save(t, dirp, None) != 0:
+            raise RuntimeError("td_splay_save failed")
+        td.release(t)
+        for _ in range(args.warmup):
+            r = td.check(L.td_gpu_splay_load(dirp), "td_gpu_splay_load")
+            L.td_gpu_unpin(r)
+            td.release(r)
+        barrier()
+        clk = Clocks(local).__enter__()
+        tc0 = time.monotonic()
+        l0 = L.tdg_launch_count()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            r = td.check(L.td_gpu_splay_load(dirp), "td_gpu_splay_load")
+            L.td_gpu_unpin(r)
+            td.release(r)
+        barrier()
+        dt = max_over_ranks((time.perf_counter() - t0) / args.steps)
+        launches = int(L.tdg_launch_count() - l0)            # the min/max statistics of each column
+        tc1 = time.monotonic()
+        clk.__exit__(None, None, None)
+        value = bytes_ * world / dt / 1e9
+        cpu = None
+        if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
+            from teide_b200.td import Td
+            rtd = Td(REF_LIB)
+            # the column files, not ".d": its name ids belong to this process's other symbol table
+            files = [os.path.join(dirp, f) for f in sorted(os.listdir(dirp)) if not f.startswith(b".")]
+            k = 0
+            t1 = time.perf_counter()
+            while k < 3:
+                for f in files:
+                    rtd.release(rtd.check(rtd.lib.td_col_load(f), "td_col_load"))
+                k += 1
+            cdt = (time.perf_counter() - t1) / k
+            cpu = {"value": bytes_ / cdt / 1e9, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                   "sample": f"Teide's td_col_load of the same {len(files)} column files into host memory, "
+                             f"mean of {k}"}
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+    return {
+        "metric": METRIC, "value": value, "unit": "GB/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+        "config": {"workload": "splay_load", "rows_per_gpu": n, "bytes_per_gpu": bytes_,
+                   "source": "column files in the page cache (written just before)", "scale": args.scale},
+        "roofline": None, "roofline_note": "bound by the host read and the host->device link, not by an HBM kernel",
+        "e2e": {"value": value, "unit": "GB/s", "h2d_bytes_per_step": bytes_, "d2h_bytes_per_step": 0},
+        "gpu_launches": launches, "clocks": clk.summary(tc0, tc1), "cpu_baseline": cpu,
+    }
+
+
 def run_query(td, workload, tabs, world=1):
     """One step.  With several ranks every rank runs its shard and the partial
     groups are merged across ranks (teide_b200.shard) inside the step."""
@@ -513,12 +584,53 @@ def reference_sample(workload, scale_rows):
     return td, q, desc
 
 
+def reference_splay(args):
+    """Teide's td_splay_load of a 50M-row splayed table (cfg 2 columns) into host memory."""
+    import ctypes as C
+    import shutil
+    import tempfile
+    from teide_b200 import workloads
+    from teide_b200.td import Td
+    td = Td(REF_LIB)
+    td.lib.td_splay_load.restype = C.c_void_p
+    n = int(50_000_000 * args.scale)
+    c = workloads.config2(n=n, seed=2)
+    bytes_ = sum(v.nbytes for v in c.values())
+    t = td.table(c)
+    del c
+    root = tempfile.mkdtemp(prefix="td_splay_ref_")
+    dirp = os.path.join(root, "t").encode()
+    try:
+        if td.lib.td_splay_save(t, dirp, None) != 0:
+            raise RuntimeError("td_splay_save failed")
+        td.release(t)
+        for _ in range(args.warmup):
+            td.release(td.check(td.lib.td_splay_load(dirp), "td_splay_load"))
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            td.release(td.check(td.lib.td_splay_load(dirp), "td_splay_load"))
+        dt = (time.perf_counter() - t0) / args.steps
+    finally:
+        shutil.rmtree(root, ignore_errors=True)
+    v = bytes_ / dt / 1e9
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "GB/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
+        "config": {"workload": "splay_load", "rows_per_gpu": n, "bytes_per_gpu": bytes_, "scale": args.scale},
+        "cpu_baseline": {"value": v, "unit": "GB/s", "cores": os.cpu_count(), "kind": "reference",
+                         "sample": "the whole table, td_splay_load into host memory"},
+        "e2e": {"value": v, "unit": "GB/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
 def reference_arm(args):
     if int(os.environ.get("RANK", "0")) != 0:
         return
     if not os.path.exists(REF_LIB):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libteide_ref.so not built"}))
         return
+    if args.workload == "splay_load":
+        return reference_splay(args)
     rows = {"join_group": 10_000_000, "group_radix": 20_000_000, "group_sort": 20_000_000,
             "readme_group": 10_000_000, "batch": BATCH_REF_QUERIES, "serve": SERVE_REF_REQUESTS}[args.workload]
     td, q, desc = reference_sample(args.workload, rows)
@@ -555,7 +667,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="teide_b200", choices=["teide_b200", "reference"])
     ap.add_argument("--workload", default="join_group", choices=["join_group", "group_radix", "group_sort", "readme_group", "batch",
-                                                        "serve"])
+                                                        "serve", "splay_load"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-table (upload) pass")
@@ -604,8 +716,8 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    if args.workload in ("batch", "serve"):
-        fn = batch_main if args.workload == "batch" else serve_main
+    if args.workload in ("batch", "serve", "splay_load"):
+        fn = {"batch": batch_main, "serve": serve_main, "splay_load": splay_main}[args.workload]
         line = fn(args, td, L, rank, world, local, barrier, max_over_ranks)
         if rank == 0:
             print(json.dumps(line))

@@ -507,6 +507,17 @@ int64_t td_table_ncols(td_t* tbl);
 int64_t td_table_nrows(td_t* tbl);
 td_t*   td_table_schema(td_t* tbl);
 
+/* Column files and splayed tables (src/store/col.c, splay.c): scalar
+ * columns as the 32-byte header plus raw data; a splayed table is a
+ * directory of column files and a ".d" file of column-name symbol ids. */
+td_err_t td_col_save(td_t* vec, const char* path);
+td_t*    td_col_load(const char* path);
+td_err_t td_splay_save(td_t* tbl, const char* dir, const char* sym_path);
+td_t*    td_splay_load(const char* dir);
+/* The symbol table file ("TSYM", count, then length-prefixed strings). */
+td_err_t td_sym_save(const char* path);
+td_err_t td_sym_load(const char* path);
+
 /* DAG construction */
 td_graph_t* td_graph_new(td_t* tbl);
 void        td_graph_free(td_graph_t* g);

@@ -110,6 +110,10 @@ void         td_server_free(td_server_t* s);
  * largest input table, 16 per row of the others). */
 size_t       td_server_estimate(td_graph_t* g, td_op_t* root);
 
+/* td_splay_load, then every column made resident in HBM (td_gpu_pin): a
+ * splayed table straight into device memory.  No counterpart in Teide. */
+td_t*        td_gpu_splay_load(const char* dir);
+
 #ifdef __cplusplus
 }
 #endif

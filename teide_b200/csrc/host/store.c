@@ -1,0 +1,283 @@
+/*
+ * Column files, splayed tables and the symbol file, in Teide's on-disk
+ * formats (src/store/col.c, src/store/splay.c, src/table/sym.c of
+ * TeideDB/teide), so files written by either library load in the other.
+ *
+ *   column file   the 32-byte td_t header (nullmap bytes kept only when the
+ *                 column has inline nulls; mmod, order, rc and the slice
+ *                 flag cleared) followed by len * element-size data bytes
+ *                 (col.c:34-41, td_col_save 344-444, td_col_load 449-561).
+ *                 Scalar types only: BOOL, U8, CHAR, I16, I32, I64, F64,
+ *                 DATE, TIME, TIMESTAMP, GUID, SYM.
+ *   splayed table a directory: ".d", an I64 column of the column-name symbol
+ *                 ids, and one column file per column named by its column
+ *                 (splay.c:46-176).
+ *   symbol file   "TSYM", a u32 count, then per symbol a u32 length and its
+ *                 bytes; loading interns them in order (sym.c:314-437).
+ *
+ * td_gpu_splay_load is the device form: the splayed table is read and its
+ * columns are made resident in HBM (td_gpu_pin), each file read straight
+ * into its final host block -- large blocks are heap-mapped and page-locked
+ * before the upload, so the data crosses PCIe at DMA speed.
+ */
+#include "internal.h"
+#include <errno.h>
+#include <pthread.h>
+#include <fcntl.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+#define TD_SYM_FILE_MAGIC 0x4D595354u            /* "TSYM" */
+
+static int serializable(int8_t t) {
+    switch (t) {
+        case TD_BOOL: case TD_U8: case TD_CHAR: case TD_I16: case TD_I32: case TD_I64: case TD_F64:
+        case TD_DATE: case TD_TIME: case TD_TIMESTAMP: case TD_GUID: case TD_SYM:
+            return 1;
+        default:
+            return 0;
+    }
+}
+
+static int write_all(int fd, const void* p, size_t n) {
+    const char* c = p;
+    while (n) {
+        ssize_t w = write(fd, c, n);
+        if (w < 0) { if (errno == EINTR) continue; return -1; }
+        c += w;
+        n -= (size_t)w;
+    }
+    return 0;
+}
+
+static int read_at(int fd, void* p, size_t n, off_t off) {
+    char* c = p;
+    while (n) {
+        ssize_t r = pread(fd, c, n, off);
+        if (r < 0) { if (errno == EINTR) continue; return -1; }
+        if (r == 0) return -1;
+        c += r;
+        n -= (size_t)r;
+        off += r;
+    }
+    return 0;
+}
+
+/* Large column files are read by several threads, each a contiguous range
+ * of the file, straight into the column's block: one copy out of the page
+ * cache, at the bandwidth of several cores. */
+#define STORE_PAR_MIN ((size_t)64 << 20)
+#define STORE_PAR_MAX 8
+
+typedef struct { int fd; char* dst; size_t n; off_t off; int bad; } rd_part_t;
+
+static void* rd_part_main(void* a) {
+    rd_part_t* r = a;
+    r->bad = read_at(r->fd, r->dst, r->n, r->off);
+    return NULL;
+}
+
+static int read_big(int fd, void* dst, size_t n, off_t off) {
+    if (n < STORE_PAR_MIN) return read_at(fd, dst, n, off);
+    long cores = sysconf(_SC_NPROCESSORS_ONLN);
+    int k = (int)(n / (STORE_PAR_MIN / 2));
+    if (k > STORE_PAR_MAX) k = STORE_PAR_MAX;
+    if (cores > 0 && k > cores) k = (int)cores;
+    if (k < 2) return read_at(fd, dst, n, off);
+    rd_part_t parts[STORE_PAR_MAX];
+    pthread_t th[STORE_PAR_MAX];
+    const size_t step = (n / (size_t)k + 4095) & ~(size_t)4095;
+    int started = 0, bad = 0;
+    for (int i = 0; i < k; i++) {
+        const size_t b = (size_t)i * step;
+        if (b >= n) break;
+        parts[i] = (rd_part_t){ fd, (char*)dst + b, b + step < n ? step : n - b, off + (off_t)b, 0 };
+        if (pthread_create(&th[i], NULL, rd_part_main, &parts[i]) != 0) { parts[i].bad = read_at(fd, parts[i].dst, parts[i].n, parts[i].off); bad |= parts[i].bad; continue; }
+        started |= 1 << i;
+    }
+    for (int i = 0; i < k; i++)
+        if (started & (1 << i)) { pthread_join(th[i], NULL); bad |= parts[i].bad; }
+    return bad ? -1 : 0;
+}
+
+td_err_t td_col_save(td_t* vec, const char* path) {
+    if (!vec || TD_IS_ERR(vec)) return TD_ERR_TYPE;
+    if (!path) return TD_ERR_IO;
+    if (!serializable(vec->type)) return TD_ERR_NYI;
+    if (vec->len < 0) return TD_ERR_CORRUPT;
+    if ((vec->attrs & TD_ATTR_HAS_NULLS) && (vec->attrs & TD_ATTR_NULLMAP_EXT)) return TD_ERR_NYI;
+    const size_t esz = td_sym_elem_size(vec->type, vec->attrs);
+    const size_t bytes = (size_t)vec->len * esz;
+    td_t h;
+    memcpy(&h, vec, 32);
+    h.mmod = 0;
+    h.order = 0;
+    atomic_store_explicit(&h.rc, 0, memory_order_relaxed);
+    h.attrs &= (uint8_t)~TD_ATTR_SLICE;
+    if (!(h.attrs & TD_ATTR_HAS_NULLS)) memset(h.nullmap, 0, 16);
+    const char* data = (vec->attrs & TD_ATTR_SLICE)
+        ? (const char*)td_data(vec->slice_parent) + (size_t)vec->slice_offset * esz
+        : (const char*)td_data(vec);
+    int fd = open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (fd < 0) return TD_ERR_IO;
+    int bad = write_all(fd, &h, 32) || (bytes && write_all(fd, data, bytes));
+    if (close(fd) != 0) bad = 1;
+    return bad ? TD_ERR_IO : TD_OK;
+}
+
+td_t* td_col_load(const char* path) {
+    if (!path) return TD_ERR_PTR(TD_ERR_IO);
+    int fd = open(path, O_RDONLY);
+    if (fd < 0) return TD_ERR_PTR(TD_ERR_IO);
+    struct stat sb;
+    td_t h;
+    if (fstat(fd, &sb) != 0 || sb.st_size < 32 || read_at(fd, &h, 32, 0)) { close(fd); return TD_ERR_PTR(TD_ERR_CORRUPT); }
+    if (!serializable(h.type)) { close(fd); return TD_ERR_PTR(TD_ERR_NYI); }
+    if (h.len < 0) { close(fd); return TD_ERR_PTR(TD_ERR_CORRUPT); }
+    if ((h.attrs & TD_ATTR_HAS_NULLS) && (h.attrs & TD_ATTR_NULLMAP_EXT)) { close(fd); return TD_ERR_PTR(TD_ERR_NYI); }
+    const size_t esz = td_sym_elem_size(h.type, h.attrs);
+    if (esz && (uint64_t)h.len > (SIZE_MAX - 32) / esz) { close(fd); return TD_ERR_PTR(TD_ERR_IO); }
+    const size_t bytes = (size_t)h.len * esz;
+    if ((uint64_t)sb.st_size < 32 + (uint64_t)bytes) { close(fd); return TD_ERR_PTR(TD_ERR_CORRUPT); }
+    td_t* v = td_alloc(bytes);
+    if (!v || TD_IS_ERR(v)) { close(fd); return v ? v : TD_ERR_PTR(TD_ERR_OOM); }
+    const uint8_t order = v->order;
+    if (bytes && read_big(fd, td_data(v), bytes, 32)) { close(fd); td_free(v); return TD_ERR_PTR(TD_ERR_IO); }
+    close(fd);
+    memcpy(v, &h, 32);                            /* the header as saved, then this block's own fields */
+    v->mmod = 0;
+    v->order = order;
+    v->attrs &= (uint8_t)~(TD_ATTR_SLICE | TD_ATTR_NULLMAP_EXT);
+    atomic_store_explicit(&v->rc, 1, memory_order_relaxed);
+    return v;
+}
+
+/* A column name usable as a file name (splay.c:79-85). */
+static int plain_name(const char* s, size_t n) {
+    return n && s[0] != '.' && !memchr(s, '/', n) && !memchr(s, '\\', n) && !memchr(s, '\0', n);
+}
+
+td_err_t td_sym_save(const char* path) {
+    if (!path) return TD_ERR_IO;
+    FILE* f = fopen(path, "wb");
+    if (!f) return TD_ERR_IO;
+    const uint32_t magic = TD_SYM_FILE_MAGIC;
+    const uint32_t count = td_sym_count();
+    int bad = fwrite(&magic, 4, 1, f) != 1 || fwrite(&count, 4, 1, f) != 1;
+    for (uint32_t i = 0; i < count && !bad; i++) {
+        td_t* s = td_sym_str((int64_t)i);
+        const uint32_t len = s ? (uint32_t)td_str_len(s) : 0;
+        bad = fwrite(&len, 4, 1, f) != 1 || (len && fwrite(td_str_ptr(s), 1, len, f) != len);
+    }
+    if (fclose(f) != 0) bad = 1;
+    return bad ? TD_ERR_IO : TD_OK;
+}
+
+td_err_t td_sym_load(const char* path) {
+    if (!path) return TD_ERR_IO;
+    FILE* f = fopen(path, "rb");
+    if (!f) return TD_ERR_IO;
+    uint32_t magic, count;
+    if (fread(&magic, 4, 1, f) != 1 || fread(&count, 4, 1, f) != 1 || magic != TD_SYM_FILE_MAGIC ||
+        count > 100000000u) {
+        fclose(f);
+        return TD_ERR_CORRUPT;
+    }
+    char* buf = NULL;
+    size_t cap = 0;
+    td_err_t err = TD_OK;
+    for (uint32_t i = 0; i < count && !err; i++) {
+        uint32_t len;
+        if (fread(&len, 4, 1, f) != 1 || len > (16u << 20)) { err = TD_ERR_CORRUPT; break; }
+        if (len > cap) {
+            char* nb = realloc(buf, len);
+            if (!nb) { err = TD_ERR_OOM; break; }
+            buf = nb;
+            cap = len;
+        }
+        if (len && fread(buf, 1, len, f) != len) { err = TD_ERR_CORRUPT; break; }
+        if (td_sym_intern(len ? buf : "", len) < 0) err = TD_ERR_OOM;
+    }
+    free(buf);
+    fclose(f);
+    return err;
+}
+
+td_err_t td_splay_save(td_t* tbl, const char* dir, const char* sym_path) {
+    if (!tbl || TD_IS_ERR(tbl) || tbl->type != TD_TABLE) return TD_ERR_TYPE;
+    if (!dir) return TD_ERR_IO;
+    if (sym_path) {
+        td_err_t e = td_sym_save(sym_path);
+        if (e != TD_OK) return e;
+    }
+    if (mkdir(dir, 0755) != 0 && errno != EEXIST) return TD_ERR_IO;
+    char path[1024];
+    td_t* schema = td_table_schema(tbl);
+    if (schema && !TD_IS_ERR(schema)) {
+        if (snprintf(path, sizeof(path), "%s/.d", dir) >= (int)sizeof(path)) return TD_ERR_RANGE;
+        td_err_t e = td_col_save(schema, path);
+        if (e != TD_OK) return e;
+    }
+    for (int64_t j = 0; j < td_table_ncols(tbl); j++) {
+        td_t* col = td_table_get_col_idx(tbl, j);
+        td_t* name = td_sym_str(td_table_col_name(tbl, j));
+        if (!col || !name) continue;
+        const char* s = td_str_ptr(name);
+        const size_t n = td_str_len(name);
+        if (!plain_name(s, n)) continue;
+        if (snprintf(path, sizeof(path), "%s/%.*s", dir, (int)n, s) >= (int)sizeof(path)) return TD_ERR_RANGE;
+        td_err_t e = td_col_save(col, path);
+        if (e != TD_OK) return e;
+    }
+    return TD_OK;
+}
+
+td_t* td_splay_load(const char* dir) {
+    if (!dir) return TD_ERR_PTR(TD_ERR_IO);
+    char path[1024];
+    if (snprintf(path, sizeof(path), "%s/.d", dir) >= (int)sizeof(path)) return TD_ERR_PTR(TD_ERR_RANGE);
+    td_t* schema = td_col_load(path);
+    if (!schema || TD_IS_ERR(schema)) return schema;
+    if (schema->type != TD_I64) { td_release(schema); return TD_ERR_PTR(TD_ERR_CORRUPT); }
+    const int64_t nc = schema->len;
+    const int64_t* ids = (const int64_t*)td_data(schema);
+    td_t* tbl = td_table_new(nc);
+    for (int64_t j = 0; j < nc && tbl && !TD_IS_ERR(tbl); j++) {
+        td_t* name = td_sym_str(ids[j]);
+        if (!name) continue;
+        const char* s = td_str_ptr(name);
+        const size_t n = td_str_len(name);
+        if (!plain_name(s, n)) continue;
+        if (snprintf(path, sizeof(path), "%s/%.*s", dir, (int)n, s) >= (int)sizeof(path)) {
+            td_release(tbl);
+            tbl = TD_ERR_PTR(TD_ERR_RANGE);
+            break;
+        }
+        td_t* col = td_col_load(path);
+        if (!col || TD_IS_ERR(col)) {
+            td_release(tbl);
+            tbl = col ? col : TD_ERR_PTR(TD_ERR_IO);
+            break;
+        }
+        td_t* t2 = td_table_add_col(tbl, ids[j], col);
+        td_release(col);
+        if (!t2 || TD_IS_ERR(t2)) { td_release(tbl); tbl = t2 ? t2 : TD_ERR_PTR(TD_ERR_OOM); break; }
+        tbl = t2;
+    }
+    td_release(schema);
+    return tbl ? tbl : TD_ERR_PTR(TD_ERR_OOM);
+}
+
+td_t* td_gpu_splay_load(const char* dir) {
+    td_t* tbl = td_splay_load(dir);
+    if (!tbl || TD_IS_ERR(tbl)) return tbl;
+    td_err_t e = td_gpu_pin(tbl);
+    if (e != TD_OK) {
+        td_release(tbl);
+        return TD_ERR_PTR(e);
+    }
+    return tbl;
+}

@@ -25,6 +25,13 @@ def gpu():
 
 
 @pytest.fixture(scope="session")
+def td():
+    """td.h binding of the product library for host-side calls (no GPU needed)."""
+    import teide_b200
+    return teide_b200.load()
+
+
+@pytest.fixture(scope="session")
 def ref():
     """td.h binding of Teide itself, compiled from its sources (checker)."""
     if not os.path.exists(REF_LIB):
