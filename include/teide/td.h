@@ -517,6 +517,10 @@ td_t*    td_splay_load(const char* dir);
 /* The symbol table file ("TSYM", count, then length-prefixed strings). */
 td_err_t td_sym_save(const char* path);
 td_err_t td_sym_load(const char* path);
+/* A partitioned database: every partition directory of db_root (a name of
+ * digits and dots, in name order) holds the splayed table `table_name`; the
+ * partitions' columns are concatenated (src/store/part.c). */
+td_t*    td_part_load(const char* db_root, const char* table_name);
 
 /* DAG construction */
 td_graph_t* td_graph_new(td_t* tbl);

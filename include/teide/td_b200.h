@@ -113,6 +113,8 @@ size_t       td_server_estimate(td_graph_t* g, td_op_t* root);
 /* td_splay_load, then every column made resident in HBM (td_gpu_pin): a
  * splayed table straight into device memory.  No counterpart in Teide. */
 td_t*        td_gpu_splay_load(const char* dir);
+/* td_part_load, then every column made resident in HBM.  No counterpart in Teide. */
+td_t*        td_gpu_part_load(const char* db_root, const char* table_name);
 
 #ifdef __cplusplus
 }

@@ -21,6 +21,7 @@
  * before the upload, so the data crosses PCIe at DMA speed.
  */
 #include "internal.h"
+#include <dirent.h>
 #include <errno.h>
 #include <pthread.h>
 #include <fcntl.h>
@@ -273,6 +274,136 @@ td_t* td_splay_load(const char* dir) {
 
 td_t* td_gpu_splay_load(const char* dir) {
     td_t* tbl = td_splay_load(dir);
+    if (!tbl || TD_IS_ERR(tbl)) return tbl;
+    td_err_t e = td_gpu_pin(tbl);
+    if (e != TD_OK) {
+        td_release(tbl);
+        return TD_ERR_PTR(e);
+    }
+    return tbl;
+}
+
+/* ---- partitioned databases (part.c:111-279) ------------------------------------
+ * db_root holds one directory per partition (a name of digits and dots, such as
+ * "2024.01.15"), each holding the splayed table `table_name`.  td_part_load
+ * loads the partitions in name order and concatenates every column: one
+ * allocation per column, each partition copied in once. */
+
+static int part_dir_name(const char* s) {
+    int dot = 0;
+    for (const char* c = s; *c; c++) {
+        if (*c == '.') { dot = 1; continue; }
+        if (*c < '0' || *c > '9') return 0;
+    }
+    return dot;
+}
+
+static int cmp_str(const void* a, const void* b) { return strcmp(*(char* const*)a, *(char* const*)b); }
+
+static td_t* concat_cols(td_t** parts, int64_t np) {
+    int64_t total = 0;
+    int same = 1;
+    for (int64_t p = 0; p < np; p++) {
+        if (parts[p]->type != parts[0]->type) return TD_ERR_PTR(TD_ERR_TYPE);
+        same = same && td_sym_elem_size(parts[p]->type, parts[p]->attrs) ==
+                       td_sym_elem_size(parts[0]->type, parts[0]->attrs);
+        total += parts[p]->len;
+    }
+    if (!same) {                                  /* SYM columns of different widths: widen pairwise */
+        td_t* acc = parts[0];
+        td_retain(acc);
+        for (int64_t p = 1; p < np; p++) {
+            td_t* n = td_vec_concat(acc, parts[p]);
+            td_release(acc);
+            if (!n || TD_IS_ERR(n)) return n ? n : TD_ERR_PTR(TD_ERR_OOM);
+            acc = n;
+        }
+        return acc;
+    }
+    const size_t esz = td_sym_elem_size(parts[0]->type, parts[0]->attrs);
+    td_t* v = td_alloc((size_t)total * esz);
+    if (!v || TD_IS_ERR(v)) return v ? v : TD_ERR_PTR(TD_ERR_OOM);
+    v->type = parts[0]->type;
+    v->attrs = parts[0]->attrs & (uint8_t)~(TD_ATTR_SLICE | TD_ATTR_NULLMAP_EXT | TD_ATTR_HAS_NULLS);
+    v->len = total;
+    char* dst = td_data(v);
+    for (int64_t p = 0; p < np; p++) {
+        const size_t b = (size_t)parts[p]->len * esz;
+        if (b) memcpy(dst, td_data(parts[p]), b);
+        dst += b;
+    }
+    return v;
+}
+
+td_t* td_part_load(const char* db_root, const char* table_name) {
+    if (!db_root || !table_name) return TD_ERR_PTR(TD_ERR_IO);
+    if (strchr(table_name, '/') || strchr(table_name, '\\') || strstr(table_name, "..") || table_name[0] == '.')
+        return TD_ERR_PTR(TD_ERR_IO);
+    DIR* d = opendir(db_root);
+    if (!d) return TD_ERR_PTR(TD_ERR_IO);
+    char** names = NULL;
+    int64_t np = 0, cap = 0;
+    struct dirent* e;
+    while ((e = readdir(d))) {
+        if (e->d_name[0] == '.' || !part_dir_name(e->d_name)) continue;
+        if (np == cap) {
+            cap = cap ? cap * 2 : 16;
+            char** nn = realloc(names, (size_t)cap * sizeof(char*));
+            if (!nn) break;
+            names = nn;
+        }
+        if (!(names[np] = strdup(e->d_name))) break;
+        np++;
+    }
+    closedir(d);
+    td_t* res = NULL;
+    td_t** tabs = np ? calloc((size_t)np, sizeof(td_t*)) : NULL;
+    if (!np) res = TD_ERR_PTR(TD_ERR_IO);
+    else if (!tabs) res = TD_ERR_PTR(TD_ERR_OOM);
+    else {
+        qsort(names, (size_t)np, sizeof(char*), cmp_str);
+        char path[1024];
+        for (int64_t p = 0; p < np && !res; p++) {
+            if (snprintf(path, sizeof(path), "%s/%s/%s", db_root, names[p], table_name) >= (int)sizeof(path)) {
+                res = TD_ERR_PTR(TD_ERR_IO);
+                break;
+            }
+            tabs[p] = td_splay_load(path);
+            if (!tabs[p] || TD_IS_ERR(tabs[p])) { tabs[p] = NULL; res = TD_ERR_PTR(TD_ERR_IO); }
+        }
+        if (!res && np == 1) { res = tabs[0]; tabs[0] = NULL; }
+        else if (!res) {
+            const int64_t nc = td_table_ncols(tabs[0]);
+            td_t** cols = malloc((size_t)np * sizeof(td_t*));
+            res = cols ? td_table_new(nc) : TD_ERR_PTR(TD_ERR_OOM);
+            for (int64_t c = 0; c < nc && res && !TD_IS_ERR(res); c++) {
+                int ok = 1;
+                for (int64_t p = 0; p < np; p++) {
+                    cols[p] = td_table_get_col_idx(tabs[p], c);
+                    if (!cols[p]) ok = 0;
+                }
+                if (!ok) continue;
+                td_t* v = concat_cols(cols, np);
+                if (!v || TD_IS_ERR(v)) { td_release(res); res = v ? v : TD_ERR_PTR(TD_ERR_OOM); break; }
+                td_t* t2 = td_table_add_col(res, td_table_col_name(tabs[0], c), v);
+                td_release(v);
+                if (!t2 || TD_IS_ERR(t2)) { td_release(res); res = t2 ? t2 : TD_ERR_PTR(TD_ERR_OOM); break; }
+                res = t2;
+            }
+            free(cols);
+        }
+    }
+    for (int64_t p = 0; p < np; p++) {
+        if (tabs && tabs[p]) td_release(tabs[p]);
+        free(names[p]);
+    }
+    free(tabs);
+    free(names);
+    return res ? res : TD_ERR_PTR(TD_ERR_OOM);
+}
+
+td_t* td_gpu_part_load(const char* db_root, const char* table_name) {
+    td_t* tbl = td_part_load(db_root, table_name);
     if (!tbl || TD_IS_ERR(tbl)) return tbl;
     td_err_t e = td_gpu_pin(tbl);
     if (e != TD_OK) {

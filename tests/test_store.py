@@ -102,3 +102,38 @@ def test_corrupt_files_are_refused(td, tmp_path):
     r = td.lib.td_col_load(str(p).encode())
     assert r is not None and r < 32                            # TD_ERR_PTR(corrupt)
     td.release(v)
+
+
+PARTS = {"2024.01.02": 700, "2023.12.31": 1300, "2024.01.01": 0, "2024.01.10": 55}
+
+
+def _write_db(lib, root, parts, seed=9):
+    r = np.random.default_rng(seed)
+    cols = {}
+    for name, n in parts.items():
+        d = {"k": r.integers(0, 40, n), "px": r.standard_normal(n), "q": r.integers(-9, 9, n).astype(np.int32)}
+        cols[name] = d
+        t = lib.table({"k": d["k"], "px": d["px"], "q": (d["q"], I32)})
+        os.makedirs(f"{root}/{name}", exist_ok=True)             # td_splay_save makes only the leaf
+        assert lib.lib.td_splay_save(t, f"{root}/{name}/trades".encode(), None) == 0
+        lib.release(t)
+    os.makedirs(f"{root}/notes", exist_ok=True)                  # not a partition name: skipped
+    return cols
+
+
+def test_partitioned_db_matches_reference(td, ref, tmp_path):
+    for p in ("ours", "theirs"):
+        os.makedirs(tmp_path / p)
+    want = _write_db(td, tmp_path / "ours", PARTS)
+    _write_db(ref, tmp_path / "theirs", PARTS)
+    r1 = td.check(td.lib.td_part_load(str(tmp_path / "ours").encode(), b"trades"), "part load")
+    r2 = ref.check(ref.lib.td_part_load(str(tmp_path / "theirs").encode(), b"trades"), "part load")
+    ours, theirs = td.table_dict(r1), ref.table_dict(r2)
+    td.release(r1)
+    ref.release(r2)
+    assert list(ours) == list(theirs) == ["k", "px", "q"]
+    order = sorted(PARTS)
+    for c in ours:
+        cat = np.concatenate([want[p][c] for p in order])
+        assert np.array_equal(ours[c], theirs[c]), c
+        assert np.array_equal(ours[c], cat), c

@@ -42,3 +42,32 @@ def test_splayed_table_loads_resident(gpu, tmp_path):
     finally:
         L.td_gpu_unpin(r)
         gpu.release(r)
+
+
+def test_partitioned_db_loads_resident(gpu, tmp_path):
+    L = gpu.lib
+    L.td_gpu_part_load.restype = C.c_void_p
+    L.td_gpu_part_load.argtypes = [C.c_char_p, C.c_char_p]
+    L.td_gpu_unpin.argtypes = [C.c_void_p]
+    parts = {}
+    for i, day in enumerate(["2024.03.01", "2024.03.02", "2024.03.03"]):
+        d = workloads.config1(n=300_000 + 1000 * i, seed=70 + i)
+        t = gpu.table(d)
+        (tmp_path / day).mkdir()
+        assert L.td_splay_save(t, str(tmp_path / day / "t").encode(), None) == 0
+        gpu.release(t)
+        parts[day] = d
+    r = gpu.check(L.td_gpu_part_load(str(tmp_path).encode(), b"t"), "td_gpu_part_load")
+    try:
+        got = readme_group(gpu, r, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+        s = St()
+        L.td_gpu_last_stats(C.byref(s))
+        assert s.h2d == 0
+        d = {k: np.concatenate([parts[p][k] for p in sorted(parts)]) for k in ("flag", "region", "amount")}
+        m = d["flag"] == 0
+        want = oracle.group({"region": d["region"][m]}, [(OP_SUM, "amount", d["amount"][m])])
+        assert np.array_equal(got["region"], want["region"])
+        assert np.allclose(got["amount_sum"], want["amount_sum"], rtol=1e-12)
+    finally:
+        L.td_gpu_unpin(r)
+        gpu.release(r)
