@@ -188,51 +188,70 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_apply(uint32_t* __restric
     }
 }
 
-// The stable scatter of one pass.  A tile's rows go 256 at a time; within a
-// round a row's place is the tile's running offset for its digit, plus the
-// rows of that digit in lower warps, plus its rank among its warp's lanes of
-// the same digit (match mask).
+// The stable scatter of one pass.  A tile's rows go 1024 at a time, as four
+// sub-rounds of 256 (row order = sub-round, then thread).  Every row's rank
+// among the lanes of its warp and sub-round with the same digit comes from a
+// warp match mask; after one barrier the thread that owns digit d turns the
+// per-(sub-round, warp) counts into running offsets from the tile's base for
+// d, and after a second every row writes at its offset plus its rank -- two
+// barriers per 1024 rows, and rows of equal digit keep their order.
+constexpr int kSortSub = 4;
+static_assert(kSortRounds % kSortSub == 0, "a tile is a whole number of 1024-row rounds");
+
 __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const uint64_t* __restrict__ kin,
                                                                 const int64_t* __restrict__ vin,
                                                                 uint64_t* __restrict__ kout, int64_t* __restrict__ vout,
                                                                 int64_t n, uint64_t kmin, int shift,
                                                                 const uint32_t* __restrict__ offs, int64_t n_tiles) {
     __shared__ uint32_t base[256];
-    __shared__ uint32_t wc[kSortWarps][256];
+    __shared__ uint8_t wc[kSortSub][kSortWarps][256];          // lanes of a warp per digit: at most 32
+    __shared__ uint32_t pre[kSortSub][kSortWarps][256];
     base[threadIdx.x] = offs[(int64_t)threadIdx.x * n_tiles + blockIdx.x];
-    for (int w = 0; w < kSortWarps; w++) wc[w][threadIdx.x] = 0;
+    for (int k = 0; k < kSortSub; k++)
+        for (int w = 0; w < kSortWarps; w++) wc[k][w][threadIdx.x] = 0;
     __syncthreads();
     const unsigned lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const unsigned lt = (1u << lane) - 1u;
     const int64_t t0 = blockIdx.x * kSortTile;
-    for (int q = 0; q < kSortRounds; q++) {
-        const int64_t i = t0 + (int64_t)q * kSortThreads + threadIdx.x;
-        const bool in = i < n;
-        uint64_t k = 0;
-        int64_t v = 0;
-        uint32_t d = 256;                          // rows past the end share a digit of their own
-        if (in) {
-            k = kin[i];
-            v = vin[i];
-            d = (uint32_t)(((k - kmin) >> shift) & 255);
+    for (int q = 0; q < kSortRounds; q += kSortSub) {
+        uint64_t k[kSortSub];
+        int64_t v[kSortSub];
+        uint32_t d[kSortSub], rank[kSortSub];
+#pragma unroll
+        for (int s = 0; s < kSortSub; s++) {
+            const int64_t i = t0 + (int64_t)(q + s) * kSortThreads + threadIdx.x;
+            const bool in = i < n;
+            k[s] = in ? kin[i] : 0;
+            v[s] = in ? vin[i] : 0;
+            d[s] = in ? (uint32_t)(((k[s] - kmin) >> shift) & 255) : 256u;
         }
-        const unsigned peers = __match_any_sync(0xffffffffu, d);
-        const uint32_t cnt = (uint32_t)__popc(peers), rank = (uint32_t)__popc(peers & lt);
-        const bool leader = (peers & lt) == 0;
-        if (in && leader) wc[warp][d] = cnt;
-        __syncthreads();
-        if (in) {
-            uint32_t pos = base[d] + rank;
-            for (unsigned w = 0; w < warp; w++) pos += wc[w][d];
-            kout[pos] = k;
-            vout[pos] = v;
+#pragma unroll
+        for (int s = 0; s < kSortSub; s++) {
+            const unsigned peers = __match_any_sync(0xffffffffu, d[s]);
+            rank[s] = (uint32_t)__popc(peers & lt);
+            if (d[s] < 256 && (peers & lt) == 0) wc[s][warp][d[s]] = (uint8_t)__popc(peers);
         }
         __syncthreads();
-        if (in && leader) {
-            atomicAdd(&base[d], cnt);
-            wc[warp][d] = 0;
+        {
+            const unsigned dg = threadIdx.x;                     // this thread's digit
+            uint32_t run = base[dg];
+            for (int s = 0; s < kSortSub; s++)
+                for (int w = 0; w < kSortWarps; w++) {
+                    const uint32_t c = wc[s][w][dg];
+                    pre[s][w][dg] = run;
+                    run += c;
+                    wc[s][w][dg] = 0;
+                }
+            base[dg] = run;
         }
         __syncthreads();
+#pragma unroll
+        for (int s = 0; s < kSortSub; s++) {
+            if (d[s] >= 256) continue;
+            const uint32_t pos = pre[s][warp][d[s]] + rank[s];
+            kout[pos] = k[s];
+            vout[pos] = v[s];
+        }
     }
 }
 
