@@ -276,6 +276,16 @@ static td_t* fetch_vec_q(ex_t* x, const void* dptr, int8_t type, uint8_t attrs, 
     return v;
 }
 
+/* A new host vector holding n elements of a result the kernels wrote into
+ * mapped host memory (read after the stream synchronized). */
+static td_t* host_vec(const void* hptr, int8_t type, uint8_t attrs, int64_t n) {
+    td_t* v = vec_like(type, attrs, n);
+    if (!v || TD_IS_ERR(v)) return v ? v : TD_ERR_PTR(TD_ERR_OOM);
+    const size_t bytes = (size_t)n * td_sym_elem_size(type, attrs);
+    if (bytes) memcpy(td_data(v), hptr, bytes);
+    return v;
+}
+
 static td_t* fetch_vec(ex_t* x, const void* dptr, int8_t type, uint8_t attrs, int64_t n) {
     return fetch_vec_q(x, dptr, type, attrs, n, 0);
 }
@@ -551,12 +561,24 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
     volatile int64_t* hng = tdb_host_scalar(&x->c, &dng);
     out.d_n_groups = hng ? dng : tdb_dev_alloc(&x->c, 8);
     if (!ws || !out.d_n_groups) return TD_ERR_PTR(TD_ERR_OOM);
+    /* a small result is emitted straight into mapped host memory: the host
+     * reads it once the group-by's synchronization returns, with no copy */
+    void* hout[TDG_MAX_KEYS + TDG_MAX_AGGS];
+    memset(hout, 0, sizeof(hout));
+    size_t obytes = 0;
+    for (int k = 0; k < nk; k++) obytes += 256 + (size_t)plan.max_groups * td_sym_elem_size(keys[k].type, keys[k].attrs);
+    obytes += (size_t)na * (256 + (size_t)plan.max_groups * 8);
+    const int mapped = !x->dev_only && obytes <= TDB_OUT_BYTES - x->c.out_used;
     for (int k = 0; k < nk; k++) {
-        out.keys[k] = tdb_dev_alloc(&x->c, (size_t)plan.max_groups * td_sym_elem_size(keys[k].type, keys[k].attrs));
+        const size_t b = (size_t)plan.max_groups * td_sym_elem_size(keys[k].type, keys[k].attrs);
+        if (mapped) hout[k] = tdb_host_out(&x->c, b ? b : 1, &out.keys[k]);
+        if (!hout[k]) out.keys[k] = tdb_dev_alloc(&x->c, b);
         if (!out.keys[k]) return TD_ERR_PTR(TD_ERR_OOM);
     }
     for (int a = 0; a < na; a++) {
-        out.aggs[a] = tdb_dev_alloc(&x->c, (size_t)plan.max_groups * 8);
+        const size_t b = (size_t)plan.max_groups * 8;
+        if (mapped) hout[nk + a] = tdb_host_out(&x->c, b ? b : 1, &out.aggs[a]);
+        if (!hout[nk + a]) out.aggs[a] = tdb_dev_alloc(&x->c, b);
         if (!out.aggs[a]) return TD_ERR_PTR(TD_ERR_OOM);
     }
     if ((st = tdb_check_cancel())) return TD_ERR_PTR(st);
@@ -582,7 +604,8 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
     memset(wide, 0, sizeof(wide));
     td_t* err = NULL;
     for (int k = 0; k < nk && !err; k++) {
-        cols[k] = fetch_vec_q(x, out.keys[k], keys[k].type, keys[k].attrs, ng, 2);
+        cols[k] = hout[k] ? host_vec(hout[k], keys[k].type, keys[k].attrs, ng)
+                          : fetch_vec_q(x, out.keys[k], keys[k].type, keys[k].attrs, ng, 2);
         if (TD_IS_ERR(cols[k])) { err = cols[k]; cols[k] = NULL; }
     }
     for (int a = 0; a < na && !err; a++) {
@@ -595,11 +618,12 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
         td_t* v;
         if (td_sym_elem_size(ot, ins[a].attrs) == 8 || op == OP_AVG || op == OP_COUNT || op == OP_SUM) {
             int8_t vt = (ot == TD_F64 || op == OP_AVG) ? TD_F64 : (td_sym_elem_size(ot, ins[a].attrs) == 8 ? ot : TD_I64);
-            v = fetch_vec_q(x, out.aggs[a], vt, vt == TD_SYM ? ins[a].attrs : 0, ng, 2);
+            v = hout[nk + a] ? host_vec(hout[nk + a], vt, vt == TD_SYM ? ins[a].attrs : 0, ng)
+                             : fetch_vec_q(x, out.aggs[a], vt, vt == TD_SYM ? ins[a].attrs : 0, ng, 2);
             if (!TD_IS_ERR(v)) cols[nk + a] = v;
         } else {
             /* MIN/MAX of a narrow integer column: int64 results, narrowed below */
-            v = fetch_vec_q(x, out.aggs[a], TD_I64, 0, ng, 1);
+            v = hout[nk + a] ? host_vec(hout[nk + a], TD_I64, 0, ng) : fetch_vec_q(x, out.aggs[a], TD_I64, 0, ng, 1);
             if (!TD_IS_ERR(v)) wide[a] = v;
         }
         if (TD_IS_ERR(v)) err = v;

@@ -462,6 +462,25 @@ volatile int64_t* tdb_host_scalar(tdb_ctx* c, void** dev) {
     return tls_scalar_h + i;
 }
 
+static _Thread_local char* tls_out_h;
+static _Thread_local char* tls_out_d;
+
+void* tdb_host_out(tdb_ctx* c, size_t bytes, void** dev) {
+    if (!tls_out_h) {
+        void* h = NULL;
+        void* d = NULL;
+        if (cudaHostAlloc(&h, TDB_OUT_BYTES, cudaHostAllocMapped) != cudaSuccess) { cudaGetLastError(); return NULL; }
+        if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) { cudaGetLastError(); cudaFreeHost(h); return NULL; }
+        tls_out_h = h;
+        tls_out_d = d;
+    }
+    const size_t off = (c->out_used + 255) & ~(size_t)255;
+    if (off + bytes > TDB_OUT_BYTES) return NULL;
+    c->out_used = off + bytes;
+    *dev = tls_out_d + off;
+    return tls_out_h + off;
+}
+
 /* Per-thread page-locked staging for small device->host copies: a copy into
  * pageable memory is synchronous in CUDA, so queued copies land here and are
  * moved to their destinations when the call synchronizes. */

@@ -69,6 +69,7 @@ typedef struct tdb_ctx {
     struct { void* host; void* stage; size_t bytes; } pending[TDB_PENDING];
     int      n_pending;
     size_t   stage_used;
+    size_t   out_used;          /* mapped result area handed out in this call (tdb_host_out) */
 } tdb_ctx;
 
 int      tdb_gpu_ensure(void);                 /* 0 ok, else td_err_t */
@@ -83,6 +84,11 @@ int      tdb_ctx_sync(tdb_ctx* c);               /* 0 ok, else td_err_t */
  * returned device pointer (*dev): once the stream has synchronized, the host
  * reads it with no copy.  Valid until the end of the call; NULL if none left. */
 volatile int64_t* tdb_host_scalar(tdb_ctx* c, void** dev);
+/* Page-locked, device-mapped host memory for small results (TDB_OUT_BYTES per
+ * thread, handed out per call): kernels write it directly, so the host reads
+ * it after the stream synchronizes with no copy.  NULL when it does not fit. */
+#define TDB_OUT_BYTES ((size_t)1 << 20)
+void*    tdb_host_out(tdb_ctx* c, size_t bytes, void** dev);
 /* 1 when `p` lies in page-locked memory (a copy to it can be asynchronous). */
 int      tdb_host_is_pinned(const void* p);
 /* Device->host copy queued on the call's stream; tdb_ctx_sync completes it. */
