@@ -257,12 +257,15 @@ tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_plan* jplan
 /* ---- sort ------------------------------------------------------------------------
  * tdg_sort_perm: the stable permutation that orders n rows by keys[0..n_keys)
  * (keys[0] most significant).  Replaces exec_sort (exec.c:3370-3862) for
- * Teide's radix key types: I64, TIMESTAMP, I32, DATE, TIME, F64 and SYM.
+ * the key types I64, TIMESTAMP, I32, DATE, TIME, F64, SYM, BOOL, U8 and I16.
  * Each key is encoded as radix_encode_fn does (exec.c:2739-2840): DESC
  * complements the code (equal keys keep their row order), F64 follows IEEE
- * order with -0.0 before +0.0 and NaN first or last by nulls_first, and SYM
- * sorts by sym_rank[id], a device array holding the rank of each intern id's
- * string (build_enum_rank, exec.c:2876-2975).  perm receives n int64 row
+ * order with NaN first or last by nulls_first, and SYM sorts by
+ * sym_rank[id], a device array holding the rank of each intern id's string
+ * (build_enum_rank, exec.c:2876-2975); BOOL / U8 compare unsigned and I16
+ * signed (sort_cmp, exec.c:2503-2558).  -0.0 sorts before +0.0 where Teide
+ * radix-sorts (one key of a radix type, more than 64 rows) and equals it
+ * elsewhere, as in Teide's comparator sort.  perm receives n int64 row
  * indices; ws is tdg_sort_ws_bytes(n) device bytes.  The stream is
  * synchronized once per key (the key's range sets how many digits to sort).
  * Other key types return TD_ERR_NYI.

@@ -224,12 +224,14 @@ def canonical(d: dict, by=None) -> dict:
     return {k: np.asarray(v)[order] for k, v in d.items()}
 
 
-def sort_code(values, desc=False, nulls_first=None, kind=None):
+def sort_code(values, desc=False, nulls_first=None, kind=None, zero_eq=False):
     """The u64 code radix_encode_fn (exec.c:2739-2840) gives each value:
-    integers flip the sign bit (I32 / DATE / TIME at 32 bits), F64 maps to
-    IEEE order (-0.0 before +0.0) with NaN smallest or largest by nulls_first
-    (default: DESC), strings (SYM) to the rank of their bytes among the
-    distinct strings, and DESC complements the code."""
+    integers flip the sign bit (I32 / DATE / TIME at 32 bits, I16 at 16),
+    BOOL / U8 keep their unsigned byte (sort_cmp, exec.c:2538-2547), F64 maps
+    to IEEE order (-0.0 before +0.0, or equal to it with zero_eq, as in
+    sort_cmp) with NaN smallest or largest by nulls_first (default: DESC),
+    strings (SYM) to the rank of their bytes among the distinct strings, and
+    DESC complements the code."""
     nf = desc if nulls_first is None else nulls_first
     v = np.asarray(values)
     if kind == "sym" or v.dtype.kind in ("O", "U", "S"):
@@ -237,7 +239,13 @@ def sort_code(values, desc=False, nulls_first=None, kind=None):
         uniq = sorted(set(b))
         rank = {x: i for i, x in enumerate(uniq)}
         e = np.array([rank[x] for x in b], dtype=np.uint64)
+    elif v.dtype == np.bool_ or v.dtype == np.uint8:
+        e = v.astype(np.uint64)
+    elif v.dtype == np.int16:
+        e = (v.view(np.uint16) ^ np.uint16(0x8000)).astype(np.uint64)
     elif v.dtype == np.float64:
+        if zero_eq:
+            v = np.where(v == 0.0, 0.0, v)   # -0.0 -> +0.0; NaN and the rest unchanged
         bits = v.view(np.uint64)
         mask = (np.uint64(0) - (bits >> np.uint64(63))) | np.uint64(1 << 63)
         e = bits ^ mask
@@ -254,9 +262,13 @@ def sort_code(values, desc=False, nulls_first=None, kind=None):
 def sort(cols: dict, keys, limit=None) -> dict:
     """Rows of `cols` ordered by keys [(name, desc, nulls_first)] (stable,
     first key most significant), cut to the first `limit` rows when given.
-    A SYM key column is passed as its strings."""
+    A SYM key column is passed as its strings.  Teide radix-sorts (exec.c:
+    3426-3453) one key of a radix type over more than 64 rows; otherwise its
+    comparator decides, where -0.0 equals +0.0 (zero_eq)."""
     n = len(next(iter(cols.values()))) if cols else 0
-    codes = [sort_code(cols[name], desc, nf) for name, desc, nf in keys]
+    small = {np.dtype(np.bool_), np.dtype(np.uint8), np.dtype(np.int16)}
+    zero_eq = n <= 64 or len(keys) > 1 or any(np.asarray(cols[k[0]]).dtype in small for k in keys)
+    codes = [sort_code(cols[name], desc, nf, zero_eq=zero_eq) for name, desc, nf in keys]
     order = np.lexsort(codes[::-1]) if codes else np.arange(n)
     if limit is not None:
         order = order[:limit]

@@ -29,10 +29,19 @@ constexpr int kSortWarps = kSortThreads / 32;
 // integers flip the sign bit, F64 flips every bit of negatives and the sign
 // of the rest (IEEE order, -0.0 before +0.0), NaN is the smallest or largest
 // key by nulls_first, SYM reads the rank of its string, DESC complements.
-__device__ __forceinline__ uint64_t sort_encode(const tdg_sort_key& K, int64_t r) {
+// BOOL / U8 sort as unsigned bytes and I16 as signed (sort_cmp, exec.c:
+// 2538-2547).  zero_eq encodes -0.0 as +0.0: the comparator Teide sorts
+// with outside its radix path (sort_cmp, exec.c:2512-2521) finds them equal.
+__device__ __forceinline__ uint64_t sort_encode(const tdg_sort_key& K, int64_t r, bool zero_eq) {
     const tdg_col& c = K.col;
     uint64_t e;
     switch (c.type) {
+        case T_BOOL: case T_U8:
+            e = ((const uint8_t*)c.data)[r];
+            break;
+        case T_I16:
+            e = (uint64_t)((uint16_t)((const short*)c.data)[r] ^ 0x8000u);
+            break;
         case T_I64: case T_TIMESTAMP:
             e = (uint64_t)((const long long*)c.data)[r] ^ (1ULL << 63);
             break;
@@ -40,7 +49,8 @@ __device__ __forceinline__ uint64_t sort_encode(const tdg_sort_key& K, int64_t r
             e = (uint64_t)((uint32_t)((const int*)c.data)[r] ^ (1u << 31));
             break;
         case T_F64: {
-            const uint64_t b = (uint64_t)__double_as_longlong(((const double*)c.data)[r]);
+            uint64_t b = (uint64_t)__double_as_longlong(((const double*)c.data)[r]);
+            if (zero_eq && b == (1ULL << 63)) b = 0;
             if ((b & 0x7FF0000000000000ULL) == 0x7FF0000000000000ULL && (b & 0x000FFFFFFFFFFFFFULL)) {
                 const uint64_t nan_e = (K.nulls_first ^ K.desc) ? 0ULL : ~0ULL;
                 return K.desc ? ~nan_e : nan_e;
@@ -68,10 +78,10 @@ __device__ __forceinline__ uint64_t sort_encode(const tdg_sort_key& K, int64_t r
 // keys[i] = encoded key of row perm[i]; folds the min and max into mm[0..1].
 __global__ void __launch_bounds__(kThreads) k_sort_encode(const tdg_sort_key K, const int64_t* __restrict__ perm,
                                                           int64_t n, uint64_t* __restrict__ keys,
-                                                          unsigned long long* mm) {
+                                                          unsigned long long* mm, bool zero_eq) {
     unsigned long long lo = ~0ULL, hi = 0ULL;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const uint64_t e = sort_encode(K, perm[i]);
+        const uint64_t e = sort_encode(K, perm[i], zero_eq);
         keys[i] = e;
         lo = e < lo ? e : lo;
         hi = e > hi ? e : hi;
@@ -263,7 +273,8 @@ __global__ void k_gather(const T* __restrict__ in, const int64_t* __restrict__ p
 
 static bool sortable(const tdg_sort_key& k) {
     switch (k.col.type) {
-        case T_I64: case T_TIMESTAMP: case T_I32: case T_DATE: case T_TIME: case T_F64: return true;
+        case T_I64: case T_TIMESTAMP: case T_I32: case T_DATE: case T_TIME: case T_F64:
+        case T_BOOL: case T_U8: case T_I16: return true;
         case T_SYM: return k.sym_rank != nullptr;
         default: return false;
     }
@@ -332,6 +343,17 @@ extern "C" tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, in
     (note_launch(), k_sort_iota<<<g, kThreads, 0, s>>>(W.va, n));
     int64_t* cur = W.va;
     int64_t* alt = W.vb;
+    // Teide radix-sorts one key of a radix type over more than 64 rows
+    // (exec.c:3426-3453); every other case goes through sort_cmp, where
+    // -0.0 equals +0.0.  Several keys of radix types pack into one composite
+    // only when their ranges fit 64 bits, which a key holding both zeros
+    // (a 64-bit range) never does, so treating the zeros as equal there is
+    // the composite's order as well.
+    bool zero_eq = n <= 64 || n_keys > 1;
+    for (int k = 0; k < n_keys; k++) {
+        const int t = keys[k].col.type;
+        if (t == T_BOOL || t == T_U8 || t == T_I16) zero_eq = true;
+    }
     unsigned long long* mmh = pinned_pair();
     unsigned long long mm_local[2];
     tdg_status st = E_OK;
@@ -339,7 +361,7 @@ extern "C" tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, in
     for (int k = n_keys - 1; k >= 0 && !st; k--) {
         (note_launch(), k_sort_mm_init<<<1, 1, 0, s>>>(W.mm));
         const int ge = grid_for((const void*)k_sort_encode, kThreads, 0, n);
-        (note_launch(), k_sort_encode<<<ge, kThreads, 0, s>>>(keys[k], cur, n, W.ka, W.mm));
+        (note_launch(), k_sort_encode<<<ge, kThreads, 0, s>>>(keys[k], cur, n, W.ka, W.mm, zero_eq));
         unsigned long long* mm = mmh ? mmh : mm_local;
         if (cudaMemcpyAsync(mm, W.mm, 16, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
             cudaStreamSynchronize(s) != cudaSuccess) { st = launch_status(); if (!st) st = E_IO; break; }

@@ -824,18 +824,34 @@ static td_t* reduce(ex_t* x, uint16_t opc, val_t* v) {
     void* ws = tdb_dev_alloc(&x->c, plan.ws_bytes);
     tdg_group_out out;
     memset(&out, 0, sizeof(out));
-    out.d_n_groups = tdb_dev_alloc(&x->c, 8);
-    out.aggs[0] = tdb_dev_alloc(&x->c, 8 * (size_t)plan.max_groups);
-    out.aggs[1] = tdb_dev_alloc(&x->c, 8 * (size_t)plan.max_groups);
+    /* the count and both aggregates land in mapped host memory when it has room */
+    const size_t ab = 8 * (size_t)plan.max_groups;
+    int64_t* h[3] = {0, 0, 0};
+    void* dng = NULL;
+    h[0] = tdb_host_out(&x->c, 8, &dng);
+    out.d_n_groups = dng;
+    if (h[0]) h[1] = tdb_host_out(&x->c, ab, &out.aggs[0]);
+    if (h[1]) h[2] = tdb_host_out(&x->c, ab, &out.aggs[1]);
+    if (!h[2]) {
+        h[0] = h[1] = NULL;
+        out.d_n_groups = tdb_dev_alloc(&x->c, 8);
+        out.aggs[0] = tdb_dev_alloc(&x->c, ab);
+        out.aggs[1] = tdb_dev_alloc(&x->c, ab);
+    }
     if (!ws || !out.d_n_groups || !out.aggs[0] || !out.aggs[1]) return TD_ERR_PTR(TD_ERR_OOM);
     st = CALL(tdg_group_run(&d, v->has_pred ? &v->pred : NULL, v->dsel, &plan, ws, &out, x->c.stream));
     if (st) return TD_ERR_PTR(st);
     int64_t ng = 0;
     uint64_t val = 0;
     int64_t cnt = 0;
-    st = tdb_d2h(&x->c, &ng, out.d_n_groups, 8);
-    if (!st && ng > 0) st = tdb_d2h(&x->c, &val, out.aggs[0], 8);
-    if (!st && ng > 0) st = tdb_d2h(&x->c, &cnt, out.aggs[1], 8);
+    if (h[2]) {   /* tdg_group_run synchronized its stream */
+        ng = h[0][0];
+        if (ng > 0) { memcpy(&val, h[1], 8); cnt = h[2][0]; }
+    } else {
+        st = tdb_d2h(&x->c, &ng, out.d_n_groups, 8);
+        if (!st && ng > 0) st = tdb_d2h(&x->c, &val, out.aggs[0], 8);
+        if (!st && ng > 0) st = tdb_d2h(&x->c, &cnt, out.aggs[1], 8);
+    }
     if (st) return TD_ERR_PTR(st);
     int isf = dc.type == TD_F64;
     double f; int64_t i;
@@ -997,12 +1013,31 @@ static td_t* exec_sort_node(ex_t* x, td_op_t* sop, int64_t limit) {
     const int64_t n_out = limit >= 0 && limit < n ? limit : n;
     const int nk = ext->sort.n_cols;
     tdg_sort_key keys[TDG_MAX_SORT_KEYS];
+    td_t* kexpr[TDG_MAX_SORT_KEYS];
+    memset(kexpr, 0, sizeof(kexpr));
     td_t* res = NULL;
     int st = 0;
     for (int k = 0; k < nk && !st; k++) {
         td_op_ext_t* ke = tdb_find_ext(g, ext->sort.columns[k]->id);
-        if (!ke || ke->base.opcode != OP_SCAN) { st = TD_ERR_NYI; break; }
-        td_t* col = td_table_get_col(tbl, ke->sym);
+        td_t* col;
+        if (ke && ke->base.opcode == OP_SCAN) {
+            col = td_table_get_col(tbl, ke->sym);
+        } else {
+            /* a key expression is evaluated over the sort's input table, as
+             * exec_sort does (exec.c:3393-3401) */
+            td_t* saved = g->table;
+            g->table = tbl;
+            val_t kv;
+            td_t* r = exec_value(x, ext->sort.columns[k], &kv);
+            g->table = saved;
+            if (TD_IS_ERR(r)) { st = TD_ERR_CODE(r); break; }
+            col = materialize(x, &kv);
+            vfree(&kv);
+            if (TD_IS_ERR(col)) { st = TD_ERR_CODE(col); break; }
+            kexpr[k] = col;
+            if (col->type <= 0 || col->type == TD_TABLE) { st = TD_ERR_NYI; break; }
+            if (col->len != n) { st = TD_ERR_LENGTH; break; }
+        }
         if (!col) { st = TD_ERR_SCHEMA; break; }
         tdb_devcol d;
         st = tdb_col_device(&x->c, col, 0, &d);
@@ -1043,6 +1078,7 @@ static td_t* exec_sort_node(ex_t* x, td_op_t* sop, int64_t limit) {
     }
     int st2 = tdb_ctx_sync(&x->c);                 /* the queued copies land before anything is returned or freed */
     if (!st) st = st2;
+    for (int k = 0; k < nk; k++) if (kexpr[k]) td_release(kexpr[k]);
     td_release(tbl);
     if (st) {
         if (res) td_release(res);

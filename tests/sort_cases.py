@@ -7,7 +7,7 @@ the oracle's answer in the same form."""
 import numpy as np
 
 import oracle
-from teide_b200.td import I32, OP_SUM
+from teide_b200.td import BOOL, I16, I32, OP_SUM, U8
 
 ROWS = 3000
 
@@ -157,7 +157,79 @@ def sort_of_group(td, seed=8, n=20_000):
         td.release(t)
 
 
-ALL = [i64_ties, f64_desc_nan_zero, f64_asc_nan_first, i32_key, two_keys, sym_key, head_of_sort, sort_of_group]
+def small_int_keys(td, seed=9, n=ROWS):
+    """BOOL ascending, I16 descending, U8 ascending (Teide's comparator sort:
+    unsigned bytes, signed 16-bit), with F64 ±0.0 carried along."""
+    r = np.random.default_rng(seed)
+    d = {"b": r.integers(0, 2, n).astype(np.bool_), "h": r.integers(-300, 300, n).astype(np.int16),
+         "u": r.integers(0, 256, n).astype(np.uint8), "f": np.where(r.integers(0, 2, n) == 1, -0.0, 0.0),
+         "i": np.arange(n)}
+    t = td.table({"b": (d["b"], BOOL), "h": (d["h"], I16), "u": (d["u"], U8), "f": d["f"], "i": d["i"]})
+    try:
+        keys = [("b", False, None), ("h", True, None), ("u", False, None)]
+        return _bits(_run(td, t, keys)), _bits(oracle.sort(d, keys))
+    finally:
+        td.release(t)
+
+
+def f64_zeros_two_keys(td, seed=10, n=ROWS):
+    """F64 key holding -0.0 and +0.0, then an I64 key: the zeros compare
+    equal (the composite does not fit 64 bits, Teide's comparator decides)."""
+    r = np.random.default_rng(seed)
+    f = np.round(r.standard_normal(n), 0)
+    f[r.integers(0, n, 600)] = -0.0
+    f[r.integers(0, n, 600)] = 0.0
+    d = {"f": f, "k": r.integers(0, 5, n), "i": np.arange(n)}
+    t = td.table(d)
+    try:
+        keys = [("f", True, None), ("k", False, None)]
+        return _bits(_run(td, t, keys)), _bits(oracle.sort(d, keys))
+    finally:
+        td.release(t)
+
+
+def f64_zeros_small(td, seed=11, n=50):
+    """At most 64 rows Teide sorts by insertion with its comparator: -0.0
+    equals +0.0, NaN last."""
+    r = np.random.default_rng(seed)
+    f = np.where(r.integers(0, 2, n) == 1, -0.0, 0.0)
+    f[r.integers(0, n, 10)] = r.standard_normal(10)
+    f[r.integers(0, n, 3)] = np.nan
+    d = {"f": f, "i": np.arange(n)}
+    t = td.table(d)
+    try:
+        keys = [("f", False, None)]
+        return _bits(_run(td, t, keys)), _bits(oracle.sort(d, keys))
+    finally:
+        td.release(t)
+
+
+def expr_keys(td, seed=12, n=ROWS):
+    """Key expressions, evaluated over the input table: a*b DESC, then
+    f + 1.0; the result holds the table's own columns."""
+    r = np.random.default_rng(seed)
+    d = {"a": r.integers(-50, 50, n), "b": r.integers(0, 10, n), "f": np.round(r.standard_normal(n), 1),
+         "i": np.arange(n)}
+    t = td.table(d)
+    try:
+        g = td.graph(t)
+        try:
+            k0 = g.op("mul", g.scan("a"), g.scan("b"))
+            k1 = g.op("add", g.scan("f"), g.f64(1.0))
+            res = g.execute(g.sort(g.const_table(t), [k0, k1], [1, 0]), optimize=False)
+        finally:
+            g.free()
+        got = td.table_dict(res)
+        td.release(res)
+        full = dict(d, _k0=d["a"] * d["b"], _k1=d["f"] + 1.0)
+        want = oracle.sort(full, [("_k0", True, None), ("_k1", False, None)])
+        return _bits(got), _bits({k: want[k] for k in d})
+    finally:
+        td.release(t)
+
+
+ALL = [i64_ties, f64_desc_nan_zero, f64_asc_nan_first, i32_key, two_keys, sym_key, head_of_sort, sort_of_group,
+       small_int_keys, f64_zeros_two_keys, f64_zeros_small, expr_keys]
 
 
 def same(got, want):

@@ -6,6 +6,7 @@ import pytest
 
 import oracle
 import sort_cases
+from teide_b200.td import I16, U8
 
 pytestmark = pytest.mark.gpu
 
@@ -14,6 +15,21 @@ pytestmark = pytest.mark.gpu
 def test_sort_matches_oracle(gpu, case):
     got, want = case(gpu)
     sort_cases.same(got, want)
+
+
+def test_small_int_and_zero_keys_many_tiles(gpu):
+    """I16 DESC, U8, then F64 with both zeros (equal under several keys) over
+    300K rows: many radix tiles, 16- and 8-bit digit counts."""
+    n = 300_001
+    r = np.random.default_rng(31)
+    d = {"h": r.integers(-2**15, 2**15, n).astype(np.int16), "u": r.integers(0, 256, n).astype(np.uint8),
+         "f": np.where(r.integers(0, 2, n) == 1, -0.0, 0.0), "i": np.arange(n)}
+    t = gpu.table({"h": (d["h"], I16), "u": (d["u"], U8), "f": d["f"], "i": d["i"]})
+    try:
+        keys = [("h", True, None), ("u", False, None), ("f", False, None)]
+        sort_cases.same(sort_cases._bits(sort_cases._run(gpu, t, keys)), sort_cases._bits(oracle.sort(d, keys)))
+    finally:
+        gpu.release(t)
 
 
 @pytest.mark.parametrize("n", [0, 1, 63, 4097, 1_000_003])
