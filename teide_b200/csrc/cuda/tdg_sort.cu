@@ -76,7 +76,7 @@ __device__ __forceinline__ uint64_t sort_encode(const tdg_sort_key& K, int64_t r
 }
 
 // keys[i] = encoded key of row perm[i]; folds the min and max into mm[0..1].
-__global__ void __launch_bounds__(kThreads) k_sort_encode(const tdg_sort_key K, const int64_t* __restrict__ perm,
+__global__ void __launch_bounds__(kThreads) k_sort_encode(const tdg_sort_key K, const uint32_t* __restrict__ perm,
                                                           int64_t n, uint64_t* __restrict__ keys,
                                                           unsigned long long* mm, bool zero_eq) {
     unsigned long long lo = ~0ULL, hi = 0ULL;
@@ -98,9 +98,16 @@ __global__ void __launch_bounds__(kThreads) k_sort_encode(const tdg_sort_key K, 
     }
 }
 
-__global__ void k_sort_iota(int64_t* __restrict__ perm, int64_t n) {
+// Row indices travel through the passes as 32 bits (n < 2^32); the result
+// is widened to int64 once at the end.
+__global__ void k_sort_iota(uint32_t* __restrict__ perm, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        perm[i] = i;
+        perm[i] = (uint32_t)i;
+}
+
+__global__ void k_sort_widen(const uint32_t* __restrict__ in, int64_t n, int64_t* __restrict__ perm) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        perm[i] = in[i];
 }
 
 __global__ void k_sort_mm_init(unsigned long long* mm) { mm[0] = ~0ULL; mm[1] = 0ULL; }
@@ -209,8 +216,8 @@ constexpr int kSortSub = 4;
 static_assert(kSortRounds % kSortSub == 0, "a tile is a whole number of 1024-row rounds");
 
 __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const uint64_t* __restrict__ kin,
-                                                                const int64_t* __restrict__ vin,
-                                                                uint64_t* __restrict__ kout, int64_t* __restrict__ vout,
+                                                                const uint32_t* __restrict__ vin,
+                                                                uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                                 int64_t n, uint64_t kmin, int shift,
                                                                 const uint32_t* __restrict__ offs, int64_t n_tiles) {
     __shared__ uint32_t base[256];
@@ -225,7 +232,7 @@ __global__ void __launch_bounds__(kSortThreads) k_sort_scatter(const uint64_t* _
     const int64_t t0 = blockIdx.x * kSortTile;
     for (int q = 0; q < kSortRounds; q += kSortSub) {
         uint64_t k[kSortSub];
-        int64_t v[kSortSub];
+        uint32_t v[kSortSub];
         uint32_t d[kSortSub], rank[kSortSub];
 #pragma unroll
         for (int s = 0; s < kSortSub; s++) {
@@ -283,8 +290,8 @@ static bool sortable(const tdg_sort_key& k) {
 struct SortWs {
     uint64_t* ka;
     uint64_t* kb;
-    int64_t* va;
-    int64_t* vb;
+    uint32_t* va;
+    uint32_t* vb;
     uint32_t* hist;
     uint32_t* sums;
     unsigned long long* mm;
@@ -309,8 +316,8 @@ static SortWs sort_ws(void* ws, int64_t n) {
     const int64_t n_tiles = (n + kSortTile - 1) / kSortTile;
     W.ka = (uint64_t*)p; p += kb;
     W.kb = (uint64_t*)p; p += kb;
-    W.va = (int64_t*)p; p += kb;
-    W.vb = (int64_t*)p; p += kb;
+    W.va = (uint32_t*)p; p += kb;
+    W.vb = (uint32_t*)p; p += kb;
     W.hist = (uint32_t*)p; p += al256((size_t)n_tiles * 256 * 4);
     W.sums = (uint32_t*)p; p += al256((size_t)scan_blocks(n_tiles) * 4);
     W.mm = (unsigned long long*)p;
@@ -341,8 +348,8 @@ extern "C" tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, in
     const int64_t n_tiles = (n + kSortTile - 1) / kSortTile;
     const int g = grid_for((const void*)k_sort_iota, kThreads, 0, n);
     (note_launch(), k_sort_iota<<<g, kThreads, 0, s>>>(W.va, n));
-    int64_t* cur = W.va;
-    int64_t* alt = W.vb;
+    uint32_t* cur = W.va;
+    uint32_t* alt = W.vb;
     // Teide radix-sorts one key of a radix type over more than 64 rows
     // (exec.c:3426-3453); every other case goes through sort_cmp, where
     // -0.0 equals +0.0.  Several keys of radix types pack into one composite
@@ -379,11 +386,11 @@ extern "C" tdg_status tdg_sort_perm(const tdg_sort_key* keys, int32_t n_keys, in
             (note_launch(), k_sort_scatter<<<(unsigned)n_tiles, kSortThreads, 0, s>>>(kc, cur, kd, alt, n, kmin, shift,
                                                                                      W.hist, n_tiles));
             uint64_t* tk = kc; kc = kd; kd = tk;
-            int64_t* tv = cur; cur = alt; alt = tv;
+            uint32_t* tv = cur; cur = alt; alt = tv;
         }
         st = launch_status();
     }
-    if (!st && cudaMemcpyAsync(perm, cur, (size_t)n * 8, cudaMemcpyDeviceToDevice, s) != cudaSuccess) st = E_IO;
+    if (!st) (note_launch(), k_sort_widen<<<g, kThreads, 0, s>>>(cur, n, perm));
     if (!st) st = launch_status();
     tm.stop(s);
     if (tm.on) {
