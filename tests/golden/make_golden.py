@@ -1,7 +1,8 @@
 """Generate tests/golden/*.npz by running Teide itself (oracle/_ref/libteide_ref.so,
 compiled from the reference's sources by oracle/Makefile) on small seeded
 inputs of each workload shape.  Each fixture stores the inputs and Teide's
-output, rows sorted by key (group-by) or by every column (join).
+output, rows sorted by key (group-by) or by every column (join); the sort
+fixture keeps Teide's row order, which is the thing under test.
 
     make -C oracle && python tests/golden/make_golden.py
 
@@ -20,7 +21,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 
 from teide_b200 import workloads  # noqa: E402
-from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM, Td  # noqa: E402
+from teide_b200.td import BOOL, I16, OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM, U8, Td  # noqa: E402
 import oracle  # noqa: E402
 
 
@@ -60,6 +61,43 @@ def ref_filter_join_group(td, build, probe, pred, lkey, rkey, keys, aggs, jt=0):
     for x in (r, jr, b, p):
         td.release(x)
     return oracle.canonical(out, by=keys), oracle.canonical(joined)
+
+
+# sort fixtures: name -> (columns, Teide type tags, keys [(column, desc, nulls_first or -1)])
+def sort_inputs():
+    r = np.random.default_rng(105)
+    n = 3000
+    a = {"k": r.integers(0, 50, n), "i": np.arange(n), "v": r.standard_normal(n)}
+    f = np.round(r.standard_normal(2000), 1)
+    f[r.integers(0, 2000, 40)] = np.nan
+    f[r.integers(0, 2000, 40)] = -0.0
+    f[r.integers(0, 2000, 40)] = 0.0
+    b = {"f": f, "i": np.arange(2000)}
+    g = np.round(r.standard_normal(n), 0)
+    g[r.integers(0, n, 600)] = -0.0
+    g[r.integers(0, n, 600)] = 0.0
+    c = {"f": g, "k": r.integers(0, 5, n), "i": np.arange(n)}
+    d = {"b": r.integers(0, 2, n).astype(np.uint8), "h": r.integers(-300, 300, n).astype(np.int16),
+         "u": r.integers(0, 256, n).astype(np.uint8), "i": np.arange(n)}
+    return {
+        "a": (a, {}, [("k", 0, -1)]),                                  # one I64 key, ties keep row order
+        "b": (b, {}, [("f", 1, -1)]),                                  # F64 DESC: NaN first, -0.0 / +0.0 apart
+        "c": (c, {}, [("f", 0, 1), ("k", 1, -1)]),                     # two keys: zeros equal, NaN-free
+        "d": (d, {"b": BOOL, "h": I16, "u": U8}, [("b", 0, -1), ("h", 1, -1), ("u", 0, -1)]),
+    }
+
+
+def ref_sort(td, cols, tags, keys):
+    t = td.table({k: ((v, tags[k]) if k in tags else v) for k, v in cols.items()})
+    g = td.graph(t)
+    nf = None if all(k[2] < 0 for k in keys) else [int(k[1] if k[2] < 0 else k[2]) for k in keys]
+    r = g.execute(g.sort(g.const_table(t), [g.scan(k[0]) for k in keys], [int(k[1]) for k in keys], nf),
+                  optimize=False)
+    g.free()
+    out = td.table_dict(r)
+    td.release(r)
+    td.release(t)
+    return out
 
 
 def save(name, **arrays):
@@ -103,6 +141,14 @@ def main():
             td.release(x)
     save("join_outer_small", **{"l_" + k: v for k, v in left.items()},
          **{"r_" + k: v for k, v in right.items()}, **res)
+
+    arrays = {}
+    for name, (cols, tags, keys) in sort_inputs().items():
+        out = ref_sort(td, cols, tags, keys)
+        arrays.update({f"{name}_in_{k}": v for k, v in cols.items()})
+        arrays.update({f"{name}_out_{k}": v for k, v in out.items()})
+        arrays[f"{name}_keys"] = np.array([f"{k}:{d}:{nf}" for k, d, nf in keys])
+    save("sort_small", **arrays)
 
 
 if __name__ == "__main__":

@@ -82,6 +82,27 @@ def test_oracle_outer_join_golden(jt):
         assert np.array_equal(got[k], want[k]), k
 
 
+@pytest.mark.parametrize("case", ["a", "b", "c", "d"])
+def test_oracle_sort_golden(case):
+    """Teide's row order for a sort: I64 ties, F64 DESC with NaN and signed
+    zeros (radix path), two keys with signed zeros (comparator), BOOL / I16 /
+    U8 keys.  Bit-exact, F64 compared as bit patterns."""
+    z = load("sort_small")
+    cols = pick(z, case + "_in_")
+    keys = []
+    for spec in z[case + "_keys"]:
+        name, desc, nf = str(spec).split(":")
+        keys.append((name, bool(int(desc)), None if int(nf) < 0 else bool(int(nf))))
+    got = oracle.sort(cols, keys)
+    want = pick(z, case + "_out_")
+    assert list(got) == list(want)
+    for k in want:
+        g, w = np.asarray(got[k]), np.asarray(want[k])
+        if w.dtype == np.float64:
+            g, w = g.view(np.uint64), w.view(np.uint64)
+        assert np.array_equal(g.astype(w.dtype), w), (case, k)
+
+
 def test_oracle_known_answers():
     id1 = np.array([1, 1, 2, 2, 3, 3, 1, 2, 3, 1])
     v1 = np.array([10, 20, 30, 40, 50, 60, 70, 80, 90, 100])
