@@ -6,7 +6,7 @@ import pytest
 
 import oracle
 import sort_cases
-from teide_b200.td import I16, U8
+from teide_b200.td import BOOL, I16, U8
 
 pytestmark = pytest.mark.gpu
 
@@ -15,6 +15,28 @@ pytestmark = pytest.mark.gpu
 def test_sort_matches_oracle(gpu, case):
     got, want = case(gpu)
     sort_cases.same(got, want)
+
+
+@pytest.mark.parametrize("case", ["a", "b", "c", "d"])
+def test_sort_golden(gpu, case):
+    """Teide's own row order (tests/golden/sort_small.npz, made by running
+    Teide) reproduced through td_sort_op on the device, bit for bit."""
+    import os
+    with np.load(os.path.join(os.path.dirname(__file__), "golden", "sort_small.npz")) as z:
+        zz = {k: z[k] for k in z.files}
+    cols = {k[len(case) + 4:]: v for k, v in zz.items() if k.startswith(case + "_in_")}
+    want = {k[len(case) + 5:]: v for k, v in zz.items() if k.startswith(case + "_out_")}
+    keys = []
+    for spec in zz[case + "_keys"]:
+        name, desc, nf = str(spec).split(":")
+        keys.append((name, bool(int(desc)), None if int(nf) < 0 else bool(int(nf))))
+    tags = {"b": BOOL, "h": I16, "u": U8} if case == "d" else {}
+    t = gpu.table({k: ((v, tags[k]) if k in tags else v) for k, v in cols.items()})
+    try:
+        got = sort_cases._run(gpu, t, keys)
+    finally:
+        gpu.release(t)
+    sort_cases.same(sort_cases._bits(got), sort_cases._bits(want))
 
 
 def test_small_int_and_zero_keys_many_tiles(gpu):
