@@ -13,8 +13,10 @@
 // key range (max - min of the encoded keys) sets the number of passes.
 //
 // One pass over n keys: a per-tile digit histogram, a prefix over
-// (digit, tile) in three coalesced steps, and a stable scatter in which every tile ranks its rows 256
-// at a time with warp match masks, so rows of equal digit keep their order.
+// (digit, tile) in three coalesced steps, and a stable scatter in which every
+// tile ranks its rows 1024 at a time (four 256-row sub-rounds, warp match
+// masks), so rows of equal digit keep their order.  Keys move as 64 bits and
+// row indices as 32 bits (n < 2^32); the permutation is widened to int64 last.
 #include "tdg_common.cuh"
 #include <string.h>
 
