@@ -364,10 +364,13 @@ void tdb_trace(const char* what) {
     }
 }
 
+static void tls_register(void);
+
 int tdb_ctx_begin(tdb_ctx* c) {
     memset(c, 0, sizeof(*c));
     int st = tdb_gpu_ensure();
     if (st) return st;
+    tls_register();
     if (!tls_stream) {
         cudaStream_t s;
         if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) { cudaGetLastError(); return TD_ERR_IO; }
@@ -486,6 +489,41 @@ void* tdb_host_out(tdb_ctx* c, size_t bytes, void** dev) {
  * moved to their destinations when the call synchronizes. */
 #define TDB_STAGE_BYTES ((size_t)16 << 20)
 static _Thread_local char* tls_stage;
+
+/* A thread that ran queries (a serve worker, a caller's thread) releases its
+ * stream and page-locked buffers when it exits; every call on it has
+ * synchronized by then. */
+static pthread_key_t tls_key;
+static pthread_once_t tls_once = PTHREAD_ONCE_INIT;
+static int tls_key_ok;                  /* the key exists (set once, under pthread_once) */
+static _Thread_local int tls_keyed;     /* this thread's release is registered */
+
+static void tls_release(void* unused) {
+    (void)unused;
+    if (tls_stream) {
+        cudaStreamSynchronize((cudaStream_t)tls_stream);
+        cudaStreamDestroy((cudaStream_t)tls_stream);
+        tls_stream = NULL;
+    }
+    if (tls_stage) { cudaFreeHost(tls_stage); tls_stage = NULL; }
+    if (tls_out_h) { cudaFreeHost(tls_out_h); tls_out_h = tls_out_d = NULL; }
+    if (tls_scalar_h) { cudaFreeHost(tls_scalar_h); tls_scalar_h = NULL; tls_scalar_d = NULL; }
+    free(tls_tm);
+    tls_tm = NULL;
+    tls_ntm = tls_captm = 0;
+    cudaGetLastError();
+}
+
+static void tls_make_key(void) {
+    tls_key_ok = pthread_key_create(&tls_key, tls_release) == 0;
+}
+
+static void tls_register(void) {
+    if (tls_keyed) return;
+    pthread_once(&tls_once, tls_make_key);
+    tls_keyed = 1;                      /* one attempt per thread */
+    if (tls_key_ok) pthread_setspecific(tls_key, (void*)1);
+}
 
 int tdb_d2h_async(tdb_ctx* c, void* host, const void* dev, size_t bytes) {
     if (!bytes) return TD_OK;
