@@ -115,20 +115,20 @@ class Clocks:
 def make_tables(td, workload, rank, device, scale=1.0):
     from teide_b200 import workloads
     if workload == "join_group":
-        b, p = workloads.config3(n_probe=int(100_000_000 * scale), seed=3 + 1000 * rank, device=device)
+        b, p = workloads.join_tables(n_probe=int(100_000_000 * scale), seed=3 + 1000 * rank, device=device)
         bt, pt = td.table(b), td.table(p)
         return {"build": bt, "probe": pt}, len(p["fk"]), 16 * len(b["pk"]) + 24 * len(p["fk"]), 24 * len(p["fk"])
     if workload in ("group_radix", "group_sort"):
-        c = workloads.config2(n=int(200_000_000 * scale), seed=2 + 1000 * rank, device=device)
+        c = workloads.zipf_group_table(n=int(200_000_000 * scale), seed=2 + 1000 * rank, device=device)
         t = td.table(c)
         return {"t": t}, len(c["key"]), 24 * len(c["key"]), 24 * len(c["key"])
-    c = workloads.config1(n=int(10_000_000 * scale), seed=1 + 1000 * rank)
+    c = workloads.readme_table(n=int(10_000_000 * scale), seed=1 + 1000 * rank)
     t = td.table(c)
     return {"t": t}, len(c["flag"]), 24 * len(c["flag"]), 24 * len(c["flag"])
 
 
 def splay_main(args, td, L, rank, world, local, barrier, max_over_ranks):
-    """A splayed table on local disk (the cfg 2 columns: key, v1, v2 at 50M
+    """A splayed table on local disk (the Zipf group-by columns: key, v1, v2 at 50M
     rows, 1.2 GB) read into HBM by td_gpu_splay_load each step: the column
     files come from the page cache into page-locked blocks and are copied to
     the device.  value = column bytes resident per second, whole job."""
@@ -139,7 +139,7 @@ def splay_main(args, td, L, rank, world, local, barrier, max_over_ranks):
     L.td_gpu_splay_load.restype = C.c_void_p
     L.td_gpu_splay_load.argtypes = [C.c_char_p]
     n = int(50_000_000 * args.scale)
-    c = workloads.config2(n=n, seed=2 + 1000 * rank, device="cuda")
+    c = workloads.zipf_group_table(n=n, seed=2 + 1000 * rank, device="cuda")
     bytes_ = sum(v.nbytes for v in c.values())
     t = td.table(c)
     del c
@@ -254,7 +254,7 @@ class Batch:
         from teide_b200 import workloads
         from teide_b200.td import F64, I64, OP_COUNT, OP_MAX, OP_SUM
         self.td = td
-        rows, ks = workloads.config4_shapes(n_queries=n_queries, seed=seed)
+        rows, ks = workloads.batch_shapes(n_queries=n_queries, seed=seed)
         if first:
             rows, ks = rows[:first], ks[:first]
         self.rows = int(rows.sum())
@@ -410,8 +410,8 @@ def serve_main(args, td, L, rank, world, local, barrier, max_over_ranks):
     from teide_b200 import serve, workloads
     scale = args.scale
     n_group, n_probe = int(200_000_000 * scale), int(100_000_000 * scale)
-    c2 = workloads.config2(n=n_group, seed=2 + 1000 * rank, device="cuda")
-    b, p = workloads.config3(n_probe=n_probe, seed=3 + 1000 * rank, device="cuda")
+    c2 = workloads.zipf_group_table(n=n_group, seed=2 + 1000 * rank, device="cuda")
+    b, p = workloads.join_tables(n_probe=n_probe, seed=3 + 1000 * rank, device="cuda")
     tg, tb, tp = td.table(c2), td.table(b), td.table(p)
     del c2, b, p
     torch.cuda.empty_cache()
@@ -420,7 +420,7 @@ def serve_main(args, td, L, rank, world, local, barrier, max_over_ranks):
         if st:
             raise RuntimeError(f"td_gpu_pin failed: {st}")
     n_req = args.requests
-    raw = workloads.config5_requests(n_req, rate=2000.0, seed=5 + rank, group_rows=n_group, probe_rows=n_probe,
+    raw = workloads.serve_requests(n_req, rate=2000.0, seed=5 + rank, group_rows=n_group, probe_rows=n_probe,
                                      len_range=(100_000, max(100_000, int(50_000_000 * scale))))
     reqs = [serve.Request(*r) for r in raw]
     serve.build(td, reqs, tg, tb, tp)
@@ -496,9 +496,9 @@ def serve_reference(td):
     from gpu_pipelines import const
     from teide_b200 import serve as sv
     from teide_b200 import workloads
-    c2 = workloads.config2(n=SERVE_REF_ROWS, seed=32)
-    b, p = workloads.config3(n_build=10_000_000, n_probe=SERVE_REF_ROWS, seed=33)
-    raw = workloads.config5_requests(SERVE_REF_REQUESTS, seed=55, group_rows=SERVE_REF_ROWS,
+    c2 = workloads.zipf_group_table(n=SERVE_REF_ROWS, seed=32)
+    b, p = workloads.join_tables(n_build=10_000_000, n_probe=SERVE_REF_ROWS, seed=33)
+    raw = workloads.serve_requests(SERVE_REF_REQUESTS, seed=55, group_rows=SERVE_REF_ROWS,
                                      probe_rows=SERVE_REF_ROWS)
     bt = td.table(b)
 
@@ -550,7 +550,7 @@ def reference_sample(workload, scale_rows):
         desc = (f"the first {b.n} of the 4096 queries ({b.rows / 1e6:.1f}M rows), one td_execute each")
         return td, b.plain, desc
     if workload == "join_group":
-        b, p = workloads.config3(n_build=10_000_000, n_probe=scale_rows, seed=33)
+        b, p = workloads.join_tables(n_build=10_000_000, n_probe=scale_rows, seed=33)
         bt, pt = td.table(b), td.table(p)
 
         def q():
@@ -558,7 +558,7 @@ def reference_sample(workload, scale_rows):
                             [(OP_SUM, "price"), (OP_COUNT, "price")])
         desc = f"build 10M rows + probe {scale_rows / 1e6:g}M rows per query (probe side sampled from 100M)"
     elif workload == "group_radix":
-        c = workloads.config2(n=scale_rows, seed=32)
+        c = workloads.zipf_group_table(n=scale_rows, seed=32)
         t = td.table(c)
 
         def q():
@@ -566,7 +566,7 @@ def reference_sample(workload, scale_rows):
                             [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")])
         desc = f"{scale_rows / 1e6:g}M of 200M rows per query"
     elif workload == "group_sort":
-        c = workloads.config2(n=scale_rows, seed=32)
+        c = workloads.zipf_group_table(n=scale_rows, seed=32)
         t = td.table(c)
 
         def q():
@@ -575,7 +575,7 @@ def reference_sample(workload, scale_rows):
                                    "v1_sum", desc=True)
         desc = f"{scale_rows / 1e6:g}M of 200M rows per query, group result sorted by v1_sum DESC"
     else:
-        c = workloads.config1(n=scale_rows, seed=31)
+        c = workloads.readme_table(n=scale_rows, seed=31)
         t = td.table(c)
 
         def q():
@@ -585,7 +585,7 @@ def reference_sample(workload, scale_rows):
 
 
 def reference_splay(args):
-    """Teide's td_splay_load of a 50M-row splayed table (cfg 2 columns) into host memory."""
+    """Teide's td_splay_load of a 50M-row splayed table (the Zipf group-by columns) into host memory."""
     import ctypes as C
     import shutil
     import tempfile
@@ -594,7 +594,7 @@ def reference_splay(args):
     td = Td(REF_LIB)
     td.lib.td_splay_load.restype = C.c_void_p
     n = int(50_000_000 * args.scale)
-    c = workloads.config2(n=n, seed=2)
+    c = workloads.zipf_group_table(n=n, seed=2)
     bytes_ = sum(v.nbytes for v in c.values())
     t = td.table(c)
     del c

@@ -27,7 +27,7 @@ def _zipf_cdf(n=ZIPF_N, s=ZIPF_S):
     return c / c[-1]
 
 
-def config1(n=10_000_000, seed=1):
+def readme_table(n=10_000_000, seed=1):
     """README pipeline: flag U{0..3}, region U[0,64), amount U[0,1000)."""
     r = np.random.default_rng(seed)
     return {
@@ -37,7 +37,7 @@ def config1(n=10_000_000, seed=1):
     }
 
 
-def config2(n=200_000_000, seed=2, device=None, nkeys=ZIPF_N):
+def zipf_group_table(n=200_000_000, seed=2, device=None, nkeys=ZIPF_N):
     """Radix group-by: key Zipf(1.1) over `nkeys` values, v1 U[-1e6,1e6],
     v2 N(0,1)."""
     if device is not None:
@@ -70,7 +70,7 @@ def config2(n=200_000_000, seed=2, device=None, nkeys=ZIPF_N):
     }
 
 
-def config3(n_build=10_000_000, n_probe=100_000_000, seed=3, device=None):
+def join_tables(n_build=10_000_000, n_probe=100_000_000, seed=3, device=None):
     """Filter -> join -> group: build pk = permutation of [0,n_build),
     cat U[0,1000); probe fk U[0, 1.2 n_build), qty U[1,100], price U[1,500)."""
     fk_hi = int(round(n_build * 1.2))
@@ -104,7 +104,7 @@ def config3(n_build=10_000_000, n_probe=100_000_000, seed=3, device=None):
     return build, probe
 
 
-def config4_shapes(n_queries=4096, seed=4, rows=(1_000, 2_000_000), groups=(16, 65_536)):
+def batch_shapes(n_queries=4096, seed=4, rows=(1_000, 2_000_000), groups=(16, 65_536)):
     """Per-query (rows, K): both log-uniform."""
     r = np.random.default_rng(seed)
     lr = r.uniform(math.log(rows[0]), math.log(rows[1]), n_queries)
@@ -112,13 +112,13 @@ def config4_shapes(n_queries=4096, seed=4, rows=(1_000, 2_000_000), groups=(16, 
     return np.exp(lr).astype(np.int64), np.exp(lk).astype(np.int64)
 
 
-def config4_query(rows, k, seed):
+def batch_query(rows, k, seed):
     """One batched query's table: key U[0,K), val U[0,1)."""
     r = np.random.default_rng(seed)
     return {"key": r.integers(0, k, rows, dtype=np.int64), "val": r.random(rows)}
 
 
-def config5_requests(n, rate=2000.0, seed=5, group_rows=200_000_000, probe_rows=100_000_000,
+def serve_requests(n, rate=2000.0, seed=5, group_rows=200_000_000, probe_rows=100_000_000,
                      join_frac=0.3, len_range=(100_000, 50_000_000)):
     """The served mix: n requests with Poisson arrivals at `rate` per second.
     70% filter + group-by over the group table (v1 > t, t ~ U[-1e6, 1e6]),

@@ -109,19 +109,19 @@ def save(name, **arrays):
 def main():
     td = Td(os.path.join(ROOT, "oracle", "_ref", "libteide_ref.so"))
 
-    c1 = workloads.config1(n=20_000, seed=101)
+    c1 = workloads.readme_table(n=20_000, seed=101)
     out = ref_filter_group(td, c1, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
-    save("config1_small", **{"in_" + k: v for k, v in c1.items()}, **{"out_" + k: v for k, v in out.items()})
+    save("readme_small", **{"in_" + k: v for k, v in c1.items()}, **{"out_" + k: v for k, v in out.items()})
 
-    c2 = workloads.config2(n=30_000, seed=102, nkeys=1 << 12)
+    c2 = workloads.zipf_group_table(n=30_000, seed=102, nkeys=1 << 12)
     aggs = [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")]
     out = ref_filter_group(td, c2, ("v1", "gt", 0), ["key"], aggs)
-    save("config2_small", **{"in_" + k: v for k, v in c2.items()}, **{"out_" + k: v for k, v in out.items()})
+    save("zipf_group_small", **{"in_" + k: v for k, v in c2.items()}, **{"out_" + k: v for k, v in out.items()})
 
-    b3, p3 = workloads.config3(n_build=5_000, n_probe=30_000, seed=103)
+    b3, p3 = workloads.join_tables(n_build=5_000, n_probe=30_000, seed=103)
     out, joined = ref_filter_join_group(td, b3, p3, ("qty", "gt", 10), "fk", "pk", ["cat"],
                                         [(OP_SUM, "price"), (OP_COUNT, "price")])
-    save("config3_small", **{"b_" + k: v for k, v in b3.items()}, **{"p_" + k: v for k, v in p3.items()},
+    save("join_group_small", **{"b_" + k: v for k, v in b3.items()}, **{"p_" + k: v for k, v in p3.items()},
          **{"out_" + k: v for k, v in out.items()}, **{"join_" + k: v for k, v in joined.items()})
 
     # outer joins with duplicates on both sides

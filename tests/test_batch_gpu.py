@@ -1,4 +1,5 @@
-"""td_execute_batch: many group-by graphs in one launch (BASELINE config 4 shape).
+"""td_execute_batch: many group-by graphs in one launch (the batched-query shape:
+thousands of small SUM/COUNT/MAX-by-key queries over resident tables).
 
 Each query's rows in the packed result must equal the oracle's group-by of
 that query's table (keys, COUNT exact; SUM/MAX of F64 within 1e-12), and a
@@ -44,8 +45,8 @@ def run_batch(td, tables, ops=(OP_SUM, OP_COUNT, OP_MAX)):
 def test_batch_matches_oracle_per_query(gpu, tmp_path, monkeypatch):
     monkeypatch.setenv("TD_TUNE_CACHE", str(tmp_path / "tune.json"))
     # 300 queries: the batch runs as 4 chunks whose results are copied while later chunks compute
-    rows, ks = workloads.config4_shapes(n_queries=300, seed=41, rows=(1, 200_000), groups=(1, 70_000))
-    datas = [workloads.config4_query(int(r), int(k), seed=1000 + i) for i, (r, k) in enumerate(zip(rows, ks))]
+    rows, ks = workloads.batch_shapes(n_queries=300, seed=41, rows=(1, 200_000), groups=(1, 70_000))
+    datas = [workloads.batch_query(int(r), int(k), seed=1000 + i) for i, (r, k) in enumerate(zip(rows, ks))]
     tables = [gpu.table(d) for d in datas]
     L = _bind(gpu)
     for t in tables:

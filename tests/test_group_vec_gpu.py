@@ -136,7 +136,7 @@ def test_partitioned_shapes(gpu, preds, aggs, n, lo, span):
 def test_partitioned_zipf_keys(gpu):
     """Skewed keys: the hot cache takes the head, the partitions the tail."""
     from teide_b200 import workloads
-    c = workloads.config2(n=2_000_000, seed=95, nkeys=1 << 16)
+    c = workloads.zipf_group_table(n=2_000_000, seed=95, nkeys=1 << 16)
     d = {"region": c["key"], "qty": c["v1"], "amount": c["v2"], "flag": (c["v1"] & 3)}
     t = gpu.table(d)
     try:

@@ -37,7 +37,7 @@ def _check(got, want):
 
 def _zipf_table(n, bits, seed):
     from teide_b200 import workloads
-    c = workloads.config2(n=n, seed=seed, nkeys=1 << bits)
+    c = workloads.zipf_group_table(n=n, seed=seed, nkeys=1 << bits)
     return c
 
 

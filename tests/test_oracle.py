@@ -41,16 +41,16 @@ def assert_group_equal(got, want, keys, ftol=1e-12):
             assert np.array_equal(g, w), k
 
 
-def test_oracle_config1_golden():
-    z = load("config1_small")
+def test_oracle_readme_golden():
+    z = load("readme_small")
     cin = pick(z, "in_")
     m = oracle.conj(cin, [("flag", "eq", 0)])
     got = oracle.group({"region": cin["region"]}, [(OP_SUM, "amount", cin["amount"])], m)
     assert_group_equal(got, pick(z, "out_"), ["region"])
 
 
-def test_oracle_config2_golden():
-    z = load("config2_small")
+def test_oracle_zipf_group_golden():
+    z = load("zipf_group_small")
     c = pick(z, "in_")
     m = oracle.conj(c, [("v1", "gt", 0)])
     got = oracle.group({"key": c["key"]}, [(OP_COUNT, "v1", None), (OP_SUM, "v1", c["v1"]),
@@ -59,8 +59,8 @@ def test_oracle_config2_golden():
     assert_group_equal(got, pick(z, "out_"), ["key"])
 
 
-def test_oracle_config3_golden():
-    z = load("config3_small")
+def test_oracle_join_group_golden():
+    z = load("join_group_small")
     b, p = pick(z, "b_"), pick(z, "p_")
     m = oracle.conj(p, [("qty", "gt", 10)])
     j = oracle.join(p, b, ["fk"], ["pk"], 0, m)
@@ -138,7 +138,7 @@ def _ref_group(ref, cols, pred, keys, aggs):
 
 @pytest.mark.parametrize("seed", [7, 8])
 def test_oracle_vs_reference_filter_group(ref, seed):
-    c = workloads.config2(n=60_000, seed=seed, nkeys=1 << 14)
+    c = workloads.zipf_group_table(n=60_000, seed=seed, nkeys=1 << 14)
     aggs = [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")]
     want = _ref_group(ref, c, ("v1", "gt", 0), ["key"], aggs)
     m = oracle.conj(c, [("v1", "gt", 0)])
@@ -150,7 +150,7 @@ def test_oracle_vs_reference_filter_join_group(ref):
     import sys
     sys.path.insert(0, GOLD)
     from make_golden import ref_filter_join_group
-    b, p = workloads.config3(n_build=20_000, n_probe=80_000, seed=9)
+    b, p = workloads.join_tables(n_build=20_000, n_probe=80_000, seed=9)
     want, joined = ref_filter_join_group(ref, b, p, ("qty", "gt", 10), "fk", "pk", ["cat"],
                                          [(OP_SUM, "price"), (OP_COUNT, "price")])
     m = oracle.conj(p, [("qty", "gt", 10)])

@@ -60,8 +60,8 @@ def oracle_c2(c, mask):
 # ---- golden fixtures (Teide's own outputs) -------------------------------------------
 
 @pytest.mark.parametrize("form", ["readme", "two_graph"])
-def test_config1_golden(gpu, form):
-    z = load("config1_small")
+def test_readme_golden(gpu, form):
+    z = load("readme_small")
     c = pick(z, "in_")
     t = gpu.table(c)
     fn = readme_group if form == "readme" else two_graph_group
@@ -72,8 +72,8 @@ def test_config1_golden(gpu, form):
 
 
 @pytest.mark.parametrize("form", ["readme", "two_graph"])
-def test_config2_golden(gpu, form):
-    z = load("config2_small")
+def test_zipf_group_golden(gpu, form):
+    z = load("zipf_group_small")
     c = pick(z, "in_")
     t = gpu.table(c)
     fn = readme_group if form == "readme" else two_graph_group
@@ -86,8 +86,8 @@ def test_config2_golden(gpu, form):
 
 
 @pytest.mark.parametrize("form", ["fused", "two_call"])
-def test_config3_golden(gpu, form):
-    z = load("config3_small")
+def test_join_group_golden(gpu, form):
+    z = load("join_group_small")
     b, p = pick(z, "b_"), pick(z, "p_")
     bt, pt = gpu.table(b), gpu.table(p)
     aggs = [(OP_SUM, "price"), (OP_COUNT, "price")]
@@ -128,8 +128,8 @@ def test_outer_join_golden(gpu, jt):
 
 @pytest.mark.parametrize("n,nkeys,seed", [(1, 16, 1), (1000, 1 << 10, 2), (250_000, 1 << 16, 3),
                                           (2_000_000, 1 << 24, 4)])
-def test_config2_shapes_vs_oracle(gpu, n, nkeys, seed):
-    c = workloads.config2(n=n, seed=seed, nkeys=nkeys)
+def test_zipf_group_shapes_vs_oracle(gpu, n, nkeys, seed):
+    c = workloads.zipf_group_table(n=n, seed=seed, nkeys=nkeys)
     t = gpu.table(c)
     got = readme_group(gpu, t, ("v1", "gt", 0), ["key"], C2_AGGS)
     gpu.release(t)
@@ -179,8 +179,8 @@ def test_multi_key_group(gpu):
     check_group(got, want, ["a", "b"])
 
 
-def test_config1_full_size(gpu):
-    c = workloads.config1(n=10_000_000, seed=21)
+def test_readme_full_size(gpu):
+    c = workloads.readme_table(n=10_000_000, seed=21)
     t = gpu.table(c)
     got = readme_group(gpu, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
     gpu.release(t)
@@ -189,8 +189,8 @@ def test_config1_full_size(gpu):
     check_group(got, want, ["region"], abs_sums_of({"region": c["region"]}, c["amount"], m, "amount", "_sum"))
 
 
-def test_config3_medium_vs_oracle(gpu):
-    b, p = workloads.config3(n_build=1_000_000, n_probe=10_000_000, seed=22)
+def test_join_group_medium_vs_oracle(gpu):
+    b, p = workloads.join_tables(n_build=1_000_000, n_probe=10_000_000, seed=22)
     bt, pt = gpu.table(b), gpu.table(p)
     aggs = [(OP_SUM, "price"), (OP_COUNT, "price")]
     got = fused_join_group(gpu, bt, pt, ("qty", "gt", 10), "fk", "pk", ["cat"], aggs)
@@ -219,9 +219,9 @@ def test_fused_outer_join_group(gpu, jt):
     check_group(got, want, ["id"])
 
 
-def test_config3_full_size_properties(gpu):
+def test_join_group_full_size_properties(gpu):
     """100M-row probe: totals match (every fk < 10M has exactly one partner)."""
-    b, p = workloads.config3(seed=23)
+    b, p = workloads.join_tables(seed=23)
     bt, pt = gpu.table(b), gpu.table(p)
     got = fused_join_group(gpu, bt, pt, ("qty", "gt", 10), "fk", "pk", ["cat"],
                            [(OP_SUM, "price"), (OP_COUNT, "price")])
@@ -234,8 +234,8 @@ def test_config3_full_size_properties(gpu):
     assert np.array_equal(np.sort(got["cat"]), np.arange(1000))
 
 
-def test_config2_full_size_properties(gpu):
-    c = workloads.config2(n=200_000_000, seed=24, device="cuda")
+def test_zipf_group_full_size_properties(gpu):
+    c = workloads.zipf_group_table(n=200_000_000, seed=24, device="cuda")
     t = gpu.table(c)
     got = readme_group(gpu, t, ("v1", "gt", 0), ["key"], C2_AGGS)
     gpu.release(t)

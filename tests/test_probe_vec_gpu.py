@@ -61,7 +61,7 @@ CASES = [
 @pytest.mark.parametrize("preds,aggs", CASES)
 @pytest.mark.parametrize("n_probe", [300_001, 300_000])
 def test_vector_probe_shapes(gpu, preds, aggs, n_probe):
-    b, p = workloads.config3(n_build=50_000, n_probe=n_probe, seed=81)
+    b, p = workloads.join_tables(n_build=50_000, n_probe=n_probe, seed=81)
     bt, pt = gpu.table(b), gpu.table(p)
     try:
         _same(_run(gpu, bt, pt, preds, aggs), _want(b, p, preds, aggs))
@@ -71,7 +71,7 @@ def test_vector_probe_shapes(gpu, preds, aggs, n_probe):
 
 
 def test_unaligned_probe_view_falls_back(gpu):
-    b, p = workloads.config3(n_build=50_000, n_probe=200_000, seed=82)
+    b, p = workloads.join_tables(n_build=50_000, n_probe=200_000, seed=82)
     bt, pt = gpu.table(b), gpu.table(p)
     view = serve.table_slice(gpu, pt, 1, 150_001)          # starts 8 bytes into each column
     try:

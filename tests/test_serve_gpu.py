@@ -20,8 +20,8 @@ N_GROUP, N_BUILD, N_PROBE = 3_000_000, 200_000, 3_000_000
 
 @pytest.fixture(scope="module")
 def tables(gpu):
-    c2 = workloads.config2(n=N_GROUP, seed=52)
-    b, p = workloads.config3(n_build=N_BUILD, n_probe=N_PROBE, seed=53)
+    c2 = workloads.zipf_group_table(n=N_GROUP, seed=52)
+    b, p = workloads.join_tables(n_build=N_BUILD, n_probe=N_PROBE, seed=53)
     tg, tb, tp = gpu.table(c2), gpu.table(b), gpu.table(p)
     gpu.lib.td_gpu_pin.argtypes = [serve.P]
     gpu.lib.td_gpu_unpin.argtypes = [serve.P]
@@ -34,7 +34,7 @@ def tables(gpu):
 
 
 def _requests(n, seed):
-    raw = workloads.config5_requests(n, rate=1e9, seed=seed, group_rows=N_GROUP, probe_rows=N_PROBE,
+    raw = workloads.serve_requests(n, rate=1e9, seed=seed, group_rows=N_GROUP, probe_rows=N_PROBE,
                                      len_range=(10_000, 1_000_000))
     return [serve.Request(*r) for r in raw]
 

@@ -24,9 +24,9 @@ def test_splayed_table_loads_resident(gpu, tmp_path):
     L.td_gpu_splay_load.restype = C.c_void_p
     L.td_gpu_splay_load.argtypes = [C.c_char_p]
     L.td_gpu_unpin.argtypes = [C.c_void_p]
-    d = workloads.config1(n=2_000_000, seed=61)
+    d = workloads.readme_table(n=2_000_000, seed=61)
     t = gpu.table(d)
-    dirp = str(tmp_path / "cfg1")
+    dirp = str(tmp_path / "readme")
     assert L.td_splay_save(t, dirp.encode(), None) == 0
     gpu.release(t)
     r = gpu.check(L.td_gpu_splay_load(dirp.encode()), "td_gpu_splay_load")
@@ -51,7 +51,7 @@ def test_partitioned_db_loads_resident(gpu, tmp_path):
     L.td_gpu_unpin.argtypes = [C.c_void_p]
     parts = {}
     for i, day in enumerate(["2024.03.01", "2024.03.02", "2024.03.03"]):
-        d = workloads.config1(n=300_000 + 1000 * i, seed=70 + i)
+        d = workloads.readme_table(n=300_000 + 1000 * i, seed=70 + i)
         t = gpu.table(d)
         (tmp_path / day).mkdir()
         assert L.td_splay_save(t, str(tmp_path / day / "t").encode(), None) == 0
