@@ -1,5 +1,5 @@
 """Teide's own known answers, run on Teide itself (CPU).  Pins the td.h
-translations in known_cases.py before they judge the GPU library."""
+translations in known_cases.py before they are used to check the GPU library."""
 import pytest
 
 import known_cases
