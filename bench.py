@@ -24,6 +24,7 @@ oracle/_ref/) on a bounded sample of the same workload per step, with every
 host thread.
 """
 import argparse
+import functools
 import json
 import os
 import re
@@ -35,7 +36,6 @@ import time
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
-sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 METRIC = "fused filter/join/group-by rows/s & %HBM peak; served q/s + p99 vs plain"
 REF_LIB = os.path.join(ROOT, "oracle", "_ref", "libteide_ref.so")
@@ -112,19 +112,45 @@ class Clocks:
 
 # ---- workloads through the td.h API ------------------------------------------------
 
-def make_tables(td, workload, rank, device, scale=1.0):
+def workload_inputs(workload, rank=0, scale=1.0, device=None):
+    """The seeded numpy columns of a workload at its stated size (times
+    `scale`): {"build", "probe"} for the join, {"t"} otherwise.  Both arms of
+    the benchmark draw their inputs here, so the reference engine and the GPU
+    see the same shapes and, in one process, the same buffers.  `device`
+    draws the 200M-row Zipf table on that torch device (a numpy draw of it
+    takes about a minute)."""
     from teide_b200 import workloads
     if workload == "join_group":
-        b, p = workloads.join_tables(n_probe=int(100_000_000 * scale), seed=3 + 1000 * rank, device=device)
-        bt, pt = td.table(b), td.table(p)
-        return {"build": bt, "probe": pt}, len(p["fk"]), 16 * len(b["pk"]) + 24 * len(p["fk"]), 24 * len(p["fk"])
+        b, p = workloads.join_tables(n_probe=int(100_000_000 * scale), seed=3 + 1000 * rank)
+        return {"build": b, "probe": p}
     if workload in ("group_radix", "group_sort"):
-        c = workloads.zipf_group_table(n=int(200_000_000 * scale), seed=2 + 1000 * rank, device=device)
-        t = td.table(c)
-        return {"t": t}, len(c["key"]), 24 * len(c["key"]), 24 * len(c["key"])
-    c = workloads.readme_table(n=int(10_000_000 * scale), seed=1 + 1000 * rank)
-    t = td.table(c)
-    return {"t": t}, len(c["flag"]), 24 * len(c["flag"]), 24 * len(c["flag"])
+        return {"t": workloads.zipf_group_table(n=int(200_000_000 * scale), seed=2 + 1000 * rank, device=device)}
+    return {"t": workloads.readme_table(n=int(10_000_000 * scale), seed=1 + 1000 * rank)}
+
+
+def workload_rows(workload, cols):
+    """(rows per query, algorithmic bytes per query, bytes the main kernel streams)."""
+    if workload == "join_group":
+        n = len(cols["probe"]["fk"])
+        return n, 16 * len(cols["build"]["pk"]) + 24 * n, 24 * n
+    n = len(next(iter(cols["t"].values())))
+    return n, 24 * n, 24 * n
+
+
+def bench_config(workload, rows, alg_bytes, world, scale):
+    """The `config` object of a workload's JSON line; both arms print the same one."""
+    return {"workload": workload, "rows_per_gpu_per_step": rows, "algorithmic_bytes_per_step": alg_bytes,
+            "l2": "inputs larger than L2 (no flush)",
+            "parallelism": f"shards{world}" if world > 1 else "single",
+            "exchange": ("partial groups merged across ranks (all-gather, or all-to-all by key hash "
+                         "when large) inside every step") if world > 1 else None,
+            "scale": scale}
+
+
+def make_tables(td, workload, rank, device, scale=1.0):
+    cols = workload_inputs(workload, rank, scale, device)
+    tabs = {k: td.table(v) for k, v in cols.items()}
+    return (tabs, cols) + workload_rows(workload, cols)
 
 
 def splay_main(args, td, L, rank, world, local, barrier, max_over_ranks):
@@ -201,7 +227,7 @@ def splay_main(args, td, L, rank, world, local, barrier, max_over_ranks):
 def run_query(td, workload, tabs, world=1):
     """One step.  With several ranks every rank runs its shard and the partial
     groups are merged across ranks (teide_b200.shard) inside the step."""
-    from gpu_pipelines import fused_join_group, group_sorted, readme_group
+    from teide_b200.pipelines import fused_join_group, group_sorted, readme_group
     from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
     if world > 1:
         from teide_b200 import shard
@@ -379,7 +405,7 @@ def batch_main(args, td, L, rank, world, local, barrier, max_over_ranks):
         "clocks": clk.summary(tc0, tc1),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
-        rtd, q, desc = reference_sample("batch", 0)
+        rtd, q, desc = reference_sample("batch")
         q()
         t0 = time.perf_counter()
         n = 0
@@ -456,7 +482,7 @@ def serve_main(args, td, L, rank, world, local, barrier, max_over_ranks):
     achieved = alg / sv["closed_s"] / 1e9
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
-        _, q, desc = reference_sample("serve", 0)
+        _, q, desc = reference_sample("serve")
         secs = q()
         cpu = {"value": SERVE_REF_REQUESTS / secs, "unit": "queries/s", "cores": os.cpu_count(),
                "kind": "reference", "sample": desc}
@@ -493,7 +519,7 @@ def serve_reference(td):
     same shapes.  Each range is copied into its own table before the clock
     starts; the query runs Teide's filter -> group and filter -> join -> group
     graphs.  The returned callable gives the seconds spent in queries."""
-    from gpu_pipelines import const
+    from teide_b200.pipelines import const
     from teide_b200 import serve as sv
     from teide_b200 import workloads
     c2 = workloads.zipf_group_table(n=SERVE_REF_ROWS, seed=32)
@@ -536,52 +562,62 @@ def serve_reference(td):
     return td, q, desc
 
 
-def reference_sample(workload, scale_rows):
-    """Teide's CPU engine on a bounded sample of the workload: returns
-    (seconds per query, rows per query, description)."""
-    from gpu_pipelines import join_then_group, two_graph_group, two_graph_group_sorted
-    from teide_b200 import workloads
-    from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM, Td
+REF_BUILD = ("gcc -std=c17 -O3 -march=x86-64-v3 -DNDEBUG: the reference's release flags, with "
+             "x86-64-v3 (AVX2) in place of -march=native so one binary runs on every host")
+
+
+@functools.lru_cache(maxsize=1)
+def reference_engine():
+    """Teide's own engine (compiled from its sources into oracle/_ref) and the
+    number of threads its td_execute runs on (the pool's workers + caller)."""
+    import ctypes as C
+    from teide_b200.td import Td
     td = Td(REF_LIB)
+    td.lib.td_thread_count.restype = C.c_uint32
+    return td, int(td.lib.td_thread_count())
+
+
+def reference_sample(workload, cols=None, scale=1.0):
+    """Teide's CPU engine on one query of the workload at the same size as
+    the GPU arm: returns (td, query callable, description).  `cols` are the
+    GPU arm's own input arrays when this runs in its process; otherwise they
+    are drawn from the same generators."""
+    from teide_b200.pipelines import join_then_group, two_graph_group, two_graph_group_sorted
+    from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
+    td, threads = reference_engine()
     if workload == "serve":
         return serve_reference(td)
     if workload == "batch":
         b = Batch(td, first=BATCH_REF_QUERIES)
         desc = (f"the first {b.n} of the 4096 queries ({b.rows / 1e6:.1f}M rows), one td_execute each")
         return td, b.plain, desc
+    if cols is None:
+        cols = workload_inputs(workload, 0, scale, device="cpu")
     if workload == "join_group":
-        b, p = workloads.join_tables(n_build=10_000_000, n_probe=scale_rows, seed=33)
-        bt, pt = td.table(b), td.table(p)
+        bt, pt = td.table(cols["build"]), td.table(cols["probe"])
 
         def q():
             join_then_group(td, bt, pt, ("qty", "gt", 10), "fk", "pk", ["cat"],
-                            [(OP_SUM, "price"), (OP_COUNT, "price")])
-        desc = f"build 10M rows + probe {scale_rows / 1e6:g}M rows per query (probe side sampled from 100M)"
-    elif workload == "group_radix":
-        c = workloads.zipf_group_table(n=scale_rows, seed=32)
-        t = td.table(c)
-
-        def q():
-            two_graph_group(td, t, ("v1", "gt", 0), ["key"],
-                            [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")])
-        desc = f"{scale_rows / 1e6:g}M of 200M rows per query"
-    elif workload == "group_sort":
-        c = workloads.zipf_group_table(n=scale_rows, seed=32)
-        t = td.table(c)
-
-        def q():
-            two_graph_group_sorted(td, t, ("v1", "gt", 0), ["key"],
-                                   [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")],
-                                   "v1_sum", desc=True)
-        desc = f"{scale_rows / 1e6:g}M of 200M rows per query, group result sorted by v1_sum DESC"
+                            [(OP_SUM, "price"), (OP_COUNT, "price")], as_dict=False)
+        desc = (f"build {len(cols['build']['pk']) / 1e6:g}M + probe {len(cols['probe']['fk']) / 1e6:g}M rows per "
+                "query: Teide's filter + join graph, then the group graph over the joined table")
     else:
-        c = workloads.readme_table(n=scale_rows, seed=31)
-        t = td.table(c)
-
-        def q():
-            two_graph_group(td, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
-        desc = f"{scale_rows / 1e6:g}M rows per query"
-    return td, q, desc
+        t = td.table(cols["t"])
+        n = len(next(iter(cols["t"].values())))
+        aggs5 = [(OP_COUNT, "v1"), (OP_SUM, "v1"), (OP_MIN, "v1"), (OP_MAX, "v1"), (OP_AVG, "v2")]
+        if workload == "group_radix":
+            def q():
+                two_graph_group(td, t, ("v1", "gt", 0), ["key"], aggs5, as_dict=False)
+            desc = f"{n / 1e6:g}M rows per query: Teide's filter graph, then the group graph"
+        elif workload == "group_sort":
+            def q():
+                two_graph_group_sorted(td, t, ("v1", "gt", 0), ["key"], aggs5, "v1_sum", desc=True)
+            desc = f"{n / 1e6:g}M rows per query, group result sorted by v1_sum DESC"
+        else:
+            def q():
+                two_graph_group(td, t, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")], as_dict=False)
+            desc = f"{n / 1e6:g}M rows per query: Teide's filter graph, then the group graph"
+    return td, q, desc + f"; {threads} threads; {REF_BUILD}"
 
 
 def reference_splay(args):
@@ -624,6 +660,8 @@ def reference_splay(args):
 
 
 def reference_arm(args):
+    """Teide's own CPU engine on the same workload, sizes and config as the
+    GPU arm (rank 0 only; other ranks exit without work)."""
     if int(os.environ.get("RANK", "0")) != 0:
         return
     if not os.path.exists(REF_LIB):
@@ -631,13 +669,20 @@ def reference_arm(args):
         return
     if args.workload == "splay_load":
         return reference_splay(args)
-    rows = {"join_group": 10_000_000, "group_radix": 20_000_000, "group_sort": 20_000_000,
-            "readme_group": 10_000_000, "batch": BATCH_REF_QUERIES, "serve": SERVE_REF_REQUESTS}[args.workload]
-    td, q, desc = reference_sample(args.workload, rows)
+    td, q, desc = reference_sample(args.workload, scale=args.scale)
     if args.workload == "serve":                 # q() reports its own query seconds
         for _ in range(min(args.warmup, 1)):
             q()
         dt = sum(q() for _ in range(max(1, min(args.steps, 2)))) / max(1, min(args.steps, 2))
+        rows, config = SERVE_REF_REQUESTS, {"workload": "serve", "sample": desc}
+    elif args.workload == "batch":
+        for _ in range(args.warmup):
+            q()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            q()
+        dt = (time.perf_counter() - t0) / args.steps
+        rows, config = BATCH_REF_QUERIES, {"workload": "batch", "sample": desc}
     else:
         for _ in range(args.warmup):
             q()
@@ -645,17 +690,29 @@ def reference_arm(args):
         for _ in range(args.steps):
             q()
         dt = (time.perf_counter() - t0) / args.steps
+        rows, alg, _ = workload_rows(args.workload, workload_inputs_shape(args.workload, args.scale))
+        config = bench_config(args.workload, rows, alg, args.gpus, args.scale)
     v = rows / dt
     unit = "queries/s" if args.workload in ("batch", "serve") else "rows/s"
-    cores = os.cpu_count()
+    _, threads = reference_engine()
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": unit, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
-        "config": {"workload": args.workload, "sample": desc},
-        "cpu_baseline": {"value": v, "unit": unit, "cores": cores, "kind": "reference", "sample": desc},
+        "config": config, "tables": "host memory (Teide's heap)",
+        "cpu_baseline": {"value": v, "unit": unit, "cores": threads, "kind": "reference",
+                         "sample": f"the whole workload, every step; {desc}"},
         "e2e": {"value": v, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def workload_inputs_shape(workload, scale=1.0):
+    """Row counts of a workload's inputs, without drawing them."""
+    import numpy as np
+    if workload == "join_group":
+        return {"build": {"pk": np.empty(10_000_000)}, "probe": {"fk": np.empty(int(100_000_000 * scale))}}
+    n = int((200_000_000 if workload in ("group_radix", "group_sort") else 10_000_000) * scale)
+    return {"t": {"key": np.empty(n, dtype=np.uint8)}}
 
 
 # ---- GPU arm -------------------------------------------------------------------------------
@@ -726,7 +783,7 @@ def main():
             dist.destroy_process_group()
         return
 
-    tabs, rows, alg_bytes, main_bytes = make_tables(td, args.workload, rank, "cuda", args.scale)
+    tabs, cols, rows, alg_bytes, main_bytes = make_tables(td, args.workload, rank, "cuda", args.scale)
     torch.cuda.empty_cache()
 
     # ---- resident: tables pinned in HBM ----
@@ -789,13 +846,8 @@ def main():
         "metric": METRIC, "value": value, "unit": "rows/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64/f64", "data": "synthetic",
-        "config": {"workload": args.workload, "rows_per_gpu_per_step": rows,
-                   "algorithmic_bytes_per_step": alg_bytes, "l2": "inputs larger than L2 (no flush)",
-                   "tables": "resident in HBM (td_gpu_pin)",
-                   "parallelism": f"shards{world}" if world > 1 else "single",
-                   "exchange": ("partial groups merged across ranks (all-gather, or all-to-all by key hash "
-                                "when large) inside every step") if world > 1 else None,
-                   "scale": args.scale},
+        "config": bench_config(args.workload, rows, alg_bytes, world, args.scale),
+        "tables": "resident in HBM (td_gpu_pin)",
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": (achieved / hbm) if achieved else None, "traffic": profile_traffic(prof),
                      "kernel": {"join_group": "k_probe_vec (fused probe + aggregate)",
@@ -815,18 +867,19 @@ def main():
     if args.workload == "group_sort" and sort_ms:
         line["sort_ms"] = sum(sort_ms) / len(sort_ms)      # tdg_sort_perm: the 5.9M-row permutation
     if rank == 0 and world == 1 and not args.no_cpu_baseline and os.path.exists(REF_LIB):
-        rows_s = {"join_group": 10_000_000, "group_radix": 20_000_000, "group_sort": 20_000_000,
-                  "readme_group": 10_000_000}[args.workload]
-        rtd, q, desc = reference_sample(args.workload, rows_s)
+        # Teide's engine on the same input arrays and the same query as every
+        # GPU step: one warm-up, then whole queries until about 10 s have passed.
+        rtd, q, desc = reference_sample(args.workload, cols)
         q()
         t0 = time.perf_counter()
         n = 0
-        while n < 3 or time.perf_counter() - t0 < 10:
+        while n < 2 or time.perf_counter() - t0 < 10:
             q()
             n += 1
         dt = (time.perf_counter() - t0) / n
-        line["cpu_baseline"] = {"value": rows_s / dt, "unit": "rows/s", "cores": os.cpu_count(),
-                                "kind": "reference", "sample": desc + f", mean of {n} runs"}
+        _, threads = reference_engine()
+        line["cpu_baseline"] = {"value": rows / dt, "unit": "rows/s", "cores": threads,
+                                "kind": "reference", "sample": f"the whole workload, mean of {n} queries; {desc}"}
     if rank == 0:
         print(json.dumps(line))
     if dist:

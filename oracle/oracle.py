@@ -139,6 +139,89 @@ def group(keys: dict, aggs, mask=None) -> dict:
     return out
 
 
+def abs_bounds(keys: dict, aggs, mask=None) -> dict:
+    """Per group, the scale of the F64 tolerance rule |got - want| <= 1e-12 *
+    max(|want|, bound): sum |x| for an F64 SUM, sum |x| / count for AVG.
+    Same arguments and row order as group(); only F64 SUM/AVG columns."""
+    fa = [(op, nm, np.abs(np.asarray(a))) for op, nm, a in aggs
+          if op in (OP_SUM, OP_AVG) and a is not None and np.asarray(a).dtype.kind == "f"]
+    return group(keys, fa, mask) if fa else {}
+
+
+def group_direct(key, aggs, mask=None, key_name="key") -> dict:
+    """Group-by on one integer key through a direct array, slot = key - min
+    (the DA path, exec.c:5948-6404; da_accum_row 5045-5099): the same result
+    as group() for one integer key, in ascending key order, computed with
+    scatter updates so that hundreds of millions of rows take seconds.
+    Integer SUM wraps (np.add.at on int64, like exec.c:5075); F64 SUM adds
+    in row order; AVG = sum / count; MIN/MAX keep the input type."""
+    key = np.asarray(key)
+    sel = None if mask is None else np.nonzero(mask)[0]
+    k = key if sel is None else key[sel]
+    out = {}
+    if len(k) == 0:
+        out[key_name] = key[:0].copy()
+        for op, nm, arr in aggs:
+            dt = np.int64 if op == OP_COUNT else (np.float64 if op == OP_AVG else
+                                                  (np.float64 if np.asarray(arr).dtype.kind == "f" else np.int64))
+            out[f"{nm}{SUFFIX[op]}"] = np.zeros(0, dt)
+        return out
+    lo = int(k.min())
+    slot = (k.astype(np.int64) - lo)
+    nslot = int(slot.max()) + 1
+    cnt = np.bincount(slot, minlength=nslot).astype(np.int64)
+    present = np.nonzero(cnt)[0]
+    out[key_name] = (present + lo).astype(key.dtype)
+    for op, nm, arr in aggs:
+        col = f"{nm}{SUFFIX[op]}"
+        if op == OP_COUNT:
+            out[col] = cnt[present]
+            continue
+        v = np.asarray(arr)
+        v = v if sel is None else v[sel]
+        isf = v.dtype.kind == "f"
+        if op in (OP_SUM, OP_AVG):
+            if isf:
+                acc = np.bincount(slot, weights=v.astype(np.float64), minlength=nslot)
+            else:
+                acc = np.zeros(nslot, np.int64)
+                np.add.at(acc, slot, v.astype(np.int64))
+            acc = acc[present]
+            out[col] = acc if op == OP_SUM else acc.astype(np.float64) / cnt[present]
+        elif op in (OP_MIN, OP_MAX):
+            if isf:
+                acc = np.full(nslot, np.inf if op == OP_MIN else -np.inf, v.dtype)
+            else:
+                info = np.iinfo(v.dtype)
+                acc = np.full(nslot, info.max if op == OP_MIN else info.min, v.dtype)
+            (np.minimum if op == OP_MIN else np.maximum).at(acc, slot, v)
+            out[col] = acc[present]
+    return out
+
+
+def join_unique_direct(lkey, rkey, lmask=None):
+    """(left row, right row) pairs of an inner equi-join on one integer key
+    whose build-side (right) values are unique, through a direct map of the
+    build keys: the pairs join_pairs() gives for that case (left-row order),
+    at hundreds of millions of rows.  Raises if a build key repeats."""
+    rkey = np.asarray(rkey).astype(np.int64)
+    lkey = np.asarray(lkey).astype(np.int64)
+    lsel = np.arange(len(lkey)) if lmask is None else np.nonzero(lmask)[0]
+    if len(rkey) == 0 or len(lsel) == 0:
+        return np.zeros(0, np.int64), np.zeros(0, np.int64)
+    lo, hi = int(rkey.min()), int(rkey.max())
+    row = np.full(hi - lo + 1, -1, np.int64)
+    row[rkey - lo] = np.arange(len(rkey))
+    if int((row >= 0).sum()) != len(rkey):
+        raise ValueError("join_unique_direct: build keys repeat")
+    lk = lkey[lsel]
+    inr = (lk >= lo) & (lk <= hi)
+    ri = np.full(len(lk), -1, np.int64)
+    ri[inr] = row[lk[inr] - lo]
+    hit = ri >= 0
+    return lsel[hit].astype(np.int64), ri[hit]
+
+
 def _join_ids(lkeys, rkeys):
     """Map key tuples of both sides onto shared dense ids."""
     nl = len(lkeys[0])

@@ -33,7 +33,7 @@ def readme_group(td, tbl, pred, keys, aggs, as_dict=True):
     return _result(td, r, as_dict)
 
 
-def two_graph_group(td, tbl, pred, keys, aggs):
+def two_graph_group(td, tbl, pred, keys, aggs, as_dict=True):
     """Filter graph -> compacted table -> group graph."""
     g = td.graph(tbl)
     try:
@@ -47,8 +47,7 @@ def two_graph_group(td, tbl, pred, keys, aggs):
                               [g.scan(n) for _, n in aggs]))
     finally:
         g.free()
-    out = td.table_dict(r)
-    td.release(r)
+    out = _result(td, r, as_dict)
     td.release(t2)
     return out
 
@@ -67,8 +66,11 @@ def fused_join_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_ty
     return _result(td, r, as_dict)
 
 
-def join_then_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_type=0):
-    """Two calls: materialized join, then a group graph over its result."""
+def join_then_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_type=0, as_dict=True):
+    """Two calls: materialized join, then a group graph over its result.
+    Returns (groups, joined rows) as {name: numpy array}; with as_dict False
+    both host results are produced and dropped unread, so a timed step holds
+    only the engine's own work."""
     g = td.graph(probe_t)
     try:
         c, op, k = pred
@@ -76,15 +78,14 @@ def join_then_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_typ
         jr = g.execute(g.join(left, [g.scan(lkey)], g.const_table(build_t), [g.scan(rkey)], join_type))
     finally:
         g.free()
-    joined = td.table_dict(jr)
+    joined = td.table_dict(jr) if as_dict else None
     g = td.graph(jr)
     try:
         r = g.execute(g.group([g.scan(n) for n in keys], [a for a, _ in aggs],
                               [g.scan(n) for _, n in aggs]))
     finally:
         g.free()
-    out = td.table_dict(r)
-    td.release(r)
+    out = _result(td, r, as_dict)
     td.release(jr)
     return out, joined
 

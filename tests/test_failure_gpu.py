@@ -10,7 +10,7 @@ import numpy as np
 import pytest
 
 import oracle
-from gpu_pipelines import readme_group
+from teide_b200.pipelines import readme_group
 from teide_b200.td import OP_SUM, TdError
 
 pytestmark = pytest.mark.gpu

@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
-from gpu_pipelines import const
+from teide_b200.pipelines import const, f64_tolerance_ok
 from teide_b200 import serve
 from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
 
@@ -44,15 +44,21 @@ def _want(d, preds, aggs):
     m = np.ones(len(d["region"]), bool)
     for c, op, k in preds:
         m &= oracle.compare(op, d[c], k)
-    return oracle.group({"region": d["region"][m]},
-                        [(op, n, None if op == OP_COUNT else d[n][m]) for op, n in aggs])
+    keys = {"region": d["region"][m]}
+    a = [(op, n, None if op == OP_COUNT else d[n][m]) for op, n in aggs]
+    want = oracle.group(keys, a)
+    want["_abs"] = oracle.abs_bounds(keys, a)
+    return want
 
 
 def _same(got, want):
+    """Integers and F64 MIN/MAX exact; F64 SUM/AVG by the 1e-12 rule, with
+    the bounds _want put under "_abs"."""
+    bounds = want.pop("_abs", {})
     assert list(got) == list(want)
     for k in want:
-        if want[k].dtype.kind == "f":
-            assert np.allclose(got[k], want[k], rtol=1e-12, atol=1e-9), k
+        if k in bounds:
+            assert f64_tolerance_ok(got[k], want[k], bounds[k]), k
         else:
             assert np.array_equal(got[k], want[k]), k
 
@@ -103,8 +109,8 @@ def test_wide_key_range_takes_other_kernels(gpu):
     t = gpu.table(d)
     try:
         preds, aggs = CASES[0]
-        _same(oracle.canonical(_run(gpu, t, preds, aggs), by=["region"]),
-              oracle.canonical(_want(d, preds, aggs), by=["region"]))
+        want = _want(d, preds, aggs)          # already in ascending key order, like its bounds
+        _same(oracle.canonical(_run(gpu, t, preds, aggs), by=["region"]), want)
     finally:
         gpu.release(t)
 

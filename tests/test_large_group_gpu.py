@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 import oracle
-from gpu_pipelines import readme_group
+from teide_b200.pipelines import readme_group
 from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
 
 pytestmark = pytest.mark.gpu

@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import oracle
-from gpu_pipelines import const
+from teide_b200.pipelines import const
 from teide_b200.td import I16, I32, OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM, U8
 
 pytestmark = pytest.mark.gpu

@@ -159,3 +159,53 @@ def test_oracle_vs_reference_filter_join_group(ref):
         assert np.array_equal(v, joined[k]), k
     got = oracle.group({"cat": j["cat"]}, [(OP_SUM, "price", j["price"]), (OP_COUNT, "price", None)])
     assert_group_equal(got, want, ["cat"])
+
+
+# ---- the direct-array forms used by the full-size parity tests ---------------------
+
+def test_group_direct_zipf_golden():
+    """group_direct gives Teide's own output on the Zipf fixture."""
+    z = load("zipf_group_small")
+    c = pick(z, "in_")
+    m = oracle.conj(c, [("v1", "gt", 0)])
+    got = oracle.group_direct(c["key"], [(OP_COUNT, "v1", None), (OP_SUM, "v1", c["v1"]),
+                                         (OP_MIN, "v1", c["v1"]), (OP_MAX, "v1", c["v1"]),
+                                         (OP_AVG, "v2", c["v2"])], m)
+    assert_group_equal(got, pick(z, "out_"), ["key"])
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_group_direct_equals_group(seed):
+    r = np.random.default_rng(seed)
+    n = 300_000
+    k = r.integers(-5000, 70_000, n)
+    vi = r.integers(-(2**62), 2**62, n)            # sums wrap
+    vf = r.standard_normal(n)
+    m = r.random(n) < 0.6
+    aggs = [(OP_COUNT, "vi", None), (OP_SUM, "vi", vi), (OP_MIN, "vi", vi), (OP_MAX, "vi", vi),
+            (OP_SUM, "vf", vf), (OP_AVG, "vf", vf), (OP_MIN, "vf", vf), (OP_MAX, "vf", vf)]
+    want = oracle.group({"key": k}, aggs, m)
+    got = oracle.group_direct(k, aggs, m)
+    assert list(got) == list(want)
+    for name in want:
+        if want[name].dtype.kind == "f":
+            assert np.allclose(got[name], want[name], rtol=1e-12, atol=1e-9), name
+        else:
+            assert np.array_equal(got[name], want[name]), name
+    empty = oracle.group_direct(k, aggs, np.zeros(n, bool))
+    assert all(len(v) == 0 for v in empty.values())
+
+
+def test_join_unique_direct_golden():
+    """join_unique_direct gives the same pairs as join_pairs and Teide's joined rows."""
+    z = load("join_group_small")
+    b, p = pick(z, "b_"), pick(z, "p_")
+    m = oracle.conj(p, [("qty", "gt", 10)])
+    li, ri = oracle.join_unique_direct(p["fk"], b["pk"], m)
+    li2, ri2 = oracle.join_pairs([p["fk"]], [b["pk"]], 0, m)
+    assert np.array_equal(li, li2) and np.array_equal(ri, ri2)
+    j = {"fk": p["fk"][li], "qty": p["qty"][li], "price": p["price"][li], "cat": b["cat"][ri]}
+    for k, v in oracle.canonical(j).items():
+        assert np.array_equal(v, pick(z, "join_")[k]), k
+    with pytest.raises(ValueError):
+        oracle.join_unique_direct(np.arange(5), np.array([1, 2, 2]))

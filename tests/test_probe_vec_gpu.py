@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from gpu_pipelines import const
+from teide_b200.pipelines import const, f64_tolerance_ok
 from teide_b200 import serve, workloads
 from teide_b200.td import OP_COUNT, OP_MAX, OP_SUM
 
@@ -36,14 +36,21 @@ def _want(b, p, preds, aggs):
     for c, op, k in preds:
         m &= oracle.compare(op, p[c], k)
     j = oracle.join(p, b, ["fk"], ["pk"], 0, lmask=m)
-    return oracle.group({"cat": j["cat"]}, [(op, n, None if op == OP_COUNT else j[n]) for op, n in aggs])
+    keys = {"cat": j["cat"]}
+    a = [(op, n, None if op == OP_COUNT else j[n]) for op, n in aggs]
+    want = oracle.group(keys, a)
+    want["_abs"] = oracle.abs_bounds(keys, a)
+    return want
 
 
 def _same(got, want):
+    """Integers and F64 MIN/MAX exact; F64 SUM/AVG by the 1e-12 rule, with
+    the bounds _want put under "_abs"."""
+    bounds = want.pop("_abs", {})
     assert list(got) == list(want)
     for k in want:
-        if want[k].dtype.kind == "f":
-            assert np.allclose(got[k], want[k], rtol=1e-12, atol=1e-9), k
+        if k in bounds:
+            assert f64_tolerance_ok(got[k], want[k], bounds[k]), k
         else:
             assert np.array_equal(got[k], want[k]), k
 
