@@ -185,7 +185,9 @@ tdg_status tdg_group_run(const tdg_group_desc* d, const tdg_expr* pred, const ui
  * plan.max_groups rows, where tdg_group_plan_make(d, 0, &plan) gives the plan
  * (and its ws_bytes); a group-by that needs more scratch than the array holds
  * is refused with TD_ERR_RANGE.  The first call on a device looks up the
- * array's device address; make it before any stream capture.  Every call
+ * array's device address; make it before any stream capture.  Each call
+ * waits for its stream before it returns (it reads the group count back to
+ * size the emit).  Every call
  * shares the array, and each call re-initializes what it reads, but calls
  * that overlap on the GPU race: serialize them. */
 #define TDG_STATIC_SCRATCH_BYTES (16u << 20)
@@ -253,6 +255,22 @@ tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_plan* jplan
                               const tdg_expr* lpred, const uint64_t* lsel,
                               const tdg_group_desc* g, const tdg_group_plan* gplan, void* gws,
                               const tdg_group_out* out, void* stream);
+
+/* ---- hash table ------------------------------------------------------------------
+ * The open-addressing table the hash group-by and hash join build on, as an
+ * entry point: finds or inserts n key tuples (n_keys int64 key columns laid
+ * out column-wise in kv, kv[k * n + i]) in a caller-owned table of `cap`
+ * slots (a power of two): state[cap] (0 empty, 1 being written, 2 ready) and
+ * keys[n_keys * cap].  d_slot[i] receives tuple i's slot, or -1.  A thread
+ * that meets a slot in state 1 polls it at most spin_limit times (0: the
+ * library's limit, 2^20) before it fails that row with TD_ERR_IO, so a
+ * writer that never publishes ends the kernel with an error instead of a
+ * hang.  Returns the first error recorded (TD_ERR_RANGE: table full);
+ * d_err is one device int32 of scratch.  Synchronizes the stream.
+ * Replaces the find-or-insert of group_probe_entry (exec.c:4131-4170). */
+tdg_status tdg_hash_upsert(uint32_t* state, int64_t* keys, uint64_t cap, int32_t n_keys,
+                           const int64_t* kv, int64_t n, int32_t spin_limit, int64_t* d_slot,
+                           int32_t* d_err, void* stream);
 
 /* ---- sort ------------------------------------------------------------------------
  * tdg_sort_perm: the stable permutation that orders n rows by keys[0..n_keys)

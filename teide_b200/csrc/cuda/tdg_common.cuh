@@ -362,7 +362,6 @@ void set_last_main_ms(float ms);
 void set_last_build_ms(float ms);
 void set_last_sort_ms(float ms);
 
-// While alive, this thread's tdg calls record no timing events.
 // While alive, this thread's tdg calls make no allocating CUDA call (no
 // page-locked status buffers either): the entry points that allocate nothing.
 struct ThreadNoAlloc {
@@ -371,6 +370,7 @@ struct ThreadNoAlloc {
 };
 bool no_alloc();
 
+// While alive, this thread's tdg calls record no timing events.
 struct ThreadTimingOff {
     ThreadTimingOff();
     ~ThreadTimingOff();

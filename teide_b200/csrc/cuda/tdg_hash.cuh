@@ -24,6 +24,7 @@ struct HtRef {
     int64_t*  keys;        // n_keys * cap
     uint64_t  mask;        // cap - 1
     int32_t   nk;
+    int32_t   spin_limit;  // polls of a state-1 slot before giving up (0: kSpinLimit)
     int32_t*  err;
 };
 
@@ -55,10 +56,11 @@ __device__ inline int64_t ht_upsert(const HtRef& H, const int64_t* kv, uint64_t 
             s = prev;
         }
         if (s == 1) {
+            const int limit = H.spin_limit > 0 ? H.spin_limit : kSpinLimit;
             int spins = 0;
             do {
                 s = *(volatile uint32_t*)&H.state[i];
-                if (++spins > kSpinLimit) { set_err(H.err, E_IO); return -1; }
+                if (++spins > limit) { set_err(H.err, E_IO); return -1; }
             } while (s == 1);
         }
         __threadfence();

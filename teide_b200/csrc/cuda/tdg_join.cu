@@ -399,3 +399,43 @@ extern "C" tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_
     if (d->join_type == 2 && d->n_right > 0) cudaMemsetAsync(J.matched, 0, (size_t)d->n_right, s);
     return group_run_joined(g, gp, gws, lpred, lsel, &J, d->n_left, d->n_right, out, s);
 }
+
+// ---- the hash-table upsert as an entry point --------------------------------------
+// One thread per key tuple; each one finds or claims its slot with ht_upsert.
+__global__ void k_ht_upsert(tdg::HtRef H, const int64_t* kv, int64_t n, int64_t* slot) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int64_t t[TDG_MAX_KEYS];
+    for (int k = 0; k < H.nk; k++) t[k] = kv[(int64_t)k * n + i];
+    slot[i] = tdg::ht_upsert(H, t, tdg::hash_keys(t, H.nk));
+}
+
+extern "C" tdg_status tdg_hash_upsert(uint32_t* state, int64_t* keys, uint64_t cap, int32_t n_keys,
+                                      const int64_t* kv, int64_t n, int32_t spin_limit, int64_t* d_slot,
+                                      int32_t* d_err, void* stream) {
+    using namespace tdg;
+    if (cap == 0 || (cap & (cap - 1)) || n_keys < 1 || n_keys > TDG_MAX_KEYS || n < 0 || spin_limit < 0)
+        return E_RANGE;
+    cudaStream_t s = (cudaStream_t)stream;
+    if (cudaMemsetAsync(d_err, 0, 4, s) != cudaSuccess) return launch_status();
+    if (n > 0) {
+        HtRef H;
+        memset(&H, 0, sizeof(H));
+        H.state = state;
+        H.keys = keys;
+        H.mask = cap - 1;
+        H.nk = n_keys;
+        H.spin_limit = spin_limit;
+        H.err = d_err;
+        const int threads = 256;
+        (note_launch(), k_ht_upsert<<<(unsigned)((n + threads - 1) / threads), threads, 0, s>>>(H, kv, n, d_slot));
+    }
+    int32_t err = 0;
+    if (cudaMemcpyAsync(&err, d_err, 4, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        const tdg_status e = launch_status();
+        return e ? e : E_IO;
+    }
+    return err ? err : launch_status();
+}
+

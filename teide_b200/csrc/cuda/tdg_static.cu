@@ -20,7 +20,9 @@
 //     threads -- race on it and must be serialized by the caller;
 //   - the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (a host-side symbol is not a device address); make
-//     that first call before any stream capture.
+//     that first call before any stream capture;
+//   - each call waits for its stream before it returns (the group count is
+//     read back to size the emit).
 #include "tdg_hash.cuh"
 #include <mutex>
 

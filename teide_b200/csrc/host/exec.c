@@ -592,9 +592,14 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
     if (st) return TD_ERR_PTR(st);
     tdb_trace("group kernels done");
     int64_t ng = 0;
-    if (hng) ng = *hng;
+    if (hng) { ng = *hng; x->c.d2h_bytes += 8; }          /* written over the link by the kernel */
     else if ((st = tdb_d2h(&x->c, &ng, out.d_n_groups, 8))) return TD_ERR_PTR(st);
     tdb_trace("group count read");
+    /* rows the kernels wrote into mapped host memory crossed the link too */
+    for (int k = 0; k < nk; k++)
+        if (hout[k]) x->c.d2h_bytes += (uint64_t)ng * td_sym_elem_size(keys[k].type, keys[k].attrs);
+    for (int a = 0; a < na; a++)
+        if (hout[nk + a]) x->c.d2h_bytes += (uint64_t)ng * 8;
 
     /* every result column is copied with one stream synchronization */
     td_t* cols[TDG_MAX_KEYS + TDG_MAX_AGGS];
@@ -847,6 +852,7 @@ static td_t* reduce(ex_t* x, uint16_t opc, val_t* v) {
     if (h[2]) {   /* tdg_group_run synchronized its stream */
         ng = h[0][0];
         if (ng > 0) { memcpy(&val, h[1], 8); cnt = h[2][0]; }
+        x->c.d2h_bytes += 8 + 16 * (uint64_t)ng;        /* the kernel wrote them over the link */
     } else {
         st = tdb_d2h(&x->c, &ng, out.d_n_groups, 8);
         if (!st && ng > 0) st = tdb_d2h(&x->c, &val, out.aggs[0], 8);

@@ -312,16 +312,57 @@ void td_sel_recompute(td_t* sel) {
     m->total_pass = total;
 }
 
+/* BOOL vector -> TD_SEL (sel.c:128-161 packs bytes into bits in one
+ * thread, then td_sel_recompute counts every segment).  Here the device
+ * does both in one pass: tdg_select_bitmap evaluates `pred != 0` over the
+ * vector's device copy (uploaded unless resident), packs each warp's 32
+ * rows with a ballot and writes every 1024-row segment's flag and popcount;
+ * the bits, flags, popcounts and total come back into the block. */
 td_t* td_sel_from_pred(td_t* pred) {
     if (!pred || TD_IS_ERR(pred)) return pred;
     if (pred->type != TD_BOOL) return TD_ERR_PTR(TD_ERR_TYPE);
     td_t* s = td_sel_new(pred->len);
-    if (!s || TD_IS_ERR(s)) return s;
-    uint64_t* bits = td_sel_bits(s);
-    const uint8_t* b = (const uint8_t*)td_data(pred);
-    for (int64_t r = 0; r < pred->len; r++)
-        if (b[r]) bits[r >> 6] |= 1ULL << (r & 63);
-    td_sel_recompute(s);
+    if (!s || TD_IS_ERR(s) || pred->len == 0) return s;
+    const int64_t n = pred->len;
+    const int64_t words = (n + 63) >> 6;
+    const uint32_t n_segs = td_sel_meta(s)->n_segs;
+    tdb_ctx c;
+    int st = tdb_ctx_begin(&c);
+    tdb_devcol dc;
+    if (!st) st = tdb_col_device(&c, pred, 0, &dc);
+    uint64_t* dbits = NULL;
+    uint8_t* dflags = NULL;
+    uint16_t* dpop = NULL;
+    int64_t* dtotal = NULL;
+    if (!st) {
+        dbits = tdb_dev_alloc(&c, (size_t)words * 8);
+        dflags = tdb_dev_alloc(&c, n_segs);
+        dpop = tdb_dev_alloc(&c, (size_t)n_segs * 2);
+        dtotal = tdb_dev_alloc(&c, 8);
+        if (!dbits || !dflags || !dpop || !dtotal) st = TD_ERR_OOM;
+    }
+    if (!st) {
+        tdg_expr e;
+        memset(&e, 0, sizeof(e));
+        e.n_cols = 1;
+        e.cols[0].data = dc.dptr;
+        e.cols[0].type = TD_BOOL;
+        e.n_ins = 3;
+        e.ins[0].op = TDG_X_COL;
+        e.ins[1].op = TDG_X_CONST;
+        e.ins[2].op = TDG_X_NE; e.ins[2].a = 0; e.ins[2].b = 1;
+        e.out = 2;
+        st = tdg_select_bitmap(n, &e, NULL, dbits, dflags, dpop, dtotal, c.stream);
+    }
+    int64_t total = 0;
+    if (!st) st = tdb_d2h(&c, td_sel_bits(s), dbits, (size_t)words * 8);
+    if (!st) st = tdb_d2h(&c, td_sel_flags(s), dflags, n_segs);
+    if (!st) st = tdb_d2h(&c, td_sel_popcnt(s), dpop, (size_t)n_segs * 2);
+    if (!st) st = tdb_d2h(&c, &total, dtotal, 8);
+    if (!st) st = tdb_ctx_sync(&c);
+    tdb_ctx_end(&c);
+    if (st) { td_release(s); return TD_ERR_PTR(st); }
+    td_sel_meta(s)->total_pass = total;
     return s;
 }
 

@@ -268,7 +268,76 @@ def case_join_multikey(td):
         td.release(x)
 
 
+def _sel_total(td, sel):
+    """td_sel_meta(sel)->total_pass (td.h: the TD_SEL body starts with it)."""
+    import ctypes as C
+    typ, _, _ = td.header(sel)
+    assert typ == 16, typ                             # TD_SEL
+    return C.c_int64.from_address(sel + 32).value
+
+
+def _sel_bits(td, sel, n):
+    import ctypes as C
+    n_segs = C.c_uint32.from_address(sel + 32 + 8).value
+    off = 32 + 16 + ((n_segs + 7) & ~7) + 2 * ((n_segs + 3) & ~3)
+    words = (n + 63) // 64
+    return np.frombuffer(C.string_at(sel + off, 8 * words), np.uint64)
+
+
+def case_sel_from_pred(td):
+    """test_sel.c:42-64 -- BOOL [1,0,1,0,1] -> TD_SEL with total_pass 3."""
+    b = td.vec(np.array([1, 0, 1, 0, 1], np.bool_))
+    s = td.check(td.lib.td_sel_from_pred(b), "sel_from_pred")
+    assert _sel_total(td, s) == 3
+    assert int(_sel_bits(td, s, 5)[0]) == 0b10101
+    td.release(s)
+    td.release(b)
+
+
+def case_sel_and(td):
+    """test_sel.c:66-92 -- {1,1,0,0,1} AND {1,0,1,0,1} -> 2 passing."""
+    a = td.vec(np.array([1, 1, 0, 0, 1], np.bool_))
+    b = td.vec(np.array([1, 0, 1, 0, 1], np.bool_))
+    sa = td.check(td.lib.td_sel_from_pred(a), "sel_from_pred")
+    sb = td.check(td.lib.td_sel_from_pred(b), "sel_from_pred")
+    s = td.check(td.lib.td_sel_and(sa, sb), "sel_and")
+    assert _sel_total(td, s) == 2
+    assert int(_sel_bits(td, s, 5)[0]) == 0b10001
+    for x in (s, sa, sb, a, b):
+        td.release(x)
+
+
+def case_sel_large(td):
+    """td_sel_from_pred over 5000 rows (five segments: NONE, ALL, MIX) --
+    the bits and total match the BOOL vector (sel.c:128-161)."""
+    import ctypes as C
+    n = 5000
+    m = np.zeros(n, np.bool_)
+    m[1024:2048] = True
+    m[2048:] = (np.arange(n - 2048) % 3) == 0
+    b = td.vec(m)
+    s = td.check(td.lib.td_sel_from_pred(b), "sel_from_pred")
+    assert _sel_total(td, s) == int(m.sum())
+    bits = _sel_bits(td, s, n)
+    got = np.unpackbits(bits.view(np.uint8), bitorder="little")[:n].astype(bool)
+    assert np.array_equal(got, m)
+    flags = np.frombuffer(C.string_at(s + 48, 5), np.uint8)
+    assert flags.tolist() == [0, 1, 2, 2, 2]
+    td.release(s)
+    td.release(b)
+
+
+def case_sel_filter_integration(td):
+    """test_sel.c:94-122 -- SUM(filter(x, x > 25)) over {10..50} = 120."""
+    t = td.table({"x": np.array([10, 20, 30, 40, 50], np.int64)})
+    r = _run(td, t, lambda g: g.op("sum", g.filter(g.scan("x"), g.op("gt", g.scan("x"), g.i64(25)))))
+    assert td.atom_value(r) == 120
+    td.release(r)
+    td.release(t)
+
+
 ALL = [case_comparisons, case_filter_count, case_arithmetic_sum, case_group_sum,
        case_group_affine, case_parallel_group_sum, case_parallel_min_max, case_join_small,
        case_join_large, case_join_asymmetric, case_join_empty, case_join_left_large,
-       case_join_full_large, case_join_skewed, case_join_boundary, case_join_multikey]
+       case_join_full_large, case_join_skewed, case_join_boundary, case_join_multikey,
+       case_sel_from_pred, case_sel_and, case_sel_large, case_sel_filter_integration]

@@ -101,3 +101,51 @@ def test_cancel_racing_queries_never_corrupts(gpu):
     assert np.array_equal(got["region"], want["region"])
     gpu.release(t)
     assert len(outcomes) == 30
+
+
+def _upsert(gpu):
+    L = gpu.lib
+    L.tdg_hash_upsert.restype = C.c_int32
+    L.tdg_hash_upsert.argtypes = [C.c_void_p, C.c_void_p, C.c_uint64, C.c_int32, C.c_void_p, C.c_int64,
+                                  C.c_int32, C.c_void_p, C.c_void_p, C.c_void_p]
+    return L.tdg_hash_upsert
+
+
+def test_hash_wait_limit_returns_error(gpu):
+    """A slot left in state 1 ("being written") by a writer that never
+    publishes: the readers give up after their poll limit and the call
+    returns TD_ERR_IO instead of hanging.  The table is seeded on the host
+    with every slot in state 1, so each key's first probe meets one; the
+    same context then serves a normal upsert."""
+    import torch
+    TD_ERR_IO = 8
+    up = _upsert(gpu)
+    dev = torch.device("cuda", int(__import__("os").environ.get("TD_GPU_DEVICE", "0")))
+    cap, n = 64, 100
+    kv = torch.arange(n, dtype=torch.int64, device=dev) * 7919
+    keys = torch.zeros(cap, dtype=torch.int64, device=dev)
+    slot = torch.empty(n, dtype=torch.int64, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    state = torch.ones(cap, dtype=torch.int32, device=dev)
+    torch.cuda.synchronize()
+    st = up(state.data_ptr(), keys.data_ptr(), cap, 1, kv.data_ptr(), n, 1000, slot.data_ptr(), err.data_ptr(),
+            None)
+    assert st == TD_ERR_IO
+    assert (slot.cpu() == -1).all()
+    # the context still works: an empty table takes every key, each once
+    state.zero_()
+    cap2 = 256
+    state2 = torch.zeros(cap2, dtype=torch.int32, device=dev)
+    keys2 = torch.zeros(cap2, dtype=torch.int64, device=dev)
+    torch.cuda.synchronize()
+    st = up(state2.data_ptr(), keys2.data_ptr(), cap2, 1, kv.data_ptr(), n, 0, slot.data_ptr(), err.data_ptr(),
+            None)
+    assert st == 0
+    s = slot.cpu().numpy()
+    assert (s >= 0).all() and len(np.unique(s)) == n
+    assert np.array_equal(np.sort(keys2.cpu().numpy()[s]), np.sort(kv.cpu().numpy()))
+    assert (state2.cpu().numpy()[s] == 2).all()
+    # a full table reports TD_ERR_RANGE
+    st = up(state2.data_ptr(), keys2.data_ptr(), 64, 1, (kv + 1).data_ptr(), n, 0, slot.data_ptr(),
+            err.data_ptr(), None)
+    assert st == 3                                  # TD_ERR_RANGE
