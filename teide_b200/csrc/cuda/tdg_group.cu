@@ -609,6 +609,32 @@ __global__ void __launch_bounds__(kThreads) k_payload_build(const GroupK G, cons
     }
 }
 
+// The 16-bit map (group slots below 0xFFFF): each key's entry is a plain
+// 2-byte store, and a bitmap over the key range -- one native 32-bit
+// atomicOr per key, an eighth of a byte per slot -- finds a repeated build
+// key (two rows setting the same bit).  Half the map bytes of the 32-bit
+// form, so twice the keys per L2 sector during the probe.
+__global__ void __launch_bounds__(kThreads) k_payload_build16(const GroupK G, const JoinK J, uint16_t* map,
+                                                              uint32_t* seen, int64_t n_right, int32_t* dup) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_right;
+         r += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t k = ld_i(J.rkeys[0], r) - J.kmin;
+        if (k < 0 || k >= J.n_slots) { set_err(G.err, E_DOMAIN); continue; }
+        int64_t s = 0;
+        bool ok = true;
+        for (int kk = 0; kk < G.nk; kk++) {
+            if (!G.key[kk].side) continue;
+            const int64_t d = ld_i(G.key[kk], r) - G.kmin[kk];
+            ok = ok && d >= 0 && d < G.krange[kk];
+            s += d * G.stride[kk];
+        }
+        if (!ok) { set_err(G.err, E_DOMAIN); continue; }
+        const uint32_t bit = 1u << (k & 31);
+        if (atomicOr(seen + (k >> 5), bit) & bit) atomicExch(dup, 1);
+        map[k] = (uint16_t)s;
+    }
+}
+
 template <int PK, bool SMEM, typename PT, bool W8>
 __global__ void __launch_bounds__(kThreads, TDG_MINB) k_payload_probe(const GroupK G, const Pred P, const tdg_expr prog,
                                                             const tdg_col lkey, int64_t kmin, int64_t n_map,
@@ -727,10 +753,30 @@ __device__ __forceinline__ long long vec_pick(const long long (&cv)[NC > 0 ? NC 
 // map, whose entry is the slot; otherwise slot = key - key_min.  MODE 0:
 // every slot has shared-memory accumulators; MODE 1: hot slots do, the rest
 // update the global records.
-template <int NT, int NC, int MODE, bool MAP>
+// A payload-map entry, read through L2 with the evict-last policy `pol`:
+// the map is the one structure the probe re-reads, so the streamed columns
+// (evict-first) should leave before it does.
+__device__ __forceinline__ uint32_t ld_map(const uint32_t* p, uint64_t pol) {
+    uint32_t v;
+    asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ uint32_t ld_map(const uint16_t* p, uint64_t pol) {
+    unsigned short v;
+    asm volatile("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
+    return v;
+}
+__device__ __forceinline__ uint64_t evict_last_policy() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+template <int NT, int NC, int MODE, bool MAP, typename PT = uint32_t>
 __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, const Pred& P, const VecAgg& A,
                                          const tdg_col& kcol, int64_t kmin, int64_t n_map,
-                                         const uint32_t* __restrict__ map, int64_t n, int64_t base) {
+                                         const PT* __restrict__ map, int64_t n, int64_t base,
+                                         uint64_t pol = 0) {
     int64_t row[4];
     long long fk[4], cv[NC > 0 ? NC : 1][4];
 #pragma unroll
@@ -764,8 +810,8 @@ __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, con
         const int64_t k = fk[i] - kmin;
         if (MAP) {
             const bool in = m && k >= 0 && k < n_map;
-            const uint32_t pl = in ? __ldg(map + k) : 0xFFFFFFFFu;
-            ok[i] = pl != 0xFFFFFFFFu;
+            const uint32_t pl = in ? ld_map(map + k, pol) : (uint32_t)Empty<PT>::v;
+            ok[i] = pl != (uint32_t)Empty<PT>::v;
             slot[i] = pl;
         } else {
             const bool in = k >= 0 && k < n_map;
@@ -890,17 +936,18 @@ __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, con
     }
 }
 
-template <int NT, int NC>
+template <int NT, int NC, typename PT>
 __global__ void __launch_bounds__(kThreads, TDG_MINB) k_probe_vec(const GroupK G, const Pred P, const VecAgg A,
                                                                   const tdg_col lkey, int64_t kmin, int64_t n_map,
-                                                                  const uint32_t* __restrict__ map, int64_t n) {
+                                                                  const PT* __restrict__ map, int64_t n) {
     extern __shared__ unsigned long long sm[];
     const SmemView V = smem_setup<0>(G, sm);
+    const uint64_t pol = evict_last_policy();
     const int64_t tile = (int64_t)kThreads * 4;
     for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
         const int64_t nb = base + (int64_t)gridDim.x * tile;
         prefetch_rows(G.pf, nb, nb + tile < n ? nb + tile : n);
-        vec_tile<NT, NC, 0, true>(G, V, P, A, lkey, kmin, n_map, map, n, base);
+        vec_tile<NT, NC, 0, true, PT>(G, V, P, A, lkey, kmin, n_map, map, n, base, pol);
     }
     smem_flush<0>(G, V);
 }
@@ -918,7 +965,7 @@ k_group_vec(const GroupK G, const Pred P, const VecAgg A, int64_t n) {
     for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
         const int64_t nb = base + (int64_t)gridDim.x * tile;
         prefetch_rows(G.pf, nb, nb + tile < n ? nb + tile : n);
-        vec_tile<NT, NC, MODE, false>(G, V, P, A, G.key[0], G.kmin[0], G.krange[0], nullptr, n, base);
+        vec_tile<NT, NC, MODE, false>(G, V, P, A, G.key[0], G.kmin[0], G.krange[0], (const uint32_t*)nullptr, n, base);
     }
     if (MODE == 0 || V.n_hot) smem_flush<MODE>(G, V);
 }
@@ -1830,15 +1877,24 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     G.hot_cap = 0;
     tdg_status st = prepare(G, s);
     if (st) return st;
-    // 32-bit entries: the build's atomicCAS is native (a 16-bit CAS is a loop
-    // on the containing word), and 4 bytes per key still keeps a 10M-row
-    // build side's map (40 MB) in L2.
-    const bool narrow = false;
+    // 16-bit entries when every group slot fits below the EMPTY value: the
+    // map is half the size (a 10M-key build side: 20 MB instead of 40 MB),
+    // and the key bitmap that detects repeated keys sits in head[]'s second
+    // half (head holds 4 bytes per key slot).  Otherwise 32-bit entries with
+    // a native atomicCAS.
+    const bool narrow = p->n_slots < 0xFFFF;
     void* map = J->head;
+    // 2n bytes of map, 16-byte aligned, then ceil(n / 32) words: within the 4n
+    // bytes (at least 256) that head[] holds for every n >= 1
+    uint32_t* seen = (uint32_t*)((char*)J->head + (((size_t)J->n_slots * 2 + 15) & ~(size_t)15));
     cudaMemsetAsync(map, 0xFF, (size_t)J->n_slots * (narrow ? 2 : 4), s);
+    if (narrow) cudaMemsetAsync(seen, 0, (((size_t)J->n_slots + 31) / 32) * 4, s);
     EventTimer tb;
     tb.start(s);
-    if (n_right > 0) {
+    if (n_right > 0 && narrow) {
+        const int g = grid_for((const void*)k_payload_build16, kThreads, 0, n_right);
+        (note_launch(), k_payload_build16<<<g, kThreads, 0, s>>>(G, *J, (uint16_t*)map, seen, n_right, G.err + 1));
+    } else if (n_right > 0) {
         const int g = grid_for((const void*)k_payload_build<uint32_t>, kThreads, 0, n_right);
         (note_launch(), k_payload_build<uint32_t><<<g, kThreads, 0, s>>>(G, *J, (uint32_t*)map, n_right, G.err + 1));
     }
@@ -1865,14 +1921,17 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     for (int k = 0; k < G.nk && vec; k++) vec = G.key[k].side == 1;
     vec = vec && vec_plan(G, pk, P, A, &nt, &nc);
     bool launched = false;
-#define TDG_PV(NTV, NCV)                                                                                  \
-    if (vec && !launched && nt == NTV && nc == NCV) {                                                     \
-        const int g = grid_for((const void*)k_probe_vec<NTV, NCV>, kThreads, smem, (n_left + 3) / 4);    \
-        (note_launch(), k_probe_vec<NTV, NCV><<<g, kThreads, smem, s>>>(G, P, A, J->lkeys[0], J->kmin,    \
-                                                                         J->n_slots, (const uint32_t*)map, n_left)); \
+#define TDG_PV(NTV, NCV, PT)                                                                              \
+    if (vec && !launched && nt == NTV && nc == NCV && narrow == (sizeof(PT) == 2)) {                      \
+        const int g = grid_for((const void*)k_probe_vec<NTV, NCV, PT>, kThreads, smem, (n_left + 3) / 4); \
+        (note_launch(), k_probe_vec<NTV, NCV, PT><<<g, kThreads, smem, s>>>(G, P, A, J->lkeys[0], J->kmin, \
+                                                                             J->n_slots, (const PT*)map, n_left)); \
         launched = true;                                                                                  \
     }
-    TDG_PV(0, 0) TDG_PV(0, 1) TDG_PV(0, 2) TDG_PV(1, 1) TDG_PV(1, 2) TDG_PV(2, 1) TDG_PV(2, 2)
+    TDG_PV(0, 0, uint16_t) TDG_PV(0, 1, uint16_t) TDG_PV(0, 2, uint16_t) TDG_PV(1, 1, uint16_t)
+    TDG_PV(1, 2, uint16_t) TDG_PV(2, 1, uint16_t) TDG_PV(2, 2, uint16_t)
+    TDG_PV(0, 0, uint32_t) TDG_PV(0, 1, uint32_t) TDG_PV(0, 2, uint32_t) TDG_PV(1, 1, uint32_t)
+    TDG_PV(1, 2, uint32_t) TDG_PV(2, 1, uint32_t) TDG_PV(2, 2, uint32_t)
 #undef TDG_PV
 #define TDG_PL(PKV, SMV, PT, W)                                                                         \
     if (!launched && pk == PKV && sm == SMV && narrow == (sizeof(PT) == 2) && w8 == W) {                \
@@ -1886,6 +1945,11 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     TDG_PL(0, true, uint32_t, false) TDG_PL(0, false, uint32_t, false)
     TDG_PL(1, true, uint32_t, false) TDG_PL(1, false, uint32_t, false)
     TDG_PL(2, true, uint32_t, false) TDG_PL(2, false, uint32_t, false)
+    TDG_PL(0, true, uint16_t, true) TDG_PL(0, false, uint16_t, true)
+    TDG_PL(1, true, uint16_t, true) TDG_PL(1, false, uint16_t, true)
+    TDG_PL(0, true, uint16_t, false) TDG_PL(0, false, uint16_t, false)
+    TDG_PL(1, true, uint16_t, false) TDG_PL(1, false, uint16_t, false)
+    TDG_PL(2, true, uint16_t, false) TDG_PL(2, false, uint16_t, false)
 #undef TDG_PL
     tm.stop(s);
     st = launch_status();
