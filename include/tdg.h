@@ -207,9 +207,15 @@ typedef struct tdg_join_desc {
     tdg_col rkeys[TDG_MAX_KEYS];
     /* single integer key statistics of the build side (enables a direct map) */
     int32_t have_range;
-    int32_t pad;
+    int32_t flags;         /* TDG_JOIN_PREBUILT, or 0 */
     int64_t rkey_min, rkey_max;
 } tdg_join_desc;
+
+/* tdg_join_desc.flags: the join workspace already holds this build side's
+ * payload map, made by tdg_join_payload_build for the same join and group
+ * descriptors.  tdg_join_group_run then reads the map and writes nothing to
+ * the join workspace, so concurrent runs may share one. */
+#define TDG_JOIN_PREBUILT 1
 
 enum { TDG_JOIN_DIRECT = 1, TDG_JOIN_HASH = 2 };
 
@@ -271,6 +277,19 @@ tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_plan* jplan
 tdg_status tdg_hash_upsert(uint32_t* state, int64_t* keys, uint64_t cap, int32_t n_keys,
                            const int64_t* kv, int64_t n, int32_t spin_limit, int64_t* d_slot,
                            int32_t* d_err, void* stream);
+
+/* The build pass of the fused join -> group-by, on its own: when the shape
+ * qualifies for the payload map (unique dense integer build keys, a direct
+ * group-by fed by probe-side values -- the case tdg_join_group_run probes
+ * with one 4-byte map read per row), writes the map into jws and sets *used
+ * to 1; otherwise (or when a build key repeats) sets *used to 0.  A caller
+ * that keeps jws may then run any number of probes against it with
+ * TDG_JOIN_PREBUILT -- a server answering many join queries over one
+ * resident build table builds it once.  Synchronizes the stream.  The map
+ * is the build half of join_radix_build_probe_fn (exec.c:7824-7950). */
+tdg_status tdg_join_payload_build(const tdg_join_desc* d, const tdg_join_plan* jp, void* jws,
+                                  const tdg_group_desc* g, const tdg_group_plan* gp, int32_t* used,
+                                  void* stream);
 
 /* ---- sort ------------------------------------------------------------------------
  * tdg_sort_perm: the stable permutation that orders n rows by keys[0..n_keys)

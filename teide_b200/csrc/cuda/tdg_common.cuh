@@ -294,6 +294,49 @@ __device__ inline int block_excl_scan(int v, int* total, int* scratch) {
     return warp_off + x - v;
 }
 
+// ---- shared-memory rings fed by bulk copies ----------------------------------------
+// A producer thread copies column chunks from global memory into a ring of
+// shared-memory stages with cp.async.bulk (the copy engine moves the bytes;
+// no registers, no thread waits on DRAM), each stage guarded by two
+// mbarriers: `full` completes when the stage's bytes have landed (the
+// producer's arrive.expect_tx plus the copies' complete_tx), `empty` when
+// every consumer warp has finished reading it.  Every wait is bounded: a
+// wait that runs out returns false and the kernel records an error instead
+// of hanging.  Plain (non-multicast) copies from this GPU's own memory only.
+__device__ __forceinline__ uint32_t sh_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(sh_addr(bar)), "r"(count) : "memory");
+}
+// Makes the initialized barriers visible to the copy engine (async proxy).
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(sh_addr(bar)) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(sh_addr(bar)), "r"(bytes) : "memory");
+}
+// Waits for the phase of parity `parity` to complete; false after `limit` polls.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+    const uint32_t a = sh_addr(bar);
+    for (uint32_t i = 0; i < limit; i++) {
+        uint32_t done;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}" : "=r"(done) : "r"(a), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+// bytes from global `src` to this CTA's shared `dst`, completing on `bar`.
+// src, dst and bytes must be multiples of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(sh_addr(dst)), "l"(src), "r"(bytes), "r"(sh_addr(bar)) : "memory");
+}
+constexpr uint32_t kWaitLimit = 1u << 22;    // polls of one bounded mbarrier wait
+
 // ---- L2 prefetch of streamed column ranges ------------------------------------------
 // cp.async.bulk.prefetch.L2 asks the copy engine to pull a contiguous range
 // into L2 without registers, shared memory or a completion wait, so a CTA can

@@ -585,7 +585,6 @@ __global__ void __launch_bounds__(kThreads) k_select_hot(const GroupK G) {
 // is a 40 MB map that stays in L2 -- instead of the head[] lookup plus the
 // build-column gather.
 template <typename PT> struct Empty;
-template <> struct Empty<uint16_t> { static constexpr uint16_t v = 0xFFFF; };
 template <> struct Empty<uint32_t> { static constexpr uint32_t v = 0xFFFFFFFFu; };
 
 template <typename PT>
@@ -609,29 +608,57 @@ __global__ void __launch_bounds__(kThreads) k_payload_build(const GroupK G, cons
     }
 }
 
-// The 16-bit map (group slots below 0xFFFF): each key's entry is a plain
-// 2-byte store, and a bitmap over the key range -- one native 32-bit
-// atomicOr per key, an eighth of a byte per slot -- finds a repeated build
-// key (two rows setting the same bit).  Half the map bytes of the 32-bit
-// form, so twice the keys per L2 sector during the probe.
-__global__ void __launch_bounds__(kThreads) k_payload_build16(const GroupK G, const JoinK J, uint16_t* map,
-                                                              uint32_t* seen, int64_t n_right, int32_t* dup) {
-    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n_right;
-         r += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t k = ld_i(J.rkeys[0], r) - J.kmin;
-        if (k < 0 || k >= J.n_slots) { set_err(G.err, E_DOMAIN); continue; }
-        int64_t s = 0;
-        bool ok = true;
-        for (int kk = 0; kk < G.nk; kk++) {
-            if (!G.key[kk].side) continue;
-            const int64_t d = ld_i(G.key[kk], r) - G.kmin[kk];
-            ok = ok && d >= 0 && d < G.krange[kk];
-            s += d * G.stride[kk];
+// The common build shape -- an 8-byte join key and one 8-byte group key on
+// the build side, both 16-byte aligned -- four rows per thread: two 16-byte
+// loads per column, then four independent CASes in flight at once.
+__global__ void __launch_bounds__(kThreads) k_payload_build_vec(const long long* __restrict__ jk,
+                                                                const long long* __restrict__ gk, int64_t jmin,
+                                                                int64_t n_slots, int64_t gmin, int64_t grange,
+                                                                int64_t gstride, uint32_t* map, int64_t n,
+                                                                int32_t* err, int32_t* dup) {
+    const int64_t step = (int64_t)gridDim.x * blockDim.x * 4;
+    for (int64_t r0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4; r0 < n; r0 += step) {
+        long long k[4], g[4];
+        if (r0 + 3 < n) {
+            const longlong2 a = __ldcs((const longlong2*)(jk + r0)), b = __ldcs((const longlong2*)(jk + r0 + 2));
+            const longlong2 c = __ldcs((const longlong2*)(gk + r0)), d = __ldcs((const longlong2*)(gk + r0 + 2));
+            k[0] = a.x; k[1] = a.y; k[2] = b.x; k[3] = b.y;
+            g[0] = c.x; g[1] = c.y; g[2] = d.x; g[3] = d.y;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                k[i] = r0 + i < n ? jk[r0 + i] : 0;
+                g[i] = r0 + i < n ? gk[r0 + i] : 0;
+            }
         }
-        if (!ok) { set_err(G.err, E_DOMAIN); continue; }
-        const uint32_t bit = 1u << (k & 31);
-        if (atomicOr(seen + (k >> 5), bit) & bit) atomicExch(dup, 1);
-        map[k] = (uint16_t)s;
+        uint32_t old[4];
+        bool on[4];
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+            const int64_t kk = k[i] - jmin, d = g[i] - gmin;
+            on[i] = r0 + i < n;
+            if (on[i] && (kk < 0 || kk >= n_slots || d < 0 || d >= grange)) { set_err(err, E_DOMAIN); on[i] = false; }
+            old[i] = on[i] ? atomicCAS(map + kk, 0xFFFFFFFFu, (uint32_t)(d * gstride)) : 0xFFFFFFFFu;
+        }
+        if ((old[0] & old[1] & old[2] & old[3]) != 0xFFFFFFFFu) atomicExch(dup, 1);
+    }
+}
+
+static void launch_payload_build(const GroupK& G, const JoinK& J, uint32_t* map, int64_t n_right, cudaStream_t s) {
+    int gi = -1, nb = 0;
+    for (int k = 0; k < G.nk; k++)
+        if (G.key[k].side) { gi = k; nb++; }
+    const bool vec = nb == 1 && J.nk == 1 && elem_size(J.rkeys[0].type, J.rkeys[0].attrs) == 8 &&
+                     J.rkeys[0].type != T_F64 && elem_size(G.key[gi].type, G.key[gi].attrs) == 8 &&
+                     (((uintptr_t)J.rkeys[0].data | (uintptr_t)G.key[gi].data) & 15) == 0;
+    if (vec) {
+        const int g = grid_for((const void*)k_payload_build_vec, kThreads, 0, (n_right + 3) / 4);
+        (note_launch(), k_payload_build_vec<<<g, kThreads, 0, s>>>(
+            (const long long*)J.rkeys[0].data, (const long long*)G.key[gi].data, J.kmin, J.n_slots, G.kmin[gi],
+            G.krange[gi], G.stride[gi], map, n_right, G.err, G.err + 1));
+    } else {
+        const int g = grid_for((const void*)k_payload_build<uint32_t>, kThreads, 0, n_right);
+        (note_launch(), k_payload_build<uint32_t><<<g, kThreads, 0, s>>>(G, J, map, n_right, G.err + 1));
     }
 }
 
@@ -716,7 +743,6 @@ __device__ __forceinline__ void ld_pair(const tdg_col& c, int64_t r, int64_t n, 
 
 // Reductions on the shared window by address: always the shared-memory
 // atomic unit, whatever the compiler can prove about a pointer.
-__device__ __forceinline__ uint32_t sh_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 __device__ __forceinline__ void sh_add_u32(uint32_t a, uint32_t v) {
     asm volatile("red.shared.add.u32 [%0], %1;" :: "r"(a), "r"(v) : "memory");
 }
@@ -761,33 +787,20 @@ __device__ __forceinline__ uint32_t ld_map(const uint32_t* p, uint64_t pol) {
     asm volatile("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
     return v;
 }
-__device__ __forceinline__ uint32_t ld_map(const uint16_t* p, uint64_t pol) {
-    unsigned short v;
-    asm volatile("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(v) : "l"(p), "l"(pol));
-    return v;
-}
 __device__ __forceinline__ uint64_t evict_last_policy() {
     uint64_t pol;
     asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
     return pol;
 }
 
-template <int NT, int NC, int MODE, bool MAP, typename PT = uint32_t>
-__device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, const Pred& P, const VecAgg& A,
-                                         const tdg_col& kcol, int64_t kmin, int64_t n_map,
-                                         const PT* __restrict__ map, int64_t n, int64_t base,
-                                         uint64_t pol = 0) {
-    int64_t row[4];
-    long long fk[4], cv[NC > 0 ? NC : 1][4];
-#pragma unroll
-    for (int j = 0; j < 2; j++) {
-        const int64_t r = base + (int64_t)j * 2 * kThreads + 2 * threadIdx.x;
-        row[2 * j] = r;
-        row[2 * j + 1] = r + 1;
-        ld_pair(kcol, r, n, fk[2 * j], fk[2 * j + 1]);
-#pragma unroll
-        for (int c = 0; c < NC; c++) ld_pair(A.vc[c], r, n, cv[c][2 * j], cv[c][2 * j + 1]);
-    }
+// The four rows of a thread once their key (fk) and value columns (cv) are
+// in registers: predicate, slot, and the aggregate updates.  vec_tile loads
+// them from global memory; the ring kernel from its shared-memory stages.
+template <int NT, int NC, int MODE, bool MAP, typename PT>
+__device__ __forceinline__ void vec_rows(const GroupK& G, const SmemView& V, const Pred& P, const VecAgg& A,
+                                         const int64_t (&row)[4], const long long (&fk)[4],
+                                         const long long (&cv)[NC > 0 ? NC : 1][4], int64_t kmin, int64_t n_map,
+                                         const PT* __restrict__ map, int64_t n, uint64_t pol) {
     int64_t slot[4];
     int hidx[4];
     bool ok[4];
@@ -934,6 +947,25 @@ __device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, con
 #undef TDG_SA
 #undef TDG_GA
     }
+}
+
+template <int NT, int NC, int MODE, bool MAP, typename PT = uint32_t>
+__device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, const Pred& P, const VecAgg& A,
+                                         const tdg_col& kcol, int64_t kmin, int64_t n_map,
+                                         const PT* __restrict__ map, int64_t n, int64_t base,
+                                         uint64_t pol = 0) {
+    int64_t row[4];
+    long long fk[4], cv[NC > 0 ? NC : 1][4];
+#pragma unroll
+    for (int j = 0; j < 2; j++) {
+        const int64_t r = base + (int64_t)j * 2 * kThreads + 2 * threadIdx.x;
+        row[2 * j] = r;
+        row[2 * j + 1] = r + 1;
+        ld_pair(kcol, r, n, fk[2 * j], fk[2 * j + 1]);
+#pragma unroll
+        for (int c = 0; c < NC; c++) ld_pair(A.vc[c], r, n, cv[c][2 * j], cv[c][2 * j + 1]);
+    }
+    vec_rows<NT, NC, MODE, MAP, PT>(G, V, P, A, row, fk, cv, kmin, n_map, map, n, pol);
 }
 
 template <int NT, int NC, typename PT>
@@ -1865,38 +1897,68 @@ static tdg_status dispatch(int pk, const GroupK& G0, bool smem, const Pred& P, c
 // Payload join -> group (see k_payload_build).  Sets *used when it ran; when
 // the shape does not qualify, or the build side turns out to hold duplicate
 // keys, it returns with *used == false and the caller takes the general path.
+// The shapes the payload map serves: a direct inner join on one integer key
+// and a direct group-by whose aggregate inputs all come from the probe side.
+static bool payload_ok(const tdg_group_desc* d, const tdg_group_plan* p, const JoinK* J) {
+    if (J->method != TDG_JOIN_DIRECT || J->join_type != 0 || p->method != TDG_GROUP_DIRECT) return false;
+    if (J->rkeys[0].type == T_F64 || p->n_slots >= 0xFFFFFFFFLL) return false;
+    for (int a = 0; a < d->n_aggs; a++)
+        if (d->aggs[a].op != A_COUNT && d->aggs[a].in.side != 0) return false;
+    return true;
+}
+
+// The payload map's build pass into J->head: errors and the repeated-key
+// flag land in err[0] and err[1] (zeroed here).
+static tdg_status payload_build(const GroupK& G0, const JoinK* J, int32_t* err, int64_t n_right, cudaStream_t s) {
+    GroupK G = G0;
+    G.err = err;
+    cudaMemsetAsync(err, 0, 8, s);
+    cudaMemsetAsync(J->head, 0xFF, (size_t)J->n_slots * 4, s);
+    if (n_right > 0) launch_payload_build(G, *J, (uint32_t*)J->head, n_right, s);
+    return launch_status();
+}
+
+tdg_status join_payload_build(const tdg_group_desc* d, const tdg_group_plan* p, const JoinK* J, int32_t* err,
+                              int64_t n_right, cudaStream_t s, int32_t* used) {
+    *used = 0;
+    if (!payload_ok(d, p, J)) return E_OK;
+    GroupK G = make_gk(d, p, err, d->nrows);          // only the key fields are read
+    tdg_status st = payload_build(G, J, err, n_right, s);
+    if (st) return st;
+    int32_t* w = pinned_words();
+    int32_t local[2] = {0, 0};
+    int32_t* dst = w ? w : local;
+    if (cudaMemcpyAsync(dst, err, 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaGetLastError();
+        return E_IO;
+    }
+    if (dst[0]) return dst[0];
+    *used = dst[1] ? 0 : 1;
+    return E_OK;
+}
+
 tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, void* ws,
                              const tdg_expr* pred, const uint64_t* sel, const JoinK* J, int64_t n_left,
-                             int64_t n_right, const tdg_group_out* out, cudaStream_t s, bool* used) {
+                             int64_t n_right, const tdg_group_out* out, cudaStream_t s, bool* used,
+                             bool prebuilt) {
     *used = false;
-    if (J->method != TDG_JOIN_DIRECT || J->join_type != 0 || p->method != TDG_GROUP_DIRECT) return E_OK;
-    if (J->rkeys[0].type == T_F64 || p->n_slots >= 0xFFFFFFFFLL) return E_OK;
-    for (int a = 0; a < d->n_aggs; a++)
-        if (d->aggs[a].op != A_COUNT && d->aggs[a].in.side != 0) return E_OK;
+    if (!payload_ok(d, p, J)) return prebuilt ? E_RANGE : E_OK;
     GroupK G = make_gk(d, p, ws, d->nrows);
     G.hot_cap = 0;
     tdg_status st = prepare(G, s);
     if (st) return st;
-    // 16-bit entries when every group slot fits below the EMPTY value: the
-    // map is half the size (a 10M-key build side: 20 MB instead of 40 MB),
-    // and the key bitmap that detects repeated keys sits in head[]'s second
-    // half (head holds 4 bytes per key slot).  Otherwise 32-bit entries with
-    // a native atomicCAS.
-    const bool narrow = p->n_slots < 0xFFFF;
+    // 32-bit entries: a native atomicCAS per build key both stores the slot
+    // and detects a repeated key, and 4 bytes per key keeps a 10M-row build
+    // side's map (40 MB) in L2.  (A 16-bit map with plain stores and a
+    // duplicate bitmap measured slower on both passes.)  A prebuilt map was
+    // checked for repeated keys when it was built.
     void* map = J->head;
-    // 2n bytes of map, 16-byte aligned, then ceil(n / 32) words: within the 4n
-    // bytes (at least 256) that head[] holds for every n >= 1
-    uint32_t* seen = (uint32_t*)((char*)J->head + (((size_t)J->n_slots * 2 + 15) & ~(size_t)15));
-    cudaMemsetAsync(map, 0xFF, (size_t)J->n_slots * (narrow ? 2 : 4), s);
-    if (narrow) cudaMemsetAsync(seen, 0, (((size_t)J->n_slots + 31) / 32) * 4, s);
     EventTimer tb;
     tb.start(s);
-    if (n_right > 0 && narrow) {
-        const int g = grid_for((const void*)k_payload_build16, kThreads, 0, n_right);
-        (note_launch(), k_payload_build16<<<g, kThreads, 0, s>>>(G, *J, (uint16_t*)map, seen, n_right, G.err + 1));
-    } else if (n_right > 0) {
-        const int g = grid_for((const void*)k_payload_build<uint32_t>, kThreads, 0, n_right);
-        (note_launch(), k_payload_build<uint32_t><<<g, kThreads, 0, s>>>(G, *J, (uint32_t*)map, n_right, G.err + 1));
+    if (!prebuilt) {
+        cudaMemsetAsync(map, 0xFF, (size_t)J->n_slots * 4, s);
+        if (n_right > 0) launch_payload_build(G, *J, (uint32_t*)map, n_right, s);
     }
     tb.stop(s);
     st = launch_status();
@@ -1921,20 +1983,17 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     for (int k = 0; k < G.nk && vec; k++) vec = G.key[k].side == 1;
     vec = vec && vec_plan(G, pk, P, A, &nt, &nc);
     bool launched = false;
-#define TDG_PV(NTV, NCV, PT)                                                                              \
-    if (vec && !launched && nt == NTV && nc == NCV && narrow == (sizeof(PT) == 2)) {                      \
-        const int g = grid_for((const void*)k_probe_vec<NTV, NCV, PT>, kThreads, smem, (n_left + 3) / 4); \
-        (note_launch(), k_probe_vec<NTV, NCV, PT><<<g, kThreads, smem, s>>>(G, P, A, J->lkeys[0], J->kmin, \
-                                                                             J->n_slots, (const PT*)map, n_left)); \
+#define TDG_PV(NTV, NCV)                                                                                  \
+    if (vec && !launched && nt == NTV && nc == NCV) {                                                     \
+        const int g = grid_for((const void*)k_probe_vec<NTV, NCV, uint32_t>, kThreads, smem, (n_left + 3) / 4); \
+        (note_launch(), k_probe_vec<NTV, NCV, uint32_t><<<g, kThreads, smem, s>>>(G, P, A, J->lkeys[0], J->kmin, \
+                                                                                  J->n_slots, (const uint32_t*)map, n_left)); \
         launched = true;                                                                                  \
     }
-    TDG_PV(0, 0, uint16_t) TDG_PV(0, 1, uint16_t) TDG_PV(0, 2, uint16_t) TDG_PV(1, 1, uint16_t)
-    TDG_PV(1, 2, uint16_t) TDG_PV(2, 1, uint16_t) TDG_PV(2, 2, uint16_t)
-    TDG_PV(0, 0, uint32_t) TDG_PV(0, 1, uint32_t) TDG_PV(0, 2, uint32_t) TDG_PV(1, 1, uint32_t)
-    TDG_PV(1, 2, uint32_t) TDG_PV(2, 1, uint32_t) TDG_PV(2, 2, uint32_t)
+    TDG_PV(0, 0) TDG_PV(0, 1) TDG_PV(0, 2) TDG_PV(1, 1) TDG_PV(1, 2) TDG_PV(2, 1) TDG_PV(2, 2)
 #undef TDG_PV
 #define TDG_PL(PKV, SMV, PT, W)                                                                         \
-    if (!launched && pk == PKV && sm == SMV && narrow == (sizeof(PT) == 2) && w8 == W) {                \
+    if (!launched && pk == PKV && sm == SMV && w8 == W) {                                                \
         const int g = grid_for((const void*)k_payload_probe<PKV, SMV, PT, W>, kThreads, smem,            \
                                (n_left + kItems - 1) / kItems);                                          \
         (note_launch(), k_payload_probe<PKV, SMV, PT, W><<<g, kThreads, smem, s>>>(                      \
@@ -1945,11 +2004,6 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     TDG_PL(0, true, uint32_t, false) TDG_PL(0, false, uint32_t, false)
     TDG_PL(1, true, uint32_t, false) TDG_PL(1, false, uint32_t, false)
     TDG_PL(2, true, uint32_t, false) TDG_PL(2, false, uint32_t, false)
-    TDG_PL(0, true, uint16_t, true) TDG_PL(0, false, uint16_t, true)
-    TDG_PL(1, true, uint16_t, true) TDG_PL(1, false, uint16_t, true)
-    TDG_PL(0, true, uint16_t, false) TDG_PL(0, false, uint16_t, false)
-    TDG_PL(1, true, uint16_t, false) TDG_PL(1, false, uint16_t, false)
-    TDG_PL(2, true, uint16_t, false) TDG_PL(2, false, uint16_t, false)
 #undef TDG_PL
     tm.stop(s);
     st = launch_status();

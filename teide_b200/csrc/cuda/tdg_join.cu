@@ -23,7 +23,10 @@ tdg_status group_run_joined(const tdg_group_desc* d, const tdg_group_plan* p, vo
                             int64_t n_right, const tdg_group_out* out, cudaStream_t s);
 tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, void* ws,
                              const tdg_expr* pred, const uint64_t* sel, const JoinK* J, int64_t n_left,
-                             int64_t n_right, const tdg_group_out* out, cudaStream_t s, bool* used);
+                             int64_t n_right, const tdg_group_out* out, cudaStream_t s, bool* used,
+                             bool prebuilt);
+tdg_status join_payload_build(const tdg_group_desc* d, const tdg_group_plan* p, const JoinK* J, int32_t* err,
+                              int64_t n_right, cudaStream_t s, int32_t* used);
 
 constexpr int kJChunk = kThreads * 16;
 constexpr int kMaxJCols = 16;
@@ -390,14 +393,27 @@ extern "C" tdg_status tdg_join_group_run(const tdg_join_desc* d, const tdg_join_
     if (st) return st;
     cudaStream_t s = (cudaStream_t)stream;
     JoinK J = make_jk(d, jp, jws);
-    cudaMemsetAsync(J.ht.err, 0, 256, s);
     bool used = false;
-    st = group_run_payload(g, gp, gws, lpred, lsel, &J, d->n_left, d->n_right, out, s, &used);
+    if (d->flags & TDG_JOIN_PREBUILT)    // the map is in jws; nothing here writes to it
+        return group_run_payload(g, gp, gws, lpred, lsel, &J, d->n_left, d->n_right, out, s, &used, true);
+    cudaMemsetAsync(J.ht.err, 0, 256, s);
+    st = group_run_payload(g, gp, gws, lpred, lsel, &J, d->n_left, d->n_right, out, s, &used, false);
     if (st || used) return st;
     st = tdg_join_build(d, jp, jws, stream);
     if (st) return st;
     if (d->join_type == 2 && d->n_right > 0) cudaMemsetAsync(J.matched, 0, (size_t)d->n_right, s);
     return group_run_joined(g, gp, gws, lpred, lsel, &J, d->n_left, d->n_right, out, s);
+}
+
+extern "C" tdg_status tdg_join_payload_build(const tdg_join_desc* d, const tdg_join_plan* jp, void* jws,
+                                             const tdg_group_desc* g, const tdg_group_plan* gp, int32_t* used,
+                                             void* stream) {
+    if (!d || !jp || !jws || !g || !gp || !used) return E_TYPE;
+    *used = 0;
+    tdg_status st = check_desc(d);
+    if (st) return st;
+    JoinK J = make_jk(d, jp, jws);
+    return join_payload_build(g, gp, &J, J.ht.err, d->n_right, (cudaStream_t)stream, used);
 }
 
 // ---- the hash-table upsert as an entry point --------------------------------------

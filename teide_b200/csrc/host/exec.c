@@ -40,6 +40,7 @@
 
 #include "internal.h"
 #include <math.h>
+#include <pthread.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -477,7 +478,118 @@ typedef struct {
     const tdg_join_desc* jd;
     const tdg_join_plan* jp;
     void*                jws;
+    td_t*                rkey;     /* host build key column (one key), or NULL */
 } jrun_t;
+
+/* ---- shared join builds -------------------------------------------------------------------
+ * A server answers many join queries over the same resident build table; the
+ * payload map of that build side (each build key's group slot) is the same
+ * for all of them.  While this thread's flag is set (td_server's workers set
+ * it), the map is built once by tdg_join_payload_build into a kept workspace
+ * and every later query with the same build key column, key range and group
+ * keys probes it with TDG_JOIN_PREBUILT, concurrently with the others.  An
+ * entry matches only the same resident device copies (tdb_col_stamp: a
+ * column freed, modified or unpinned since gets a new stamp), so a stale map
+ * is never read. */
+#define TDB_BCACHE 8
+typedef struct {
+    int           ready;
+    int           users;                       /* probes in flight */
+    uint64_t      tick;
+    uint64_t      rstamp, gstamp[TDG_MAX_KEYS];
+    int64_t       gmin[TDG_MAX_KEYS], gmax[TDG_MAX_KEYS];
+    int32_t       nk;
+    tdg_join_desc jd;
+    tdg_join_plan jp;
+    void*         jws;
+} bentry_t;
+
+static pthread_mutex_t bc_mu = PTHREAD_MUTEX_INITIALIZER;
+static bentry_t bc[TDB_BCACHE];
+static uint64_t bc_tick;
+static _Thread_local int tls_share_builds;
+
+void tdb_share_builds(int on) { tls_share_builds = on; }
+
+void tdb_build_cache_clear(void) {
+    pthread_mutex_lock(&bc_mu);
+    for (int i = 0; i < TDB_BCACHE; i++) {
+        if (!bc[i].ready || bc[i].users) continue;
+        tdb_dev_free_persistent(bc[i].jws);
+        memset(&bc[i], 0, sizeof(bc[i]));
+    }
+    pthread_mutex_unlock(&bc_mu);
+}
+
+static int bc_match(const bentry_t* e, const jrun_t* jr, const tdg_group_desc* d, const uint64_t* gst,
+                    uint64_t rst) {
+    if (!e->ready || e->rstamp != rst || e->nk != d->n_keys) return 0;
+    if (e->jd.n_right != jr->jd->n_right || e->jd.rkey_min != jr->jd->rkey_min ||
+        e->jd.rkey_max != jr->jd->rkey_max || e->jp.n_slots != jr->jp->n_slots || e->jp.method != jr->jp->method)
+        return 0;
+    for (int k = 0; k < d->n_keys; k++)
+        if (e->gstamp[k] != gst[k] || e->gmin[k] != d->key_min[k] || e->gmax[k] != d->key_max[k]) return 0;
+    return 1;
+}
+
+/* A kept map for this join -> group-by (users counted), building it on a
+ * miss; NULL when sharing does not apply. */
+static bentry_t* bc_acquire(ex_t* x, const jrun_t* jr, const tdg_group_desc* d, const tdg_group_plan* gp,
+                            const gin_t* keys) {
+    if (!tls_share_builds || !jr->rkey || jr->jd->n_keys != 1 || jr->jd->join_type != 0 || !d->have_range) return NULL;
+    const uint64_t rst = tdb_col_stamp(jr->rkey);
+    if (!rst) return NULL;
+    uint64_t gst[TDG_MAX_KEYS];
+    for (int k = 0; k < d->n_keys; k++) {
+        if (d->keys[k].side != 1 || !keys[k].src) return NULL;      /* every group key from the build side */
+        if (!(gst[k] = tdb_col_stamp(keys[k].src))) return NULL;
+    }
+    pthread_mutex_lock(&bc_mu);
+    for (int i = 0; i < TDB_BCACHE; i++) {
+        if (bc_match(&bc[i], jr, d, gst, rst)) {
+            bc[i].users++;
+            bc[i].tick = ++bc_tick;
+            pthread_mutex_unlock(&bc_mu);
+            return &bc[i];
+        }
+    }
+    pthread_mutex_unlock(&bc_mu);
+    void* jws = tdb_dev_alloc_persistent(jr->jp->ws_bytes);
+    if (!jws) return NULL;
+    int32_t used = 0;
+    int st = CALL(tdg_join_payload_build(jr->jd, jr->jp, jws, d, gp, &used, x->c.stream));
+    if (st || !used) { tdb_dev_free_persistent(jws); return NULL; }
+    pthread_mutex_lock(&bc_mu);
+    int slot = -1;
+    for (int i = 0; i < TDB_BCACHE; i++) {
+        if (!bc[i].ready) { slot = i; break; }
+        if (!bc[i].users && (slot < 0 || bc[i].tick < bc[slot].tick)) slot = i;
+    }
+    bentry_t* e = NULL;
+    if (slot >= 0) {
+        e = &bc[slot];
+        if (e->ready) tdb_dev_free_persistent(e->jws);
+        memset(e, 0, sizeof(*e));
+        e->ready = 1;
+        e->users = 1;
+        e->tick = ++bc_tick;
+        e->rstamp = rst;
+        e->nk = d->n_keys;
+        for (int k = 0; k < d->n_keys; k++) { e->gstamp[k] = gst[k]; e->gmin[k] = d->key_min[k]; e->gmax[k] = d->key_max[k]; }
+        e->jd = *jr->jd;
+        e->jp = *jr->jp;
+        e->jws = jws;
+    }
+    pthread_mutex_unlock(&bc_mu);
+    if (!e) tdb_dev_free_persistent(jws);          /* every entry busy: this query builds its own */
+    return e;
+}
+
+static void bc_release(bentry_t* e) {
+    pthread_mutex_lock(&bc_mu);
+    e->users--;
+    pthread_mutex_unlock(&bc_mu);
+}
 
 /* Group-by over `tbl` rows (or over a join's output when js/jr are given). */
 static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pred_in,
@@ -583,7 +695,15 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
     }
     if ((st = tdb_check_cancel())) return TD_ERR_PTR(st);
     if (jr) {
-        st = CALL(tdg_join_group_run(jr->jd, jr->jp, jr->jws, pp, dsel, &d, &plan, ws, &out, x->c.stream));
+        bentry_t* be = bc_acquire(x, jr, &d, &plan, keys);
+        if (be) {
+            tdg_join_desc jd = *jr->jd;
+            jd.flags |= TDG_JOIN_PREBUILT;
+            st = CALL(tdg_join_group_run(&jd, &be->jp, be->jws, pp, dsel, &d, &plan, ws, &out, x->c.stream));
+            bc_release(be);
+        }
+        if (!be || st == TD_ERR_RANGE)      /* no kept map, or this plan cannot use it */
+            st = CALL(tdg_join_group_run(jr->jd, jr->jp, jr->jws, pp, dsel, &d, &plan, ws, &out, x->c.stream));
         tdb_note_methods(plan.method, jr->jp->method, 1);
     } else {
         st = CALL(tdg_group_run(&d, pp, dsel, &plan, ws, &out, x->c.stream));
@@ -677,6 +797,7 @@ typedef struct {
     void* ws;
     td_t* left;      /* host tables (retained by the caller's val_t) */
     td_t* right;
+    td_t* rkey;      /* the build side's (single) key column */
 } jbuilt_t;
 
 /* Right side with a pending filter: compact it on the device first. */
@@ -714,6 +835,7 @@ static int prepare_join(ex_t* x, td_op_ext_t* ext, val_t* lv, td_t* right, jbuil
         if (st) return st;
         d->lkeys[k] = (tdg_col){ dl.dptr, dl.type, dl.attrs, 0, {0} };
         d->rkeys[k] = (tdg_col){ dr.dptr, dr.type, dr.attrs, 1, {0} };
+        if (nk == 1) jb->rkey = rc;
         if (nk == 1 && dr.has_stats && dr.len > 0) {
             d->have_range = 1;
             d->rkey_min = dr.kmin;
@@ -920,7 +1042,7 @@ static td_t* exec_group_node(ex_t* x, td_op_t* op) {
                 res = TD_ERR_PTR(st);
             } else {
                 jsrc_t js = { lv.obj, right, jext };
-                jrun_t jr = { &jb.d, &jb.p, jb.ws };
+                jrun_t jr = { &jb.d, &jb.p, jb.ws, jb.rkey };
                 res = run_group(x, ext, NULL, lv.has_pred ? &lv.pred : NULL, lv.dsel, &js, &jr);
             }
             td_release(right);

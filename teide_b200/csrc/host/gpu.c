@@ -174,7 +174,10 @@ typedef struct {
     uint64_t   serial;
     tdb_devcol dc;
     size_t     bytes;
+    uint64_t   stamp;     /* unique per mirror ever made (tdb_col_stamp) */
 } mirror_t;
+
+static uint64_t mirror_stamps;    /* under mu */
 
 static mirror_t* mirrors; static int n_mir, cap_mir;
 
@@ -647,6 +650,15 @@ int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
     return TD_OK;
 }
 
+uint64_t tdb_col_stamp(td_t* col) {
+    if (!col || TD_IS_ERR(col) || (col->attrs & TD_ATTR_SLICE)) return 0;
+    pthread_mutex_lock(&mu);
+    const int i = find_mirror_locked(col);
+    const uint64_t st = i >= 0 ? mirrors[i].stamp : 0;
+    pthread_mutex_unlock(&mu);
+    return st;
+}
+
 /* Keep a device buffer this call produced as the resident mirror of the host
  * vector it was copied to: a later query over the result reads it from HBM.
  * The buffer leaves the call's transient list; it is freed with the host
@@ -666,7 +678,7 @@ int tdb_adopt_mirror(tdb_ctx* c, td_t* host, void* dptr) {
     tdb_devcol dc;
     memset(&dc, 0, sizeof(dc));
     dc.dptr = dptr; dc.len = host->len; dc.type = host->type; dc.attrs = host->attrs;
-    mirrors[n_mir++] = (mirror_t){ host, tdb_block_serial(host), dc, col_bytes(host) };
+    mirrors[n_mir++] = (mirror_t){ host, tdb_block_serial(host), dc, col_bytes(host), ++mirror_stamps };
     mh_added_locked();
     pthread_mutex_unlock(&mu);
     c->tmp[k] = c->tmp[--c->n_tmp];
@@ -699,7 +711,7 @@ td_err_t td_gpu_pin(td_t* tbl) {
             if (!nm) { pthread_mutex_unlock(&mu); arena_free(dc.dptr); st = TD_ERR_OOM; break; }
             mirrors = nm; cap_mir = ncap;
         }
-        mirrors[n_mir++] = (mirror_t){ col, tdb_block_serial(col), dc, col_bytes(col) };
+        mirrors[n_mir++] = (mirror_t){ col, tdb_block_serial(col), dc, col_bytes(col), ++mirror_stamps };
         mh_added_locked();
         pthread_mutex_unlock(&mu);
     }

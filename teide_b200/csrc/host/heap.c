@@ -44,20 +44,30 @@ static size_t cache_pinned[TDB_CACHE_SLOTS];
 static int cache_n;
 static size_t cache_bytes;
 
-static void* cache_take(size_t raw_size, size_t* pinned) {
+/* The smallest cached block of at least raw_size bytes and at most four
+ * times that (page-locked blocks preferred): query results vary in size from
+ * call to call, and a block one or two size classes up is still far cheaper
+ * than fresh pages that must be faulted in and page-locked again.  *got
+ * receives the block's actual size. */
+static void* cache_take(size_t raw_size, size_t* pinned, size_t* got) {
     void* r = NULL;
     pthread_mutex_lock(&cache_mu);
+    int best = -1;
     for (int i = 0; i < cache_n; i++) {
-        if (cache_size[i] == raw_size) {
-            r = cache_raw[i];
-            *pinned = cache_pinned[i];
-            cache_bytes -= raw_size;
-            cache_n--;
-            cache_raw[i] = cache_raw[cache_n];
-            cache_size[i] = cache_size[cache_n];
-            cache_pinned[i] = cache_pinned[cache_n];
-            break;
-        }
+        if (cache_size[i] < raw_size || cache_size[i] / 4 > raw_size) continue;
+        if (best < 0 || (cache_pinned[i] != 0) > (cache_pinned[best] != 0) ||
+            ((cache_pinned[i] != 0) == (cache_pinned[best] != 0) && cache_size[i] < cache_size[best]))
+            best = i;
+    }
+    if (best >= 0) {
+        r = cache_raw[best];
+        *pinned = cache_pinned[best];
+        *got = cache_size[best];
+        cache_bytes -= cache_size[best];
+        cache_n--;
+        cache_raw[best] = cache_raw[cache_n];
+        cache_size[best] = cache_size[cache_n];
+        cache_pinned[best] = cache_pinned[cache_n];
     }
     pthread_mutex_unlock(&cache_mu);
     return r;
@@ -118,8 +128,10 @@ td_t* td_alloc(size_t data_size) {
     size_t pinned = 0;
     if (block >= TDB_MMAP_MIN) {
         raw_size = (raw_size + 4095) & ~(size_t)4095;
-        raw = cache_take(raw_size, &pinned);
-        if (!raw) {
+        size_t got = 0;
+        raw = cache_take(raw_size, &pinned, &got);
+        if (raw) raw_size = got;
+        else {
             raw = mmap(NULL, raw_size, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
             if (raw == MAP_FAILED) return NULL;
         }

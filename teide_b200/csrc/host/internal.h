@@ -117,5 +117,16 @@ void  tdb_trace_begin(void);
 
 /* 1 when the column (or a slice's parent) has a resident device copy. */
 int   tdb_col_resident(td_t* col);
+/* Identity of a column's resident device copy: unique to that copy (a copy
+ * made again after the column was freed, mutated or unpinned gets a new
+ * one); 0 when the column has none or is a slice. */
+uint64_t tdb_col_stamp(td_t* col);
+
+/* ---- shared join builds (host/exec.c) ----------------------------------------------
+ * While a thread's flag is set, fused join -> group-by queries over resident
+ * build tables reuse one payload map per build side (td_server's workers set
+ * it).  tdb_build_cache_clear frees every kept map. */
+void  tdb_share_builds(int on);
+void  tdb_build_cache_clear(void);
 
 #endif

@@ -136,3 +136,60 @@ def two_graph_group_sorted(td, tbl, pred, keys, aggs, sort_col, desc=True):
     td.release(grp)
     td.release(t2)
     td.release(r)
+
+
+class Prepared:
+    """A query DAG built (and passed through td_optimize) once and executed
+    any number of times, like a prepared statement: each run() is one
+    td_execute of the same graph, whose result is produced and then either
+    returned as {name: numpy array} (as_dict) or released unread."""
+
+    def __init__(self, td, tbl, build, optimize=True):
+        self.td = td
+        self.g = td.graph(tbl)
+        try:
+            root = build(self.g)
+            if optimize:
+                root = td.lib.td_optimize(self.g.g, root) or root
+        except Exception:
+            self.g.free()
+            raise
+        self.root = root
+
+    def run(self, as_dict=False):
+        r = self.td.check(self.td.lib.td_execute(self.g.g, self.root), "execute")
+        return _result(self.td, r, as_dict)
+
+    def free(self):
+        self.g.free()
+
+
+def prepared_readme_group(td, tbl, pred, keys, aggs):
+    """readme_group's DAG, prepared."""
+    def build(g):
+        c, op, k = pred
+        p = g.op(op, g.scan(c), const(g, k))
+        return g.group([g.filter(g.scan(n), p) for n in keys], [a for a, _ in aggs],
+                       [g.filter(g.scan(n), p) for _, n in aggs])
+    return Prepared(td, tbl, build)
+
+
+def prepared_fused_join_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, join_type=0):
+    """fused_join_group's DAG, prepared."""
+    def build(g):
+        c, op, k = pred
+        left = g.filter(g.const_table(probe_t), g.op(op, g.scan(c), const(g, k)))
+        g.join(left, [g.scan(lkey)], g.const_table(build_t), [g.scan(rkey)], join_type)
+        return g.group([g.scan(n) for n in keys], [a for a, _ in aggs], [g.scan(n) for _, n in aggs])
+    return Prepared(td, None, build)
+
+
+def prepared_group_sorted(td, tbl, pred, keys, aggs, sort_col, desc=True):
+    """group_sorted's DAG, prepared."""
+    def build(g):
+        c, op, k = pred
+        p = g.op(op, g.scan(c), const(g, k))
+        grp = g.group([g.filter(g.scan(n), p) for n in keys], [a for a, _ in aggs],
+                      [g.filter(g.scan(n), p) for _, n in aggs])
+        return g.sort(grp, [g.scan(sort_col)], [int(desc)])
+    return Prepared(td, tbl, build)

@@ -51,7 +51,7 @@ class GroupOut(C.Structure):
 class JoinDesc(C.Structure):
     _fields_ = [("n_left", C.c_int64), ("n_right", C.c_int64), ("n_keys", C.c_int32),
                 ("join_type", C.c_int32), ("lkeys", Col * MAX_KEYS), ("rkeys", Col * MAX_KEYS),
-                ("have_range", C.c_int32), ("pad", C.c_int32), ("rkey_min", C.c_int64),
+                ("have_range", C.c_int32), ("flags", C.c_int32), ("rkey_min", C.c_int64),
                 ("rkey_max", C.c_int64)]
 
 
