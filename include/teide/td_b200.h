@@ -47,6 +47,21 @@ void     td_gpu_last_stats(td_gpu_stats_t* out);
 /* Release cached device memory that no resident table uses. */
 void     td_gpu_trim(void);
 
+/* Device address of a column's resident copy (td_gpu_pin, or a result left
+ * on the device), or NULL.  Valid while the column is resident. */
+const void* td_gpu_col_data(td_t* col);
+
+/* td_execute of a group-by whose result stays on the device: the returned
+ * table has the result's columns, names, types and lengths, each resident
+ * (td_gpu_col_data), but their host elements are NOT written until
+ * td_gpu_fetch(tbl) copies them down.  For a consumer that continues on the
+ * GPU -- a partial group-by that crosses NVLink to be merged on another GPU
+ * -- so the rows never cross PCIe.  Roots other than td_group return
+ * TD_ERR_NYI.  No counterpart in Teide. */
+td_t*    td_execute_device(td_graph_t* g, td_op_t* root);
+/* Copy every resident column of tbl (or the vector tbl) to its host elements. */
+td_err_t td_gpu_fetch(td_t* tbl);
+
 /* Run n group-by graphs as one batched GPU launch.  Each graph is a
  * td_group over its bound table with one integer key (td_scan) and
  * aggregates reading one value column (td_scan; COUNT may read anything),

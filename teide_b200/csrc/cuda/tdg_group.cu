@@ -64,13 +64,19 @@ constexpr int64_t kSampleMinRows = (int64_t)1 << 22;
 constexpr int kHotHist = 1024;                // sampled-count histogram buckets (hot threshold)
 // MODE 3 (partitioned cold rows)
 constexpr int64_t kPartMinRows = (int64_t)1 << 20;   // smaller inputs keep MODE 1
-constexpr size_t kPartSmem = 96 * 1024;       // a partition's shared-memory table
+#ifndef TDG_PART_SMEM_KB
+#define TDG_PART_SMEM_KB 96
+#endif
+#ifndef TDG_PART_DENSE
+#define TDG_PART_DENSE 4
+#endif
+constexpr size_t kPartSmem = TDG_PART_SMEM_KB * 1024;       // a partition's shared-memory table
 constexpr int kPartThreads = 512;
 constexpr int64_t kPartItem = 16384;          // entries per aggregation work item
 constexpr int kPartRegions = 1024;            // partitions below this are split into stripes
 constexpr int kPartMaxStripes = 64;
 constexpr uint32_t kPartMargin = 32;          // entries every region holds beyond its estimate
-constexpr int64_t kPartDense = 4;             // entries per slot below which an item skips the table
+constexpr int64_t kPartDense = TDG_PART_DENSE;             // entries per slot below which an item skips the table
 
 enum : int32_t { K_COUNT = 0, K_SUM_I, K_SUM_F, K_MIN_I, K_MAX_I, K_MIN_F, K_MAX_F };
 

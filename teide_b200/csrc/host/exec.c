@@ -1388,10 +1388,11 @@ static td_t* exec_value(ex_t* x, td_op_t* op, val_t* out) {
     return TD_ERR_PTR(TD_ERR_NYI);
 }
 
-td_t* tdb_exec(td_graph_t* g, td_op_t* root) {
+td_t* tdb_exec(td_graph_t* g, td_op_t* root, int dev_only) {
     ex_t x;
     memset(&x, 0, sizeof(x));
     x.g = g;
+    x.dev_only = dev_only;
     tdb_reset_methods();
     int st = tdb_ctx_begin(&x.c);
     if (st) return TD_ERR_PTR(st);
@@ -1413,7 +1414,17 @@ td_t* td_execute(td_graph_t* g, td_op_t* root) {
     if (!g || !root) return TD_ERR_PTR(TD_ERR_NYI);
     atomic_store(&tdb_cancel_flag, 0);
     tdb_trace_begin();
-    td_t* r = tdb_exec(g, root);
+    td_t* r = tdb_exec(g, root, 0);
     tdb_trace("td_execute returns");
+    return r;
+}
+
+td_t* td_execute_device(td_graph_t* g, td_op_t* root) {
+    if (!g || !root) return TD_ERR_PTR(TD_ERR_NYI);
+    if (root->opcode != OP_GROUP) return TD_ERR_PTR(TD_ERR_NYI);
+    atomic_store(&tdb_cancel_flag, 0);
+    tdb_trace_begin();
+    td_t* r = tdb_exec(g, root, 1);
+    tdb_trace("td_execute_device returns");
     return r;
 }

@@ -659,6 +659,31 @@ uint64_t tdb_col_stamp(td_t* col) {
     return st;
 }
 
+const void* td_gpu_col_data(td_t* col) {
+    if (!col || TD_IS_ERR(col) || (col->attrs & TD_ATTR_SLICE)) return NULL;
+    pthread_mutex_lock(&mu);
+    const int i = find_mirror_locked(col);
+    const void* p = i >= 0 ? mirrors[i].dc.dptr : NULL;
+    pthread_mutex_unlock(&mu);
+    return p;
+}
+
+td_err_t td_gpu_fetch(td_t* tbl) {
+    if (!tbl || TD_IS_ERR(tbl)) return TD_ERR_TYPE;
+    tdb_ctx c;
+    int st = tdb_ctx_begin(&c);
+    if (st) return (td_err_t)st;
+    const int64_t nc = tbl->type == TD_TABLE ? td_table_ncols(tbl) : 1;
+    for (int64_t j = 0; j < nc && !st; j++) {
+        td_t* col = tbl->type == TD_TABLE ? td_table_get_col_idx(tbl, j) : tbl;
+        const void* d = td_gpu_col_data(col);
+        if (d) st = tdb_d2h_async(&c, td_data(col), d, col_bytes(col));
+    }
+    if (!st) st = tdb_ctx_sync(&c);
+    tdb_ctx_end(&c);
+    return (td_err_t)st;
+}
+
 /* Keep a device buffer this call produced as the resident mirror of the host
  * vector it was copied to: a later query over the result reads it from HBM.
  * The buffer leaves the call's transient list; it is freed with the host

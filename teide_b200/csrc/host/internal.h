@@ -109,7 +109,7 @@ int      tdb_check_cancel(void);
 extern _Atomic(int) tdb_cancel_flag;
 
 /* ---- executor ------------------------------------------------------------------ */
-td_t* tdb_exec(td_graph_t* g, td_op_t* root);
+td_t* tdb_exec(td_graph_t* g, td_op_t* root, int dev_only);
 /* Phase tracing: with TD_TRACE set in the environment, each call prints the
  * microseconds since this thread's td_execute began and a label to stderr. */
 void  tdb_trace(const char* what);

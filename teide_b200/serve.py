@@ -155,47 +155,76 @@ def release(td, reqs):
 
 
 def run_open_loop(server, reqs, keep=None):
-    """Submit each request at its arrival time (seconds after start) and wait
-    for all.  Returns (latencies_s, makespan_s, results) where results holds
-    the result pointers of the indices in `keep` (others are released)."""
+    """Submit each request at its arrival time (seconds after start) while a
+    second thread waits for the results in order and releases them, as a
+    client consuming answers would (results never pile up on the host).
+    Returns (latencies_s, makespan_s, results) where results holds the result
+    pointers of the indices in `keep` (others are released)."""
+    import threading
     td = server.td
     keep = set(keep or ())
-    tickets = []
+    tickets = [None] * len(reqs)
+    ready = threading.Semaphore(0)
+    lat, ends, results, errors = [0.0] * len(reqs), [0] * len(reqs), {}, []
     t0 = time.monotonic()
-    for r in reqs:
-        delay = t0 + r.arrival - time.monotonic()
-        if delay > 0.0005:
-            time.sleep(delay - 0.0003)
-        while time.monotonic() < t0 + r.arrival:
-            pass
-        tickets.append(server.submit(r.graph, r.root))
-    lat, ends, results = [], [], {}
     start_ns = int(t0 * 1e9)
-    for i, (r, t) in enumerate(zip(reqs, tickets)):
-        res, tm = server.wait(t)
-        if tm.status:
-            raise TdError(tm.status, f"request {i} ({r.kind})")
-        arrival_ns = start_ns + int(r.arrival * 1e9)
-        lat.append((tm.end_ns - min(arrival_ns, tm.submit_ns)) / 1e9)
-        ends.append(tm.end_ns)
-        if i in keep:
-            results[i] = res
-        else:
-            td.release(res)
+
+    def consume():
+        for i, r in enumerate(reqs):
+            ready.acquire()
+            res, tm = server.wait(tickets[i])
+            if tm.status:
+                errors.append(TdError(tm.status, f"request {i} ({r.kind})"))
+                continue
+            arrival_ns = start_ns + int(r.arrival * 1e9)
+            lat[i] = (tm.end_ns - min(arrival_ns, tm.submit_ns)) / 1e9
+            ends[i] = tm.end_ns
+            if i in keep:
+                results[i] = res
+            else:
+                td.release(res)
+
+    waiter = threading.Thread(target=consume, daemon=True)
+    waiter.start()
+    for i, r in enumerate(reqs):
+        delay = t0 + r.arrival - time.monotonic()
+        if delay > 0:
+            time.sleep(delay)          # sleeps, never spins: the consumer needs the interpreter too
+        tickets[i] = server.submit(r.graph, r.root)
+        ready.release()
+    waiter.join()
+    if errors:
+        raise errors[0]
     makespan = (max(ends) - start_ns) / 1e9 if ends else 0.0
     return np.array(lat), makespan, results
 
 
 def run_closed(server, reqs):
-    """Every request submitted at once; returns seconds until the last finished."""
+    """Every request submitted at once (a second thread consumes the results
+    in order as they complete); returns seconds until the last finished."""
+    import threading
     td = server.td
     t0 = time.monotonic_ns()
-    tickets = [server.submit(r.graph, r.root) for r in reqs]
-    end = t0
-    for i, t in enumerate(tickets):
-        res, tm = server.wait(t)
-        if tm.status:
-            raise TdError(tm.status, f"request {i}")
-        td.release(res)
-        end = max(end, tm.end_ns)
-    return (end - t0) / 1e9
+    tickets = []
+    ready = threading.Semaphore(0)
+    end, errors = [t0], []
+
+    def consume():
+        for i in range(len(reqs)):
+            ready.acquire()
+            res, tm = server.wait(tickets[i])
+            if tm.status:
+                errors.append(TdError(tm.status, f"request {i}"))
+                continue
+            td.release(res)
+            end[0] = max(end[0], tm.end_ns)
+
+    waiter = threading.Thread(target=consume, daemon=True)
+    waiter.start()
+    for r in reqs:
+        tickets.append(server.submit(r.graph, r.root))
+        ready.release()
+    waiter.join()
+    if errors:
+        raise errors[0]
+    return (end[0] - t0) / 1e9

@@ -15,12 +15,20 @@ exchange is the merge of partial group results:
                       them, and each owner merges its share; the owners' parts
                       are disjoint and together are the result.
 
-Merged output is in ascending key order (lexicographic over the key
-columns), like the direct-array emit of a single GPU.  The local executor is
-a parameter so the exchange and merge can be exercised on CPU ranks with any
-partial-result provider; the product path passes the td_execute one.
+Partial results never leave the GPUs: each rank's local query runs with
+td_execute_device, so its partial groups stay in device memory and cross only
+NVLink (NCCL), and the merge of the gathered rows is itself a group-by run by
+this library on the device (merge_device: tdg_group_run over the rows).  Only
+the merged result is copied to the host.  Merged output is in ascending key
+order (lexicographic over the key columns), like the direct-array emit of a
+single GPU.  The local executor and the merge are parameters so the exchange
+can be exercised on CPU ranks (gloo) with partial results and a merge from
+the test's oracle; the product path passes the td_execute_device and
+tdg_group_run ones.
 """
 from __future__ import annotations
+
+import ctypes as C
 
 import numpy as np
 import torch
@@ -29,7 +37,6 @@ import torch.distributed as dist
 from .td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
 
 SUFFIX = {OP_SUM: "_sum", OP_COUNT: "_count", OP_AVG: "_mean", OP_MIN: "_min", OP_MAX: "_max"}
-_REDUCE = {OP_SUM: "sum", OP_COUNT: "sum", OP_MIN: "amin", OP_MAX: "amax"}
 
 
 def partial_plan(aggs):
@@ -60,21 +67,66 @@ def _key_hash(keys: torch.Tensor) -> torch.Tensor:
     return h & 0x7FFFFFFFFFFFFFFF
 
 
-def merge(keys: torch.Tensor, vals: list, ops: list):
-    """Rows of partial results (keys (n, nk) int64, vals[i] (n,)) -> one row
-    per distinct key in ascending order, vals merged by ops[i]."""
-    if keys.shape[0] == 0:
+_I64, _F64 = 6, 7
+
+
+def merge_device(td, keys: torch.Tensor, vals: list, ops: list):
+    """The merge of gathered partial rows is itself a group-by: keys (n, nk)
+    int64 on the GPU, vals[i] (n,) int64 or float64, merged by ops[i] --
+    SUM of the partial SUMs and COUNTs, MIN of the MINs, MAX of the MAXs --
+    through the library's own group-by (tdg_group_run) on the device, with
+    the key ranges of the rows so the planner can take a direct array.
+    Returns (unique keys (g, nk), merged vals) on the device, ascending by
+    key (the direct array's order; a hash-method result is sorted after)."""
+    from . import device_abi
+    from .tdg import GroupDesc, GroupOut, GroupPlan, col
+    T = device_abi()
+    n, nk = keys.shape
+    if n == 0:
         return keys, [v[:0] for v in vals]
-    if keys.shape[1] == 0:                      # no group keys: one group
-        uk = keys[:1]
-        inv = torch.zeros(keys.shape[0], dtype=torch.int64, device=keys.device)
-    else:
-        uk, inv = torch.unique(keys, dim=0, sorted=True, return_inverse=True)
-    out = []
-    for v, op in zip(vals, ops):
-        r = torch.zeros(uk.shape[0], dtype=v.dtype, device=v.device)
-        out.append(r.scatter_reduce_(0, inv, v, reduce=_REDUCE[op], include_self=False))
-    return uk, out
+    kcols = [keys[:, j].contiguous() for j in range(nk)]
+    if nk == 0:                                   # no group keys: one group
+        kcols = [torch.zeros(n, dtype=torch.int64, device=keys.device)]
+    vals = [v.contiguous() for v in vals]
+    d = GroupDesc()
+    d.nrows = n
+    d.n_keys = len(kcols)
+    d.n_aggs = len(vals)
+    for j, k in enumerate(kcols):
+        d.keys[j] = col(k.data_ptr(), _I64)
+        lo, hi = torch.aminmax(k)
+        d.key_min[j], d.key_max[j] = int(lo), int(hi)
+    d.have_range = 1
+    for a, (v, op) in enumerate(zip(vals, ops)):
+        d.aggs[a].op = OP_SUM if op == OP_COUNT else op
+        d.aggs[a].in_ = col(v.data_ptr(), _F64 if v.dtype == torch.float64 else _I64)
+    plan = GroupPlan()
+    st = T.tdg_group_plan_make(C.byref(d), 0, C.byref(plan))
+    if st:
+        raise RuntimeError(f"tdg_group_plan_make: {st}")
+    ws = torch.empty(max(int(plan.ws_bytes), 1), dtype=torch.uint8, device=keys.device)
+    o = GroupOut()
+    ok = [torch.empty(max(plan.max_groups, 1), dtype=torch.int64, device=keys.device) for _ in kcols]
+    ov = [torch.empty(max(plan.max_groups, 1), dtype=v.dtype, device=keys.device) for v in vals]
+    for j, b in enumerate(ok):
+        o.keys[j] = b.data_ptr()
+    for a, b in enumerate(ov):
+        o.aggs[a] = b.data_ptr()
+    ng = torch.zeros(1, dtype=torch.int64, device=keys.device)
+    o.d_n_groups = ng.data_ptr()
+    st = T.tdg_group_run(C.byref(d), None, None, C.byref(plan), ws.data_ptr(), C.byref(o),
+                         torch.cuda.current_stream(keys.device).cuda_stream)
+    if st:
+        raise RuntimeError(f"tdg_group_run: {st}")
+    g = int(ng.item())
+    uk = torch.stack([b[:g] for b in ok], 1) if nk else torch.zeros((g, 0), dtype=torch.int64, device=keys.device)
+    mv = [b[:g] for b in ov]
+    if plan.method != 1 and nk:                   # hash method: table order -> ascending keys
+        order = torch.arange(g, device=keys.device)
+        for j in reversed(range(nk)):
+            order = order[torch.argsort(uk[order, j], stable=True)]
+        uk, mv = uk[order], [m[order] for m in mv]
+    return uk, mv
 
 
 def _all_gather_rows(t: torch.Tensor, group=None) -> torch.Tensor:
@@ -107,16 +159,20 @@ def _all_to_all_rows(t: torch.Tensor, dest: torch.Tensor, group=None) -> torch.T
 
 
 def exchange_and_merge(part: dict, key_names, parts, steps, strategy="auto", group=None,
-                       device="cpu", gather_limit=1 << 20):
-    """Merge this rank's partial result `part` ({name: numpy}) with every
-    other rank's.  Returns {name: numpy} with the final columns: the whole
-    result ("gather"), or this rank's disjoint share ("alltoall")."""
+                       device="cuda", gather_limit=1 << 20, merge=None, td=None):
+    """Merge this rank's partial result `part` ({name: tensor on `device`, or
+    numpy}) with every other rank's.  Returns {name: numpy} with the final
+    columns: the whole result ("gather"), or this rank's disjoint share
+    ("alltoall").  `merge(keys, vals, ops)` combines rows of equal keys; by
+    default the library's group-by on the GPU (merge_device)."""
     world = dist.get_world_size(group) if dist.is_initialized() else 1
     pnames = [f"{c}{SUFFIX[op]}" for op, c in parts]
-    keys = torch.stack([torch.as_tensor(np.ascontiguousarray(part[k]), device=device).to(torch.int64)
-                        for k in key_names], 1) if key_names else \
+
+    def t(x):
+        return x if isinstance(x, torch.Tensor) else torch.as_tensor(np.ascontiguousarray(x), device=device)
+    keys = torch.stack([t(part[k]).to(torch.int64) for k in key_names], 1) if key_names else \
         torch.zeros((len(part[pnames[0]]), 0), dtype=torch.int64, device=device)
-    vals = [torch.as_tensor(np.ascontiguousarray(part[n]), device=device) for n in pnames]
+    vals = [t(part[n]) for n in pnames]
     ops = [op for op, _ in parts]
     if world > 1:
         if strategy == "auto":
@@ -137,23 +193,63 @@ def exchange_and_merge(part: dict, key_names, parts, steps, strategy="auto", gro
         keys = words[:, :nk]
         vals = [words[:, nk + i].contiguous().view(torch.float64) if v.dtype == torch.float64
                 else words[:, nk + i].to(v.dtype) for i, v in enumerate(vals)]
-    uk, mv = merge(keys, vals, ops)
+    if merge is None:
+        uk, mv = merge_device(td, keys, vals, ops)
+    else:
+        uk, mv = merge(keys, vals, ops)
     out = {k: uk[:, j].cpu().numpy() for j, k in enumerate(key_names)}
     for s in steps:
         if s[0] == "id":
-            op, col = parts[s[1]]
-            out[f"{col}{SUFFIX[op]}"] = mv[s[1]].cpu().numpy()
+            op, col_ = parts[s[1]]
+            out[f"{col_}{SUFFIX[op]}"] = mv[s[1]].cpu().numpy()
         else:
-            col = parts[s[1]][1]
-            out[f"{col}_mean"] = (mv[s[1]].to(torch.float64) / mv[s[2]].to(torch.float64)).cpu().numpy()
+            col_ = parts[s[1]][1]
+            out[f"{col_}_mean"] = (mv[s[1]].to(torch.float64) / mv[s[2]].to(torch.float64)).cpu().numpy()
     return out
 
 
 # ---- the td_execute local executors ------------------------------------------------
 
+class _DevCol:
+    """A device buffer seen through __cuda_array_interface__ (no copy)."""
+
+    def __init__(self, ptr, n, typestr):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": typestr, "data": (ptr, False),
+                                         "version": 3, "strides": None}
+
+
+def _device_part(td, r):
+    """{name: tensor} viewing the device columns of a td_execute_device
+    result r (kept alive in the dict under "_result"; release it after use)."""
+    L = td.lib
+    L.td_gpu_col_data.restype = C.c_void_p
+    L.td_gpu_col_data.argtypes = [C.c_void_p]
+    out = {"_result": r}
+    for j in range(L.td_table_ncols(r)):
+        c = L.td_table_get_col_idx(r, j)
+        typ, _, n = td.header(c)
+        ptr = L.td_gpu_col_data(c)
+        name = td.sym_name(L.td_table_col_name(r, j))
+        if typ not in (_I64, _F64):
+            raise NotImplementedError("sharded partials: only 8-byte integer and F64 result columns")
+        if not ptr or n == 0:
+            out[name] = torch.zeros(0, dtype=torch.float64 if typ == _F64 else torch.int64, device="cuda")
+            continue
+        out[name] = torch.as_tensor(_DevCol(ptr, n, "<f8" if typ == _F64 else "<i8"), device="cuda")
+    return out
+
+
+def _execute_device(td, g, root):
+    L = td.lib
+    L.td_execute_device.restype = C.c_void_p
+    L.td_execute_device.argtypes = [C.c_void_p, C.c_void_p]
+    return _device_part(td, td.check(L.td_execute_device(g.g, root), "td_execute_device"))
+
+
 def local_group(td, tbl, pred, keys, parts):
-    """Partial group-by of this rank's shard: README form when pred is given
-    (pred = (column, op, constant)), else a plain group graph."""
+    """Partial group-by of this rank's shard, left on its GPU: README form
+    when pred is given (pred = (column, op, constant)), else a plain group
+    graph."""
     from .serve import _const
     g = td.graph(tbl)
     try:
@@ -165,41 +261,48 @@ def local_group(td, tbl, pred, keys, parts):
         else:
             ks = [g.scan(n) for n in keys]
             ins = [g.scan(n) for _, n in parts]
-        r = td.check(td.lib.td_execute(g.g, g.group(ks, [a for a, _ in parts], ins)), "td_execute")
+        return _execute_device(td, g, g.group(ks, [a for a, _ in parts], ins))
     finally:
         g.free()
-    out = td.table_dict(r)
-    td.release(r)
-    return out
 
 
 def local_join_group(td, build_t, probe_t, pred, lkey, rkey, keys, parts):
-    """Partial group-by over join(filter(probe shard), build), one fused graph."""
+    """Partial group-by over join(filter(probe shard), build), one fused
+    graph, left on this rank's GPU."""
     from .serve import _const
     g = td.graph(None)
     try:
         c, op, k = pred
         left = g.filter(g.const_table(probe_t), g.op(op, g.scan(c), _const(g, k)))
         g.join(left, [g.scan(lkey)], g.const_table(build_t), [g.scan(rkey)], 0)
-        root = g.group([g.scan(n) for n in keys], [a for a, _ in parts], [g.scan(n) for _, n in parts])
-        r = td.check(td.lib.td_execute(g.g, root), "td_execute")
+        return _execute_device(td, g, g.group([g.scan(n) for n in keys], [a for a, _ in parts],
+                                              [g.scan(n) for _, n in parts]))
     finally:
         g.free()
-    out = td.table_dict(r)
-    td.release(r)
-    return out
 
 
-def sharded_group(td, tbl, keys, aggs, pred=None, strategy="auto", group=None, device="cuda", local=None):
+def _finish(td, part, run):
+    try:
+        return run()
+    finally:
+        r = part.pop("_result", None) if isinstance(part, dict) else None
+        if r and td is not None:
+            td.release(r)
+
+
+def sharded_group(td, tbl, keys, aggs, pred=None, strategy="auto", group=None, device="cuda", local=None,
+                  merge=None):
     """Filter + group-by of the union of every rank's `tbl` shard."""
     parts, steps = partial_plan(aggs)
     part = (local or local_group)(td, tbl, pred, keys, parts)
-    return exchange_and_merge(part, keys, parts, steps, strategy, group, device)
+    return _finish(td, part, lambda: exchange_and_merge(part, keys, parts, steps, strategy, group, device,
+                                                        merge=merge, td=td))
 
 
 def sharded_join_group(td, build_t, probe_t, pred, lkey, rkey, keys, aggs, strategy="auto", group=None,
-                       device="cuda", local=None):
+                       device="cuda", local=None, merge=None):
     """Filter + join + group-by: probe rows sharded, build side on every rank."""
     parts, steps = partial_plan(aggs)
     part = (local or local_join_group)(td, build_t, probe_t, pred, lkey, rkey, keys, parts)
-    return exchange_and_merge(part, keys, parts, steps, strategy, group, device)
+    return _finish(td, part, lambda: exchange_and_merge(part, keys, parts, steps, strategy, group, device,
+                                                        merge=merge, td=td))

@@ -3,14 +3,16 @@
 A scaled-down served mix (group table 3M rows of the Zipf-key shape, build
 200K / probe 3M rows of the join shape, ranges of 10K..1M rows, random
 thresholds) runs once query by query on the calling thread, then all at once
-through a server with 8 slots.  Integer columns must match exactly and F64
-columns within 1e-12 relative (their summation order depends on atomics).
-A few requests are also checked against the oracle."""
+through a server with 8 slots.  Every result is checked against the oracle:
+integer columns exactly, F64 columns within 1e-12 * max(|want|, sum |x|) per
+group (their summation order depends on atomics); alone and in the mix, the
+integer columns are also identical to each other."""
 import numpy as np
 import pytest
 
 import oracle
 from teide_b200 import serve, workloads
+from teide_b200.pipelines import f64_tolerance_ok
 from teide_b200.td import OP_AVG, OP_COUNT, OP_MAX, OP_MIN, OP_SUM
 
 pytestmark = pytest.mark.gpu
@@ -39,21 +41,43 @@ def _requests(n, seed):
     return [serve.Request(*r) for r in raw]
 
 
-def _same(a, b, what):
-    assert list(a) == list(b), what
-    for k in a:
-        if a[k].dtype.kind == "f":
-            assert np.allclose(a[k], b[k], rtol=1e-12, atol=1e-9, equal_nan=True), (what, k)
-        else:
-            assert np.array_equal(a[k], b[k]), (what, k)
-
-
 def _canon(d, kind):
     return oracle.canonical(d, by=["key"] if kind == "group" else ["cat"])
 
 
+def _want(c2, b, p, r):
+    """The oracle's result of request r (canonical order) and, per F64
+    column, the scale of the tolerance rule (sum |x| for SUM, / count for AVG)."""
+    sl = slice(r.off, r.off + r.n)
+    if r.kind == "group":
+        m = c2["v1"][sl] > r.threshold
+        keys = {"key": c2["key"][sl]}
+        aggs = [(OP_COUNT, "v1", None), (OP_SUM, "v1", c2["v1"][sl]), (OP_MIN, "v1", c2["v1"][sl]),
+                (OP_MAX, "v1", c2["v1"][sl]), (OP_AVG, "v2", c2["v2"][sl])]
+    else:
+        left = {k: v[sl] for k, v in p.items()}
+        j = oracle.join(left, b, ["fk"], ["pk"], 0, lmask=left["qty"] > r.threshold)
+        m = None
+        keys = {"cat": j["cat"]}
+        aggs = [(OP_SUM, "price", j["price"]), (OP_COUNT, "price", None)]
+    return _canon(oracle.group(keys, aggs, m), r.kind), oracle.abs_bounds(keys, aggs, m)
+
+
+def _same(got, want, bounds, what):
+    """Integers exact; F64 within 1e-12 * max(|want|, bound) per group."""
+    assert list(got) == list(want), what
+    for k in want:
+        if k in bounds:
+            assert f64_tolerance_ok(got[k], want[k], bounds[k]), (what, k)
+        else:
+            assert np.array_equal(got[k], want[k]), (what, k)
+
+
 def test_alone_equals_mix(tables):
-    td, _, (tg, tb, tp) = tables
+    """Each of 48 requests run alone (the calling thread, no shared build)
+    and in the mix (8 slots; the join requests share one kept payload map)
+    matches the oracle, and the two results agree exactly on integers."""
+    td, (c2, b, p), (tg, tb, tp) = tables
     reqs = _requests(48, seed=7)
     serve.build(td, reqs, tg, tb, tp)
     try:
@@ -67,8 +91,15 @@ def test_alone_equals_mix(tables):
             for i, (r, t) in enumerate(zip(reqs, ts)):
                 res, tm = s.wait(t)
                 assert tm.status == 0, (i, tm.status)
-                _same(alone[i], _canon(td.table_dict(res), r.kind), f"request {i} ({r.kind})")
+                mix = _canon(td.table_dict(res), r.kind)
                 td.release(res)
+                want, bounds = _want(c2, b, p, r)
+                what = f"request {i} ({r.kind} [{r.off}, +{r.n}) t={r.threshold})"
+                _same(alone[i], want, bounds, what + " alone")
+                _same(mix, want, bounds, what + " in the mix")
+                for k in want:
+                    if k not in bounds:
+                        assert np.array_equal(alone[i][k], mix[k]), (what, k)
             st = s.stats()
             assert st.completed == len(reqs) and st.peak_in_flight >= 2
     finally:
@@ -87,42 +118,63 @@ def test_mix_matches_oracle(tables):
                 assert tm.status == 0
                 got = _canon(td.table_dict(res), r.kind)
                 td.release(res)
-                sl = slice(r.off, r.off + r.n)
-                if r.kind == "group":
-                    m = c2["v1"][sl] > r.threshold
-                    want = oracle.group({"key": c2["key"][sl]},
-                                        [(OP_COUNT, "v1", None), (OP_SUM, "v1", c2["v1"][sl]),
-                                         (OP_MIN, "v1", c2["v1"][sl]), (OP_MAX, "v1", c2["v1"][sl]),
-                                         (OP_AVG, "v2", c2["v2"][sl])], mask=m)
-                else:
-                    left = {k: v[sl] for k, v in p.items()}
-                    j = oracle.join(left, b, ["fk"], ["pk"], 0, lmask=left["qty"] > r.threshold)
-                    want = oracle.group({"cat": j["cat"]}, [(OP_SUM, "price", j["price"]),
-                                                            (OP_COUNT, "price", None)])
-                _same(_canon(want, r.kind), got, f"{r.kind} [{r.off}, +{r.n}) t={r.threshold}")
+                want, bounds = _want(c2, b, p, r)
+                _same(got, want, bounds, f"{r.kind} [{r.off}, +{r.n}) t={r.threshold}")
     finally:
         serve.release(td, reqs)
 
 
+def test_shared_build_follows_the_build_table(gpu):
+    """Served join queries keep one payload map per resident build side; a
+    new build table -- after the old one is unpinned and freed, so its
+    device memory may be handed out again -- must get its own map, never the
+    old one: results follow the new table's values."""
+    b, p = workloads.join_tables(n_build=200_000, n_probe=1_000_000, seed=61)
+    pt = gpu.table(p)
+    gpu.lib.td_gpu_pin.argtypes = [serve.P]
+    gpu.lib.td_gpu_unpin.argtypes = [serve.P]
+    assert gpu.lib.td_gpu_pin(pt) == 0
+    try:
+        for trial in range(3):
+            bb = dict(b)
+            bb["cat"] = (b["cat"] * (trial + 1) + trial) % 1000       # same keys, other group slots
+            bt = gpu.table(bb)
+            assert gpu.lib.td_gpu_pin(bt) == 0
+            reqs = [serve.Request("join", 0, len(p["fk"]), t, 0.0) for t in (5, 40, 90)]
+            serve.build(gpu, reqs, None, bt, pt)
+            with serve.Server(gpu, slots=2) as s:
+                ts = [s.submit(r.graph, r.root) for r in reqs]
+                for r, t in zip(reqs, ts):
+                    res, tm = s.wait(t)
+                    assert tm.status == 0
+                    got = _canon(gpu.table_dict(res), "join")
+                    gpu.release(res)
+                    want, bounds = _want(None, bb, p, r)
+                    _same(got, want, bounds, f"trial {trial} t={r.threshold}")
+            serve.release(gpu, reqs)
+            gpu.lib.td_gpu_unpin(bt)
+            gpu.release(bt)
+    finally:
+        gpu.lib.td_gpu_unpin(pt)
+        gpu.release(pt)
+
+
 def test_budget_serializes_and_stays_correct(tables):
-    td, _, (tg, tb, tp) = tables
+    td, (c2, b, p), (tg, tb, tp) = tables
     reqs = _requests(10, seed=13)
     serve.build(td, reqs, tg, tb, tp)
     try:
-        outs = []
         for slots, budget in ((8, 1), (8, 0)):
             with serve.Server(td, slots=slots, hbm_budget=budget) as s:
                 ts = [s.submit(r.graph, r.root) for r in reqs]
-                res = []
-                for r, t in zip(reqs, ts):
+                for i, (r, t) in enumerate(zip(reqs, ts)):
                     p_, tm = s.wait(t)
                     assert tm.status == 0
-                    res.append(_canon(td.table_dict(p_), r.kind))
+                    got = _canon(td.table_dict(p_), r.kind)
                     td.release(p_)
+                    want, bounds = _want(c2, b, p, r)
+                    _same(got, want, bounds, f"request {i} budget {budget}")
                 if budget == 1:
                     assert s.stats().peak_in_flight == 1
-                outs.append(res)
-        for i, (a, b_) in enumerate(zip(*outs)):
-            _same(a, b_, f"request {i}")
     finally:
         serve.release(td, reqs)
