@@ -85,6 +85,14 @@ tdg_status tdg_minmax(tdg_col col, int64_t n, int64_t* d_out, void* stream);
  * 1 (double) or 2 (bool bytes).  Replaces expr_eval_full (exec.c:1254-1273). */
 tdg_status tdg_eval(const tdg_expr* e, int64_t n, void* out, int32_t out_kind, void* stream);
 
+/* out[r] = vals[p] for starts[p] <= r < starts[p + 1] (p < n_runs, starts
+ * ascending, starts[n_runs] = n; elements of esz = 1, 2, 4 or 8 bytes):
+ * a column given as runs written out per row -- a partitioned table's
+ * MAPCOMMON key, one value per partition.  Replaces materialize_mapcommon
+ * (exec.c:201-243). */
+tdg_status tdg_expand_runs(const void* vals, int32_t esz, const int64_t* starts, int64_t n_runs,
+                           void* out, int64_t n, void* stream);
+
 /* ---- selection (filter) -----------------------------------------------------
  * A row is selected when `pred` (may be NULL) is non-zero and, if `sel_in` is
  * given, its bit in that TD_SEL bit array is set. */

@@ -66,6 +66,19 @@ extern "C" {
 #define TD_SEL       16
 #define TD_SYM       20
 
+/* Partitioned tables (src/store/part.c): a parted column is a vector of
+ * segment pointers, one per partition, typed TD_PARTED_BASE + the segments'
+ * type; the MAPCOMMON column holds the partition keys -- its two elements
+ * are the key values (DATE, I64 or SYM by the directory names, attrs
+ * TD_MC_*) and the partitions' row counts (I64). */
+#define TD_PARTED_BASE   32
+#define TD_MAPCOMMON     64
+#define TD_MC_SYM    0
+#define TD_MC_DATE   1
+#define TD_MC_I64    2
+#define TD_IS_PARTED(t)       ((t) >= TD_PARTED_BASE && (t) < TD_MAPCOMMON)
+#define TD_PARTED_BASETYPE(t) ((t) - TD_PARTED_BASE)
+
 /* dictionary-index width of a TD_SYM column: low two bits of attrs */
 #define TD_SYM_W_MASK   0x03
 #define TD_SYM_W8       0x00
@@ -521,6 +534,12 @@ td_err_t td_sym_load(const char* path);
  * digits and dots, in name order) holds the splayed table `table_name`; the
  * partitions' columns are concatenated (src/store/part.c). */
 td_t*    td_part_load(const char* db_root, const char* table_name);
+/* The same database as a partitioned table: the MAPCOMMON column first
+ * (named "date" for YYYY.MM.DD directories, else "part"), then one parted
+ * column per column of the partitions, segments in partition-name order;
+ * db_root/sym is loaded first when present.  Rows = td_parted_nrows. */
+td_t*    td_read_parted(const char* db_root, const char* table_name);
+int64_t  td_parted_nrows(td_t* parted_col);
 
 /* DAG construction */
 td_graph_t* td_graph_new(td_t* tbl);

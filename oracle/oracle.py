@@ -145,7 +145,12 @@ def abs_bounds(keys: dict, aggs, mask=None) -> dict:
     Same arguments and row order as group(); only F64 SUM/AVG columns."""
     fa = [(op, nm, np.abs(np.asarray(a))) for op, nm, a in aggs
           if op in (OP_SUM, OP_AVG) and a is not None and np.asarray(a).dtype.kind == "f"]
-    return group(keys, fa, mask) if fa else {}
+    if not fa:
+        return {}
+    out = group(keys, fa, mask)
+    for k in keys:                 # the key columns are not bounds
+        out.pop(k, None)
+    return out
 
 
 def group_direct(key, aggs, mask=None, key_name="key") -> dict:

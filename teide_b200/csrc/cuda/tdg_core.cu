@@ -419,6 +419,37 @@ extern "C" tdg_status tdg_select_gather(int64_t n, const tdg_expr* pred, const u
     return launch_status();
 }
 
+// ---- run-length expansion -----------------------------------------------------------
+// out[r] = vals[p] for starts[p] <= r < starts[p + 1]: a column given as runs
+// (a partitioned table's MAPCOMMON partition key, one value per partition)
+// written out row by row.  Each thread finds its row's run by binary search.
+__global__ void __launch_bounds__(kThreads) k_expand_runs(const char* vals, int esz, const int64_t* starts,
+                                                          int64_t n_runs, char* out, int64_t n) {
+    for (int64_t r = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; r < n; r += (int64_t)gridDim.x * blockDim.x) {
+        int64_t a = 0, b = n_runs - 1;
+        while (a < b) {
+            const int64_t m = (a + b + 1) >> 1;
+            if (__ldg(starts + m) <= r) a = m; else b = m - 1;
+        }
+        switch (esz) {
+            case 8: ((int64_t*)out)[r] = ((const int64_t*)vals)[a]; break;
+            case 4: ((int32_t*)out)[r] = ((const int32_t*)vals)[a]; break;
+            case 2: ((int16_t*)out)[r] = ((const int16_t*)vals)[a]; break;
+            default: out[r] = vals[a]; break;
+        }
+    }
+}
+
+extern "C" tdg_status tdg_expand_runs(const void* vals, int32_t esz, const int64_t* starts, int64_t n_runs,
+                                      void* out, int64_t n, void* stream) {
+    if (n <= 0) return E_OK;
+    if (n_runs <= 0 || (esz != 1 && esz != 2 && esz != 4 && esz != 8)) return E_RANGE;
+    const int g = grid_for((const void*)k_expand_runs, kThreads, 0, n);
+    (note_launch(), k_expand_runs<<<g, kThreads, 0, (cudaStream_t)stream>>>((const char*)vals, esz, starts, n_runs,
+                                                                          (char*)out, n));
+    return launch_status();
+}
+
 extern "C" void tdg_set_timing(int32_t on) { g_timing.store(on ? 1 : 0); }
 extern "C" int32_t tdg_timing_enabled(void) { return g_timing.load(); }
 extern "C" void tdg_count_launches(uint64_t n) { note_launch((int)n); }

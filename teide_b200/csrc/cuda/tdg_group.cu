@@ -64,19 +64,13 @@ constexpr int64_t kSampleMinRows = (int64_t)1 << 22;
 constexpr int kHotHist = 1024;                // sampled-count histogram buckets (hot threshold)
 // MODE 3 (partitioned cold rows)
 constexpr int64_t kPartMinRows = (int64_t)1 << 20;   // smaller inputs keep MODE 1
-#ifndef TDG_PART_SMEM_KB
-#define TDG_PART_SMEM_KB 96
-#endif
-#ifndef TDG_PART_DENSE
-#define TDG_PART_DENSE 4
-#endif
-constexpr size_t kPartSmem = TDG_PART_SMEM_KB * 1024;       // a partition's shared-memory table
+constexpr size_t kPartSmem = 192 * 1024;      // a partition's shared-memory table (4096 slots at 5 words)
 constexpr int kPartThreads = 512;
 constexpr int64_t kPartItem = 16384;          // entries per aggregation work item
 constexpr int kPartRegions = 1024;            // partitions below this are split into stripes
 constexpr int kPartMaxStripes = 64;
 constexpr uint32_t kPartMargin = 32;          // entries every region holds beyond its estimate
-constexpr int64_t kPartDense = TDG_PART_DENSE;             // entries per slot below which an item skips the table
+constexpr int64_t kPartDense = 4;             // entries per slot below which an item skips the table
 
 enum : int32_t { K_COUNT = 0, K_SUM_I, K_SUM_F, K_MIN_I, K_MAX_I, K_MIN_F, K_MAX_F };
 
@@ -849,29 +843,56 @@ __device__ __forceinline__ void vec_rows(const GroupK& G, const SmemView& V, con
         }
     }
     if (MODE == 3) {
-        // cold rows become entries of their region; the lanes of a warp that
-        // share a region reserve their places with one atomic
+        // cold rows become entries of their region.  With few partitions
+        // (striped) the lanes of a warp that share a region reserve their
+        // places with one atomic; with many, a warp's rows rarely share one,
+        // so each row reserves its own place and a thread's four atomics are
+        // in flight together.
         const PartK& K = G.pk;
         const unsigned lane = threadIdx.x & 31;
         const uint32_t stripe = blockIdx.x & (uint32_t)(K.stripes - 1);
+        uint32_t rpos[4], rcap[4];
+        long long rbase[4];
+        if (K.stripes == 1) {
+#pragma unroll
+            for (int i = 0; i < 4; i++) {
+                rpos[i] = rcap[i] = 0;
+                rbase[i] = 0;
+                if (ok[i] && hidx[i] < 0) {
+                    const uint32_t r = (uint32_t)(slot[i] >> K.shift);
+                    rpos[i] = atomicAdd(&K.fill[r], 1u);
+                    rcap[i] = K.cap[r];
+                    rbase[i] = K.base[r];
+                }
+            }
+        }
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const bool cold = ok[i] && hidx[i] < 0;
-            const unsigned act = __ballot_sync(0xffffffffu, cold);
-            if (!cold) continue;
-            const uint32_t r = (uint32_t)(slot[i] >> K.shift) * (uint32_t)K.stripes + stripe;
-            const unsigned peers = __match_any_sync(act, r);
-            const int leader = __ffs(peers) - 1;
-            uint32_t pos = 0, cap = 0;
-            long long base = 0;
-            if ((int)lane == leader) {
-                pos = atomicAdd(&K.fill[r], (uint32_t)__popc(peers));
-                cap = K.cap[r];
-                base = K.base[r];
+            uint32_t pos, cap;
+            long long base;
+            if (K.stripes == 1) {
+                if (!cold) continue;
+                pos = rpos[i];
+                cap = rcap[i];
+                base = rbase[i];
+            } else {
+                const unsigned act = __ballot_sync(0xffffffffu, cold);
+                if (!cold) continue;
+                const uint32_t r = (uint32_t)(slot[i] >> K.shift) * (uint32_t)K.stripes + stripe;
+                const unsigned peers = __match_any_sync(act, r);
+                const int leader = __ffs(peers) - 1;
+                pos = cap = 0;
+                base = 0;
+                if ((int)lane == leader) {
+                    pos = atomicAdd(&K.fill[r], (uint32_t)__popc(peers));
+                    cap = K.cap[r];
+                    base = K.base[r];
+                }
+                pos = __shfl_sync(peers, pos, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+                cap = __shfl_sync(peers, cap, leader);
+                base = __shfl_sync(peers, base, leader);
             }
-            pos = __shfl_sync(peers, pos, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
-            cap = __shfl_sync(peers, cap, leader);
-            base = __shfl_sync(peers, base, leader);
             if (pos < cap) {
                 const int64_t e = base + pos;
                 K.e_slot[e] = (uint32_t)slot[i];

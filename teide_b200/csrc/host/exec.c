@@ -119,13 +119,13 @@ static int xc_node(xc_t* xc, td_op_t* op) {
             td_t* tbl = ext ? scan_table_of(xc->x, ext, xc->tbl) : NULL;
             td_t* col = tbl ? td_table_get_col(tbl, ext->sym) : NULL;
             if (!col) { xc->err = TD_ERR_SCHEMA; return -1; }
-            if (col->len != td_table_nrows(xc->tbl)) { xc->err = TD_ERR_LENGTH; return -1; }
+            if (td_parted_nrows(col) != td_table_nrows(xc->tbl)) { xc->err = TD_ERR_LENGTH; return -1; }
             tdb_devcol d;
             int st = tdb_col_device(&xc->x->c, col, 0, &d);
             if (st) { xc->err = st; return -1; }
             int ci = add_col(xc, &d);
             if (ci < 0) return -1;
-            r = emit_ins(xc, TDG_X_COL, 0, 0, col->type == TD_F64 ? 1 : 0, ci);
+            r = emit_ins(xc, TDG_X_COL, 0, 0, d.type == TD_F64 ? 1 : 0, ci);
             break;
         }
         case OP_CONST: {
@@ -418,7 +418,7 @@ static int resolve_gin(ex_t* x, td_op_t* op, td_t* tbl, jsrc_t* js, int want_sta
             td_t* t = scan_table_of(x, ext, tbl);
             col = t ? td_table_get_col(t, ext->sym) : NULL;
             if (!col) return TD_ERR_SCHEMA;
-            if (col->len != td_table_nrows(tbl)) return TD_ERR_LENGTH;
+            if (td_parted_nrows(col) != td_table_nrows(tbl)) return TD_ERR_LENGTH;
         }
         tdb_devcol d;
         int st = tdb_col_device(&x->c, col, want_stats, &d);
@@ -426,8 +426,8 @@ static int resolve_gin(ex_t* x, td_op_t* op, td_t* tbl, jsrc_t* js, int want_sta
         gi->col.data = d.dptr; gi->col.type = d.type; gi->col.attrs = d.attrs; gi->col.side = (uint8_t)side;
         gi->name = ext->sym;
         gi->src = col;
-        gi->type = col->type;
-        gi->attrs = col->attrs;
+        gi->type = d.type;                      /* a parted column's segments' type */
+        gi->attrs = d.attrs;
         gi->has_stats = d.has_stats;
         gi->kmin = d.kmin; gi->kmax = d.kmax;
         return TD_OK;
@@ -1163,7 +1163,7 @@ static td_t* exec_sort_node(ex_t* x, td_op_t* sop, int64_t limit) {
             vfree(&kv);
             if (TD_IS_ERR(col)) { st = TD_ERR_CODE(col); break; }
             kexpr[k] = col;
-            if (col->type <= 0 || col->type == TD_TABLE) { st = TD_ERR_NYI; break; }
+            if (col->type <= 0 || col->type == TD_TABLE || col->type >= TD_PARTED_BASE) { st = TD_ERR_NYI; break; }
             if (col->len != n) { st = TD_ERR_LENGTH; break; }
         }
         if (!col) { st = TD_ERR_SCHEMA; break; }

@@ -587,6 +587,87 @@ int tdb_h2d(tdb_ctx* c, void* dev, const void* host, size_t bytes) {
     return TD_OK;
 }
 
+static int is_parted(td_t* col) { return TD_IS_PARTED(col->type) || col->type == TD_MAPCOMMON; }
+
+/* The device copy of a partitioned table's column, as one flat column of
+ * its rows: a parted column's segments one after the other (uploaded, or
+ * copied device to device when a segment is resident), a MAPCOMMON column's
+ * partition keys each repeated over its partition's rows (tdg_expand_runs).
+ * Replaces the concat fallback of exec_group_parted (exec.c:5462-5530) and
+ * materialize_mapcommon (exec.c:201-243), on the device. */
+static int flatten(tdb_ctx* c, td_t* col, tdb_devcol* out, int persistent) {
+    memset(out, 0, sizeof(*out));
+    const int64_t n = td_parted_nrows(col);
+    td_t** kids = (td_t**)td_data(col);
+    int st = TD_OK;
+    void* d = NULL;
+    if (col->type == TD_MAPCOMMON) {
+        td_t* kv = kids[0];
+        td_t* rc = kids[1];
+        if (!kv || TD_IS_ERR(kv) || !rc || TD_IS_ERR(rc) || kv->len != rc->len || rc->type != TD_I64)
+            return TD_ERR_CORRUPT;
+        const int64_t np = kv->len;
+        const size_t esz = td_sym_elem_size(kv->type, kv->attrs);
+        const size_t bytes = n > 0 ? (size_t)n * esz : 1, vbytes = np > 0 ? (size_t)np * esz : 1;
+        d = persistent ? arena_alloc(bytes) : tdb_dev_alloc(c, bytes);
+        int64_t* starts = malloc((size_t)(np + 1) * 8);
+        void* dv = tdb_dev_alloc(c, vbytes);
+        int64_t* ds = tdb_dev_alloc(c, (size_t)(np + 1) * 8);
+        if (!d || !starts || !dv || !ds) st = TD_ERR_OOM;
+        if (!st) {
+            starts[0] = 0;
+            for (int64_t p = 0; p < np; p++) starts[p + 1] = starts[p] + ((const int64_t*)td_data(rc))[p];
+            st = tdb_h2d(c, dv, td_data(kv), (size_t)np * esz);
+            if (!st) st = tdb_h2d(c, ds, starts, (size_t)(np + 1) * 8);
+            if (!st) st = tdb_ctx_sync(c);             /* the host arrays are copied before they are freed */
+            if (!st) st = tdg_expand_runs(dv, (int32_t)esz, ds, np, d, n, c->stream);
+        }
+        free(starts);
+        out->type = kv->type;
+        out->attrs = kv->attrs;
+    } else {
+        td_t* first = NULL;
+        for (int64_t p = 0; p < col->len && !first; p++) if (kids[p] && !TD_IS_ERR(kids[p])) first = kids[p];
+        const int8_t base = (int8_t)TD_PARTED_BASETYPE(col->type);
+        const uint8_t attrs = first ? first->attrs & TD_SYM_W_MASK : 0;
+        const size_t esz = td_sym_elem_size(base, attrs);
+        if (!esz) return TD_ERR_TYPE;
+        for (int64_t p = 0; p < col->len; p++)
+            if (kids[p] && !TD_IS_ERR(kids[p]) && (kids[p]->type != base ||
+                                                   td_sym_elem_size(kids[p]->type, kids[p]->attrs) != esz))
+                return TD_ERR_NYI;                         /* segments of different widths */
+        const size_t bytes = n > 0 ? (size_t)n * esz : 1;
+        d = persistent ? arena_alloc(bytes) : tdb_dev_alloc(c, bytes);
+        if (!d) return TD_ERR_OOM;
+        size_t off = 0;
+        for (int64_t p = 0; p < col->len && !st; p++) {
+            td_t* seg = kids[p];
+            if (!seg || TD_IS_ERR(seg) || seg->len <= 0) continue;
+            const size_t b = (size_t)seg->len * esz;
+            tdb_devcol sd;
+            if (tdb_col_resident(seg) && !tdb_col_device(c, seg, 0, &sd)) {
+                if (cudaMemcpyAsync((char*)d + off, sd.dptr, b, cudaMemcpyDeviceToDevice, (cudaStream_t)c->stream) !=
+                    cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; }
+            } else {
+                pin_host(seg);
+                if (cudaMemcpyAsync((char*)d + off, td_data(seg), b, cudaMemcpyHostToDevice, (cudaStream_t)c->stream) !=
+                    cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; }
+                else c->h2d_bytes += b;
+            }
+            off += b;
+        }
+        out->type = base;
+        out->attrs = attrs;
+    }
+    if (st) {
+        if (persistent && d) arena_free(d);
+        return st;
+    }
+    out->dptr = d;
+    out->len = n;
+    return TD_OK;
+}
+
 int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
     if (!col || TD_IS_ERR(col) || col->type <= 0 || col->type == TD_TABLE || col->type == TD_LIST ||
         col->type == TD_SEL)
@@ -604,9 +685,10 @@ int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
         return TD_OK;
     }
     uint64_t serial = tdb_block_serial(col);
+    const int64_t rows = td_parted_nrows(col);     /* a parted column's rows, else its length */
     pthread_mutex_lock(&mu);
     int i = find_mirror_locked(col);
-    if (i >= 0 && mirrors[i].dc.len == col->len) {
+    if (i >= 0 && mirrors[i].dc.len == rows) {
         *out = mirrors[i].dc;
         pthread_mutex_unlock(&mu);
         if (want_stats && !out->has_stats && is_int_type(out->type)) {
@@ -621,7 +703,7 @@ int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
     }
     pthread_mutex_unlock(&mu);
     for (int k = 0; k < tls_ntm; k++) {
-        if (tls_tm[k].host == col && tls_tm[k].serial == serial && tls_tm[k].dc.len == col->len) {
+        if (tls_tm[k].host == col && tls_tm[k].serial == serial && tls_tm[k].dc.len == rows) {
             if (want_stats && !tls_tm[k].dc.has_stats) {
                 int st = compute_stats(c, &tls_tm[k].dc);
                 if (st) return st;
@@ -639,7 +721,7 @@ int tdb_col_device(tdb_ctx* c, td_t* col, int want_stats, tdb_devcol* out) {
     tmirror_t* t = &tls_tm[tls_ntm];
     t->host = col;
     t->serial = serial;
-    int st = upload(c, col, &t->dc, 0);
+    int st = is_parted(col) ? flatten(c, col, &t->dc, 0) : upload(c, col, &t->dc, 0);
     if (st) return st;
     if (want_stats) {
         st = compute_stats(c, &t->dc);
@@ -725,7 +807,7 @@ td_err_t td_gpu_pin(td_t* tbl) {
         pthread_mutex_unlock(&mu);
         if (have) continue;
         tdb_devcol dc;
-        st = upload(&c, col, &dc, 1);
+        st = is_parted(col) ? flatten(&c, col, &dc, 1) : upload(&c, col, &dc, 1);
         if (st) break;
         st = compute_stats(&c, &dc);
         if (st) { arena_free(dc.dptr); break; }

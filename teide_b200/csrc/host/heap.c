@@ -196,7 +196,8 @@ static void for_each_owned(td_t* v, void (*fn)(td_t*)) {
             if (slots[1 + i] && !TD_IS_ERR(slots[1 + i])) fn(slots[1 + i]);
         return;
     }
-    if (v->type == TD_LIST) {
+    if (v->type == TD_LIST || TD_IS_PARTED(v->type) || v->type == TD_MAPCOMMON) {
+        /* a list's items, a parted column's segments, a MAPCOMMON's key values and counts */
         td_t** items = (td_t**)td_data(v);
         for (int64_t i = 0; i < v->len; i++)
             if (items[i] && !TD_IS_ERR(items[i])) fn(items[i]);

@@ -22,8 +22,13 @@ typedef struct tdb_block_prefix {
     size_t   raw_size;      /* bytes of the OS allocation */
     _Atomic(size_t) pinned; /* bytes page-locked with cudaHostRegister */
     uint64_t serial;        /* allocation serial: device mirrors key on it */
-    uint8_t  pad[16];
+    uint8_t  pad[24];
 } tdb_block_prefix;
+
+/* The header that follows the prefix must keep the 32-byte alignment td.h
+ * declares for td_t (TD_ALIGN(32), td_data assumed 32-byte aligned): the
+ * OS allocation is 64-byte (small blocks) or page aligned (large ones). */
+_Static_assert(sizeof(tdb_block_prefix) == 64, "block prefix must be 64 bytes");
 
 #define TDB_BLK_MAGIC 0x7D6B1C0Au
 #define TDB_BLK_MALLOC 1u

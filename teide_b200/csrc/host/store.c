@@ -402,6 +402,161 @@ td_t* td_part_load(const char* db_root, const char* table_name) {
     return res ? res : TD_ERR_PTR(TD_ERR_OOM);
 }
 
+/* ---- partitioned tables (part.c:284-520) ----------------------------------------- */
+
+static int is_date_dir(const char* s) {
+    if (strlen(s) != 10 || s[4] != '.' || s[7] != '.') return 0;
+    for (int i = 0; i < 10; i++)
+        if (i != 4 && i != 7 && (s[i] < '0' || s[i] > '9')) return 0;
+    const int m = (s[5] - '0') * 10 + (s[6] - '0'), d = (s[8] - '0') * 10 + (s[9] - '0');
+    return m >= 1 && m <= 12 && d >= 1 && d <= 31;
+}
+
+static int is_int_str(const char* s) {
+    if (*s == '-') s++;
+    if (!*s) return 0;
+    for (; *s; s++) if (*s < '0' || *s > '9') return 0;
+    return 1;
+}
+
+/* Days from 2000-01-01 to y-m-d in the proleptic Gregorian calendar: the
+ * count of days in whole 400-year eras (146097 each), then in the years of
+ * the era and in the months from March (so the leap day falls last). */
+static int32_t days_since_2000(int64_t y, int64_t m, int64_t d) {
+    y -= m <= 2;
+    const int64_t era = (y >= 0 ? y : y - 399) / 400;
+    const int64_t yoe = y - era * 400;
+    const int64_t doy = (153 * (m > 2 ? m - 3 : m + 9) + 2) / 5 + d - 1;
+    const int64_t doe = yoe * 365 + yoe / 4 - yoe / 100 + doy;
+    return (int32_t)(era * 146097 + doe - 719468 - 10957);
+}
+
+/* Partition directory names of db_root, in name order. */
+static int64_t list_parts(const char* db_root, char*** out) {
+    *out = NULL;
+    DIR* d = opendir(db_root);
+    if (!d) return -TD_ERR_IO;
+    char** names = NULL;
+    int64_t np = 0, cap = 0;
+    struct dirent* e;
+    while ((e = readdir(d))) {
+        if (e->d_name[0] == '.' || !part_dir_name(e->d_name)) continue;
+        if (np == cap) {
+            cap = cap ? cap * 2 : 16;
+            char** nn = realloc(names, (size_t)cap * sizeof(char*));
+            if (!nn) break;
+            names = nn;
+        }
+        if (!(names[np] = strdup(e->d_name))) break;
+        np++;
+    }
+    closedir(d);
+    if (np) qsort(names, (size_t)np, sizeof(char*), cmp_str);
+    *out = names;
+    return np;
+}
+
+static td_t* ptr_block(int8_t type, int64_t n) {
+    td_t* v = td_alloc((size_t)(n ? n : 1) * sizeof(td_t*));
+    if (!v) return TD_ERR_PTR(TD_ERR_OOM);
+    v->type = type;
+    v->len = n;
+    memset(td_data(v), 0, (size_t)(n ? n : 1) * sizeof(td_t*));
+    return v;
+}
+
+td_t* td_read_parted(const char* db_root, const char* table_name) {
+    if (!db_root || !table_name) return TD_ERR_PTR(TD_ERR_IO);
+    if (strchr(table_name, '/') || strchr(table_name, '\\') || strstr(table_name, "..") || table_name[0] == '.')
+        return TD_ERR_PTR(TD_ERR_IO);
+    char path[1024];
+    if (snprintf(path, sizeof(path), "%s/sym", db_root) >= (int)sizeof(path)) return TD_ERR_PTR(TD_ERR_IO);
+    struct stat sb;
+    if (stat(path, &sb) == 0) {
+        td_err_t e = td_sym_load(path);
+        if (e != TD_OK) return TD_ERR_PTR(e);
+    }
+    char** names = NULL;
+    const int64_t np = list_parts(db_root, &names);
+    if (np <= 0) { free(names); return TD_ERR_PTR(np < 0 ? (td_err_t)-np : TD_ERR_IO); }
+    td_t* res = NULL;
+    td_t** tabs = calloc((size_t)np, sizeof(td_t*));
+    if (!tabs) res = TD_ERR_PTR(TD_ERR_OOM);
+    for (int64_t p = 0; p < np && !res; p++) {
+        if (snprintf(path, sizeof(path), "%s/%s/%s", db_root, names[p], table_name) >= (int)sizeof(path)) {
+            res = TD_ERR_PTR(TD_ERR_IO);
+            break;
+        }
+        tabs[p] = td_splay_load(path);
+        if (!tabs[p] || TD_IS_ERR(tabs[p])) { tabs[p] = NULL; res = TD_ERR_PTR(TD_ERR_IO); }
+    }
+    if (!res) {
+        /* the partition keys: dates, integers or symbols by the directory names */
+        int all_date = 1, all_int = 1;
+        for (int64_t p = 0; p < np; p++) {
+            all_date = all_date && is_date_dir(names[p]);
+            all_int = all_int && is_int_str(names[p]);
+        }
+        const uint8_t mc = all_date ? TD_MC_DATE : all_int ? TD_MC_I64 : TD_MC_SYM;
+        td_t* kv = td_vec_new(mc == TD_MC_DATE ? TD_DATE : mc == TD_MC_I64 ? TD_I64 : TD_SYM, np);
+        td_t* rc = td_vec_new(TD_I64, np);
+        td_t* mcol = ptr_block(TD_MAPCOMMON, 2);
+        const int64_t nc = td_table_ncols(tabs[0]);
+        res = td_table_new(nc + 2);
+        if (!kv || TD_IS_ERR(kv) || !rc || TD_IS_ERR(rc) || TD_IS_ERR(mcol) || !res || TD_IS_ERR(res)) {
+            if (kv && !TD_IS_ERR(kv)) td_release(kv);
+            if (rc && !TD_IS_ERR(rc)) td_release(rc);
+            if (!TD_IS_ERR(mcol)) td_release(mcol);
+            if (res && !TD_IS_ERR(res)) td_release(res);
+            res = TD_ERR_PTR(TD_ERR_OOM);
+        } else {
+            for (int64_t p = 0; p < np; p++) {
+                const char* nm = names[p];
+                if (mc == TD_MC_DATE)
+                    ((int32_t*)td_data(kv))[p] = days_since_2000((nm[0] - '0') * 1000 + (nm[1] - '0') * 100 +
+                                                                 (nm[2] - '0') * 10 + (nm[3] - '0'),
+                                                                 (nm[5] - '0') * 10 + (nm[6] - '0'),
+                                                                 (nm[8] - '0') * 10 + (nm[9] - '0'));
+                else if (mc == TD_MC_I64)
+                    ((int64_t*)td_data(kv))[p] = strtoll(nm, NULL, 10);
+                else
+                    ((int64_t*)td_data(kv))[p] = td_sym_intern(nm, strlen(nm));
+                ((int64_t*)td_data(rc))[p] = td_table_nrows(tabs[p]);
+            }
+            kv->len = np;
+            rc->len = np;
+            mcol->attrs = mc;
+            ((td_t**)td_data(mcol))[0] = kv;             /* the block owns both */
+            ((td_t**)td_data(mcol))[1] = rc;
+            const char* mname = mc == TD_MC_DATE ? "date" : "part";
+            td_t* t2 = td_table_add_col(res, td_sym_intern(mname, strlen(mname)), mcol);
+            td_release(mcol);
+            res = t2;
+            for (int64_t c = 0; c < nc && res && !TD_IS_ERR(res); c++) {
+                td_t* first = td_table_get_col_idx(tabs[0], c);
+                if (!first) continue;
+                td_t* pc = ptr_block((int8_t)(TD_PARTED_BASE + first->type), np);
+                if (TD_IS_ERR(pc)) { td_release(res); res = pc; break; }
+                for (int64_t p = 0; p < np; p++) {
+                    td_t* seg = td_table_get_col_idx(tabs[p], c);
+                    if (seg) td_retain(seg);
+                    ((td_t**)td_data(pc))[p] = seg;
+                }
+                t2 = td_table_add_col(res, td_table_col_name(tabs[0], c), pc);
+                td_release(pc);
+                res = t2;
+            }
+        }
+    }
+    for (int64_t p = 0; p < np; p++) {
+        if (tabs && tabs[p]) td_release(tabs[p]);
+        free(names[p]);
+    }
+    free(tabs);
+    free(names);
+    return res ? res : TD_ERR_PTR(TD_ERR_OOM);
+}
+
 td_t* td_gpu_part_load(const char* db_root, const char* table_name) {
     td_t* tbl = td_part_load(db_root, table_name);
     if (!tbl || TD_IS_ERR(tbl)) return tbl;

@@ -79,7 +79,28 @@ int64_t td_table_ncols(td_t* t) { return (!t || TD_IS_ERR(t)) ? 0 : t->len; }
 int64_t td_table_nrows(td_t* t) {
     if (!t || TD_IS_ERR(t) || t->len <= 0) return 0;
     td_t* c = col_slots(t)[0];
-    return (!c || TD_IS_ERR(c)) ? 0 : c->len;
+    return (!c || TD_IS_ERR(c)) ? 0 : td_parted_nrows(c);
+}
+
+/* Rows of a column: its length, or for a parted column the sum of its
+ * segments' lengths and for a MAPCOMMON column the sum of its row counts
+ * (table.c:226-250). */
+int64_t td_parted_nrows(td_t* v) {
+    if (!v || TD_IS_ERR(v)) return 0;
+    if (v->type == TD_MAPCOMMON) {
+        td_t* counts = ((td_t**)td_data(v))[1];
+        if (!counts || TD_IS_ERR(counts)) return 0;
+        int64_t total = 0;
+        for (int64_t i = 0; i < counts->len; i++) total += ((const int64_t*)td_data(counts))[i];
+        return total;
+    }
+    if (!TD_IS_PARTED(v->type)) return v->len;
+    int64_t total = 0;
+    for (int64_t i = 0; i < v->len; i++) {
+        td_t* seg = ((td_t**)td_data(v))[i];
+        if (seg && !TD_IS_ERR(seg)) total += seg->len;
+    }
+    return total;
 }
 
 td_t* td_table_schema(td_t* t) {

@@ -137,3 +137,116 @@ def test_partitioned_db_matches_reference(td, ref, tmp_path):
         cat = np.concatenate([want[p][c] for p in order])
         assert np.array_equal(ours[c], theirs[c]), c
         assert np.array_equal(ours[c], cat), c
+
+
+# ---- partitioned tables (td_read_parted) -------------------------------------------
+
+def _parted_db(lib, root, parts, seed=9):
+    cols = _write_db(lib, root, parts, seed)
+    assert lib.lib.td_sym_save(f"{root}/sym".encode()) == 0
+    return cols
+
+
+def _col_info(lib, p):
+    """(type, attrs, len, element pointers) of a vector whose elements are td_t pointers."""
+    import ctypes as C
+    typ, attrs, n = lib.header(p)
+    ptrs = [C.c_void_p.from_address(p + 32 + 8 * i).value for i in range(n)]
+    return typ, attrs, n, ptrs
+
+
+def test_read_parted_matches_reference(td, ref, tmp_path):
+    """The partitioned table of both libraries over the same database: the
+    MAPCOMMON column first (DATE keys of the YYYY.MM.DD directories, their row
+    counts), then one parted column per column, segments in name order."""
+    import ctypes as C
+    out = {}
+    for name, lib in (("ours", td), ("theirs", ref)):
+        os.makedirs(tmp_path / name)
+        want = _parted_db(lib, tmp_path / name, PARTS)
+        lib.lib.td_read_parted.restype = C.c_void_p
+        lib.lib.td_read_parted.argtypes = [C.c_char_p, C.c_char_p]
+        lib.lib.td_parted_nrows.restype = C.c_int64
+        lib.lib.td_parted_nrows.argtypes = [C.c_void_p]
+        t = lib.check(lib.lib.td_read_parted(str(tmp_path / name).encode(), b"trades"), "read_parted")
+        L = lib.lib
+        cols = []
+        for j in range(L.td_table_ncols(t)):
+            c = L.td_table_get_col_idx(t, j)
+            typ, attrs, n, ptrs = _col_info(lib, c)
+            entry = {"name": lib.sym_name(L.td_table_col_name(t, j)), "type": typ, "n": n,
+                     "rows": L.td_parted_nrows(c)}
+            if typ == 64:                                  # MAPCOMMON: key values, row counts
+                entry["attrs"] = attrs
+                entry["keys"] = lib.vec_view(ptrs[0]).copy().tolist()
+                entry["counts"] = lib.vec_view(ptrs[1]).copy().tolist()
+            else:
+                entry["segs"] = [lib.vec_view(q).copy() for q in ptrs]
+            cols.append(entry)
+        out[name] = (cols, L.td_table_nrows(t), want)
+        lib.release(t)
+    (a, na, want), (b, nb, _) = out["ours"], out["theirs"]
+    order = sorted(PARTS)
+    assert na == nb == sum(PARTS.values())
+    assert [c["name"] for c in a] == [c["name"] for c in b] == ["date", "k", "px", "q"]
+    for x, y in zip(a, b):
+        assert x["type"] == y["type"] and x["n"] == y["n"] and x["rows"] == y["rows"], x["name"]
+        if x["type"] == 64:
+            assert x["attrs"] == y["attrs"] == 1 and x["keys"] == y["keys"] and x["counts"] == y["counts"]
+            assert x["counts"] == [PARTS[p] for p in order]
+        else:
+            for p, s1, s2 in zip(order, x["segs"], y["segs"]):
+                assert np.array_equal(s1, s2) and np.array_equal(s1, want[p][x["name"]]), (x["name"], p)
+
+
+PARTED_QUERIES = [
+    (["date"], [(50, "px"), (54, "px"), (53, "k")]),            # the partition key alone
+    (["k"], [(50, "q"), (52, "px"), (55, "px")]),               # a parted column
+    (["date", "k"], [(50, "px"), (54, "q")]),                   # both
+]
+
+
+def parted_want(cols, order, keys, aggs):
+    """The oracle's group-by over the partitions' rows, the partition key
+    (days since 2000-01-01 of each YYYY.MM.DD name) repeated over its rows."""
+    import datetime
+    import oracle
+    flat = {c: np.concatenate([cols[p][c] for p in order]) for c in ("k", "px", "q")}
+    days = [(datetime.date(int(p[:4]), int(p[5:7]), int(p[8:])) - datetime.date(2000, 1, 1)).days for p in order]
+    flat["date"] = np.repeat(np.array(days, np.int32), [len(cols[p]["k"]) for p in order])
+    return oracle.group({k: flat[k] for k in keys}, [(op, c, None if op == 54 else flat[c]) for op, c in aggs])
+
+
+def parted_group(lib, root, keys, aggs):
+    import ctypes as C
+    lib.lib.td_read_parted.restype = C.c_void_p
+    lib.lib.td_read_parted.argtypes = [C.c_char_p, C.c_char_p]
+    t = lib.check(lib.lib.td_read_parted(str(root).encode(), b"trades"), "read_parted")
+    g = lib.graph(t)
+    try:
+        r = g.execute(g.group([g.scan(k) for k in keys], [op for op, _ in aggs], [g.scan(c) for _, c in aggs]),
+                      optimize=False)
+    finally:
+        g.free()
+    out = lib.table_dict(r)
+    lib.release(r)
+    lib.release(t)
+    return out
+
+
+@pytest.mark.parametrize("q", range(len(PARTED_QUERIES)))
+def test_reference_parted_group_matches_oracle(ref, tmp_path, q):
+    """Teide's own group-by over a partitioned table (its per-partition or
+    concatenating path) pins the oracle's reading: the MAPCOMMON key repeated
+    over each partition's rows."""
+    import oracle
+    keys, aggs = PARTED_QUERIES[q]
+    cols = _parted_db(ref, tmp_path, PARTS)
+    got = oracle.canonical(parted_group(ref, tmp_path, keys, aggs), by=keys)
+    want = parted_want(cols, sorted(PARTS), keys, aggs)
+    assert list(got) == list(want)
+    for k in want:
+        if want[k].dtype.kind == "f":
+            assert np.allclose(got[k], want[k], rtol=1e-12, atol=1e-12), k
+        else:
+            assert np.array_equal(got[k].astype(want[k].dtype), want[k]), k

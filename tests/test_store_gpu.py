@@ -6,7 +6,7 @@ import numpy as np
 import pytest
 
 import oracle
-from teide_b200.pipelines import readme_group
+from teide_b200.pipelines import f64_tolerance_ok, readme_group
 from teide_b200 import workloads
 from teide_b200.td import OP_SUM
 
@@ -71,3 +71,60 @@ def test_partitioned_db_loads_resident(gpu, tmp_path):
     finally:
         L.td_gpu_unpin(r)
         gpu.release(r)
+
+
+# ---- partitioned tables -----------------------------------------------------------------
+
+BIG_PARTS = {"2024.01.02": 400_000, "2023.12.31": 700_000, "2024.01.01": 0, "2024.01.10": 90_000,
+             "2024.02.29": 250_000}
+
+
+@pytest.mark.parametrize("pinned", [False, True], ids=["uploaded", "resident"])
+def test_parted_group_by(gpu, tmp_path, pinned):
+    """Group-bys over td_read_parted's partitioned table: by the MAPCOMMON
+    partition key (expanded over the rows on the device), by a parted column
+    (its segments laid end to end on the device), and by both -- each equal
+    to the oracle over the partitions' rows.  Resident (td_gpu_pin), a second
+    query uploads nothing."""
+    import sys
+    import os
+    sys.path.insert(0, os.path.dirname(__file__))
+    from test_store import PARTED_QUERIES, _parted_db, parted_group, parted_want
+    cols = _parted_db(gpu, tmp_path, BIG_PARTS)
+    order = sorted(BIG_PARTS)
+    L = gpu.lib
+    if pinned:
+        L.td_read_parted.restype = C.c_void_p
+        L.td_read_parted.argtypes = [C.c_char_p, C.c_char_p]
+        L.td_gpu_pin.argtypes = [C.c_void_p]
+        L.td_gpu_unpin.argtypes = [C.c_void_p]
+        t = gpu.check(L.td_read_parted(str(tmp_path).encode(), b"trades"), "read_parted")
+        assert L.td_gpu_pin(t) == 0
+    for keys, aggs in PARTED_QUERIES:
+        if pinned:
+            g = gpu.graph(t)
+            try:
+                r = g.execute(g.group([g.scan(k) for k in keys], [op for op, _ in aggs],
+                                      [g.scan(c) for _, c in aggs]), optimize=False)
+            finally:
+                g.free()
+            s = St()
+            L.td_gpu_last_stats(C.byref(s))
+            assert s.h2d == 0, keys                   # every column resident, flattened once
+            got = gpu.table_dict(r)
+            gpu.release(r)
+        else:
+            got = parted_group(gpu, tmp_path, keys, aggs)
+        got = oracle.canonical(got, by=keys)
+        want = parted_want(cols, order, keys, aggs)
+        assert list(got) == list(want), keys
+        absd = {p: {**cols[p], "px": np.abs(cols[p]["px"])} for p in order}
+        bounds = parted_want(absd, order, keys, aggs)            # sum |px| (or its mean) per group
+        for k in want:
+            if want[k].dtype.kind == "f":
+                assert f64_tolerance_ok(got[k], want[k], bounds[k]), (keys, k)
+            else:
+                assert got[k].dtype == want[k].dtype and np.array_equal(got[k], want[k]), (keys, k)
+    if pinned:
+        L.td_gpu_unpin(t)
+        gpu.release(t)
