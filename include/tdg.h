@@ -374,6 +374,11 @@ typedef struct tdg_batch_plan {
     int32_t query_base;    /* added to every emitted query index (0 from plan_make;
                               a caller running a batch in parts sets it per part) */
     int32_t n_pieces;      /* emit units: each query's slots in pieces of 4096 */
+    int32_t pad;
+    const volatile int32_t* cancel;   /* device-readable word (mapped host memory) or NULL:
+                                         once it reads nonzero the persistent kernel takes no
+                                         further work item, so a cancelled run ends within one
+                                         item per CTA (the caller reports TD_ERR_CANCEL) */
 } tdg_batch_plan;
 
 typedef struct tdg_batch_out {

@@ -48,6 +48,7 @@ struct BatchK {
     unsigned long long* rec;
     unsigned long long* counter;
     int32_t* err;
+    const volatile int32_t* cancel;  // polled per work item (pool.c:485-489's per-task check)
     const int32_t* piece_q;       // emit piece -> query
     const int64_t* piece_s0;      // emit piece -> first slot within the query
     int64_t* pcount;              // groups per piece, then exclusive offsets
@@ -91,6 +92,7 @@ static BatchK make_bk(const tdg_batch_plan* p, void* ws) {
     char* w = (char*)ws;
     B.counter = (unsigned long long*)(w + L.hdr);
     B.err = (int32_t*)(w + L.hdr + 16);
+    B.cancel = p->cancel;
     B.q = (const BQ*)(w + L.q);
     B.item_q = (const int32_t*)(w + L.item_q);
     B.piece_q = (const int32_t*)(w + L.piece_q);
@@ -183,7 +185,11 @@ __global__ void __launch_bounds__(kBatchMaxThreads) k_batch_agg(const BatchK B) 
     unsigned long long* sacc = sm + ((B.smem_slots * 4 + 7) >> 3);
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) s_item = (long long)atomicAdd(B.counter, 1ULL);
+        if (threadIdx.x == 0) {
+            long long it = (long long)atomicAdd(B.counter, 1ULL);
+            if (B.cancel && *B.cancel) it = B.n_items;     // cancelled: take no further item
+            s_item = it;
+        }
         __syncthreads();
         const int64_t item = s_item;
         if (item >= B.n_items) break;

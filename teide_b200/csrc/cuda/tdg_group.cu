@@ -843,56 +843,30 @@ __device__ __forceinline__ void vec_rows(const GroupK& G, const SmemView& V, con
         }
     }
     if (MODE == 3) {
-        // cold rows become entries of their region.  With few partitions
-        // (striped) the lanes of a warp that share a region reserve their
-        // places with one atomic; with many, a warp's rows rarely share one,
-        // so each row reserves its own place and a thread's four atomics are
-        // in flight together.
+        // cold rows become entries of their region; the lanes of a warp that
+        // share a region reserve their places with one atomic.  (One atomic
+        // per row, all four in flight at once, measured slower at 2^24 keys.)
         const PartK& K = G.pk;
         const unsigned lane = threadIdx.x & 31;
         const uint32_t stripe = blockIdx.x & (uint32_t)(K.stripes - 1);
-        uint32_t rpos[4], rcap[4];
-        long long rbase[4];
-        if (K.stripes == 1) {
-#pragma unroll
-            for (int i = 0; i < 4; i++) {
-                rpos[i] = rcap[i] = 0;
-                rbase[i] = 0;
-                if (ok[i] && hidx[i] < 0) {
-                    const uint32_t r = (uint32_t)(slot[i] >> K.shift);
-                    rpos[i] = atomicAdd(&K.fill[r], 1u);
-                    rcap[i] = K.cap[r];
-                    rbase[i] = K.base[r];
-                }
-            }
-        }
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             const bool cold = ok[i] && hidx[i] < 0;
-            uint32_t pos, cap;
-            long long base;
-            if (K.stripes == 1) {
-                if (!cold) continue;
-                pos = rpos[i];
-                cap = rcap[i];
-                base = rbase[i];
-            } else {
-                const unsigned act = __ballot_sync(0xffffffffu, cold);
-                if (!cold) continue;
-                const uint32_t r = (uint32_t)(slot[i] >> K.shift) * (uint32_t)K.stripes + stripe;
-                const unsigned peers = __match_any_sync(act, r);
-                const int leader = __ffs(peers) - 1;
-                pos = cap = 0;
-                base = 0;
-                if ((int)lane == leader) {
-                    pos = atomicAdd(&K.fill[r], (uint32_t)__popc(peers));
-                    cap = K.cap[r];
-                    base = K.base[r];
-                }
-                pos = __shfl_sync(peers, pos, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
-                cap = __shfl_sync(peers, cap, leader);
-                base = __shfl_sync(peers, base, leader);
+            const unsigned act = __ballot_sync(0xffffffffu, cold);
+            if (!cold) continue;
+            const uint32_t r = (uint32_t)(slot[i] >> K.shift) * (uint32_t)K.stripes + stripe;
+            const unsigned peers = __match_any_sync(act, r);
+            const int leader = __ffs(peers) - 1;
+            uint32_t pos = 0, cap = 0;
+            long long base = 0;
+            if ((int)lane == leader) {
+                pos = atomicAdd(&K.fill[r], (uint32_t)__popc(peers));
+                cap = K.cap[r];
+                base = K.base[r];
             }
+            pos = __shfl_sync(peers, pos, leader) + (uint32_t)__popc(peers & ((1u << lane) - 1u));
+            cap = __shfl_sync(peers, cap, leader);
+            base = __shfl_sync(peers, base, leader);
             if (pos < cap) {
                 const int64_t e = base + pos;
                 K.e_slot[e] = (uint32_t)slot[i];

@@ -310,7 +310,7 @@ static int64_t agg_out_name(uint16_t op, int64_t base) {
 
 td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
     if (!graphs || !roots || n < 0 || n > INT32_MAX) return TD_ERR_PTR(TD_ERR_RANGE);
-    atomic_store(&tdb_cancel_flag, 0);
+    tdb_cancel_reset();
     tdb_trace_begin();
     tdb_ctx c;
     int st = tdb_ctx_begin(&c);
@@ -398,6 +398,7 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
             if (cudaEventCreateWithFlags(&e->done[k], cudaEventDisableTiming) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; break; }
             if ((st = tdg_batch_plan_make(&dc, tile, ctas, &ch->plan))) break;
             ch->plan.query_base = ch->q0;
+            ch->plan.cancel = tdb_cancel_word();
             ch->ws = tdb_dev_alloc_persistent(ch->plan.ws_bytes);
             if (!ch->ws || alloc_outputs(ch, (int64_t*)e->d_rows + k)) { st = TD_ERR_OOM; break; }
             if ((st = tdg_batch_prepare(&dc, &ch->plan, ch->ws, c.stream))) break;
@@ -475,6 +476,7 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
         bchunk_t* ch = &e->ch[k];
         if (cudaEventSynchronize(e->done[k]) != cudaSuccess) { cudaGetLastError(); st = TD_ERR_IO; break; }
         tdb_trace("batch chunk computed");
+        if ((st = tdb_check_cancel())) break;          /* the kernel stopped taking work: partial rows */
         const int64_t rk = ((volatile int64_t*)e->h_rows)[k];
         if (rk < 0) { st = TD_ERR_DOMAIN; break; }     /* a key outside its statistics */
         void* src[TDG_MAX_AGGS + 2];

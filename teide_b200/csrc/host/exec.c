@@ -1412,7 +1412,7 @@ td_t* tdb_exec(td_graph_t* g, td_op_t* root, int dev_only) {
 
 td_t* td_execute(td_graph_t* g, td_op_t* root) {
     if (!g || !root) return TD_ERR_PTR(TD_ERR_NYI);
-    atomic_store(&tdb_cancel_flag, 0);
+    tdb_cancel_reset();
     tdb_trace_begin();
     td_t* r = tdb_exec(g, root, 0);
     tdb_trace("td_execute returns");
@@ -1422,7 +1422,7 @@ td_t* td_execute(td_graph_t* g, td_op_t* root) {
 td_t* td_execute_device(td_graph_t* g, td_op_t* root) {
     if (!g || !root) return TD_ERR_PTR(TD_ERR_NYI);
     if (root->opcode != OP_GROUP) return TD_ERR_PTR(TD_ERR_NYI);
-    atomic_store(&tdb_cancel_flag, 0);
+    tdb_cancel_reset();
     tdb_trace_begin();
     td_t* r = tdb_exec(g, root, 1);
     tdb_trace("td_execute_device returns");

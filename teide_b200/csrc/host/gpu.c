@@ -168,6 +168,37 @@ int tdb_gpu_ensure(void) {
 
 int tdb_check_cancel(void) { return atomic_load(&tdb_cancel_flag) ? TD_ERR_CANCEL : TD_OK; }
 
+/* The cancel request as a word kernels can read: page-locked host memory
+ * mapped into the device's address space, written by td_cancel and cleared
+ * when a query starts, so a running persistent kernel sees it between work
+ * items (Teide polls its flag per task and phase, pool.c:485-489,
+ * exec.c:168-182). */
+static volatile int32_t* cancel_h;
+static void* cancel_d;
+
+const volatile int32_t* tdb_cancel_word(void) {
+    pthread_mutex_lock(&mu);
+    if (!cancel_h && gpu_ready) {
+        void* h = NULL;
+        if (cudaHostAlloc(&h, 64, cudaHostAllocMapped | cudaHostAllocPortable) == cudaSuccess &&
+            cudaHostGetDevicePointer(&cancel_d, h, 0) == cudaSuccess) {
+            cancel_h = h;
+            *cancel_h = atomic_load(&tdb_cancel_flag);
+        } else {
+            cudaGetLastError();
+            if (h) cudaFreeHost(h);
+            cancel_d = NULL;
+        }
+    }
+    pthread_mutex_unlock(&mu);
+    return cancel_h ? (const volatile int32_t*)cancel_d : NULL;
+}
+
+void tdb_cancel_reset(void) {
+    atomic_store(&tdb_cancel_flag, 0);
+    if (cancel_h) *cancel_h = 0;
+}
+
 /* ---- resident mirrors ------------------------------------------------------------------ */
 typedef struct {
     td_t*      host;
@@ -836,6 +867,9 @@ void td_gpu_unpin(td_t* tbl) {
 /* ---- execution control ------------------------------------------------------------------- */
 td_err_t td_pool_init(uint32_t n_workers) { (void)n_workers; return TD_OK; }
 void td_pool_destroy(void) {}
-void td_cancel(void) { atomic_store(&tdb_cancel_flag, 1); }
+void td_cancel(void) {
+    atomic_store(&tdb_cancel_flag, 1);
+    if (cancel_h) *cancel_h = 1;                 /* seen by running kernels that poll it */
+}
 
 uint32_t td_thread_count(void) { return 1; }

@@ -110,6 +110,10 @@ void     tdb_mirror_forget(td_t* v);             /* host block freed or mutated 
 int     tdb_adopt_mirror(tdb_ctx* c, td_t* host, void* dptr);
 void     tdb_pin_host(td_t* v);                  /* page-lock a large host block */
 int      tdb_check_cancel(void);
+/* Device address of the cancel word (NULL before the GPU is initialized);
+ * tdb_cancel_reset clears it and the host flag when a query starts. */
+const volatile int32_t* tdb_cancel_word(void);
+void     tdb_cancel_reset(void);
 
 extern _Atomic(int) tdb_cancel_flag;
 

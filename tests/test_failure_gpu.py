@@ -149,3 +149,52 @@ def test_hash_wait_limit_returns_error(gpu):
     st = up(state2.data_ptr(), keys2.data_ptr(), 64, 1, (kv + 1).data_ptr(), n, 0, slot.data_ptr(),
             err.data_ptr(), None)
     assert st == 3                                  # TD_ERR_RANGE
+
+
+def test_cancel_stops_the_persistent_batch_kernel(gpu, tmp_path, monkeypatch):
+    """td_cancel while td_execute_batch runs: the persistent kernel polls the
+    cancel word between work items and takes no further item, and the call
+    returns TD_ERR_CANCEL -- or, when the cancel came too late, the whole
+    correct result.  The batch works normally afterwards."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(__file__))
+    from test_batch_gpu import run_batch
+    from teide_b200 import workloads
+    monkeypatch.setenv("TD_TUNE_CACHE", str(tmp_path / "tune.json"))
+    rows, ks = workloads.batch_shapes(n_queries=256, seed=91, rows=(50_000, 400_000), groups=(16, 20_000))
+    tables = [gpu.table(workloads.batch_query(int(r), int(k), seed=3000 + i)) for i, (r, k) in enumerate(zip(rows, ks))]
+    try:
+        want = run_batch(gpu, tables)
+        stop = threading.Event()
+
+        def canceller():
+            while not stop.is_set():
+                gpu.lib.td_cancel()
+
+        th = threading.Thread(target=canceller)
+        th.start()
+        outcomes = []
+        try:
+            for _ in range(20):
+                try:
+                    got = run_batch(gpu, tables)
+                    for k in want:
+                        assert np.array_equal(got[k], want[k]) or got[k].dtype.kind == "f", k
+                    outcomes.append("ok")
+                except TdError as e:
+                    assert e.code == TD_ERR_CANCEL
+                    outcomes.append("cancel")
+        finally:
+            stop.set()
+            th.join()
+        assert "cancel" in outcomes
+        again = run_batch(gpu, tables)
+        for k in want:
+            if want[k].dtype.kind == "f":
+                assert np.allclose(again[k], want[k], rtol=1e-12, atol=0), k
+            else:
+                assert np.array_equal(again[k], want[k]), k
+    finally:
+        for t in tables:
+            gpu.release(t)
