@@ -157,6 +157,11 @@ typedef struct tdg_group_plan {
     int64_t n_slots;       /* direct-array slots or hash-table capacity */
     int64_t max_groups;    /* capacity each output column must have */
     size_t  ws_bytes;      /* scratch the run needs */
+    int32_t ctas_per_sm;   /* launch shape of the streaming kernel (the vector forms of the
+                              group-by and of the fused join probe): persistent CTAs per SM,
+                              0 = as many as fit.  tdg_group_plan_make sets 0; the host's
+                              autotuner picks it per shape class. */
+    int32_t pad;
 } tdg_group_plan;
 
 typedef struct tdg_group_out {

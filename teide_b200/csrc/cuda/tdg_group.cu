@@ -100,6 +100,7 @@ struct GroupK {
     int32_t nk, na, method, n_acc;
     int32_t W;                    // 8-byte words per global slot record
     int32_t hot_cap;              // hot slots a CTA caches (0: no cache)
+    int32_t cps;                  // persistent CTAs per SM of the streaming kernel (0: all that fit)
     tdg_col key[TDG_MAX_KEYS];
     int64_t kmin[TDG_MAX_KEYS], krange[TDG_MAX_KEYS], stride[TDG_MAX_KEYS];
     int32_t op[TDG_MAX_AGGS];
@@ -1608,9 +1609,21 @@ static int kind_of(const tdg_agg& a) {
     }
 }
 
+// Grid of a streaming kernel: all CTAs that fit, or cps per SM when the
+// plan's launch shape asks for fewer; never more CTAs than work items.
+static int stream_grid(const void* kernel, int threads, size_t smem, int64_t items, int cps) {
+    int g = grid_for(kernel, threads, smem, items);
+    if (cps > 0) {
+        const int64_t cap = (int64_t)cps * sm_count();
+        if (g > cap) g = (int)cap;
+    }
+    return g;
+}
+
 static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws, int64_t nrows_bound) {
     GroupK G;
     memset(&G, 0, sizeof(G));
+    G.cps = p->ctas_per_sm;
     const int n_acc = count_acc(d);
     const bool sampled = group_sampled(d, p->method, p->smem != 0, p->n_slots, nrows_bound);
     const Layout L = layout_of(p->n_slots, n_acc, d->n_keys, p->method, sampled);
@@ -1837,7 +1850,7 @@ static bool launch_group_vec(const GroupK& G, const Pred& P, int pk, int mode, i
     bool launched = false;
 #define TDG_GV(NTV, NCV, MV)                                                                            \
     if (!launched && nt == NTV && nc == NCV && mode == MV) {                                            \
-        const int g = grid_for((const void*)k_group_vec<NTV, NCV, MV>, kThreads, smem, (n + 3) / 4);   \
+        const int g = stream_grid((const void*)k_group_vec<NTV, NCV, MV>, kThreads, smem, (n + 3) / 4, G.cps); \
         (note_launch(), k_group_vec<NTV, NCV, MV><<<g, kThreads, smem, s>>>(G, P, A, n));               \
         launched = true;                                                                                \
     }
@@ -1986,7 +1999,8 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     bool launched = false;
 #define TDG_PV(NTV, NCV)                                                                                  \
     if (vec && !launched && nt == NTV && nc == NCV) {                                                     \
-        const int g = grid_for((const void*)k_probe_vec<NTV, NCV, uint32_t>, kThreads, smem, (n_left + 3) / 4); \
+        const int g = stream_grid((const void*)k_probe_vec<NTV, NCV, uint32_t>, kThreads, smem, (n_left + 3) / 4, \
+                                  G.cps);                                                                 \
         (note_launch(), k_probe_vec<NTV, NCV, uint32_t><<<g, kThreads, smem, s>>>(G, P, A, J->lkeys[0], J->kmin, \
                                                                                   J->n_slots, (const uint32_t*)map, n_left)); \
         launched = true;                                                                                  \

@@ -113,7 +113,7 @@ static void tune_key(const tdg_batch_desc* d, char* key, size_t n) {
     snprintf(key, n, "batch:q%d:r%d:s%d:a%d", q, r, s, d->n_aggs);
 }
 
-static int tune_load(const char* key, int64_t* tile, int32_t* ctas) {
+int tdb_tune_load(const char* key, int64_t* tile, int32_t* ctas) {
     char path[1024];
     tune_path(path, sizeof(path));
     FILE* f = fopen(path, "r");
@@ -135,7 +135,7 @@ static int tune_load(const char* key, int64_t* tile, int32_t* ctas) {
     return found;
 }
 
-static void tune_store(const char* key, int64_t tile, int32_t ctas) {
+void tdb_tune_store(const char* key, int64_t tile, int32_t ctas) {
     char path[1024], tmp[1100];
     tune_path(path, sizeof(path));
     /* keep other entries: one JSON object, one entry per line */
@@ -273,7 +273,7 @@ static float time_config(tdb_ctx* c, const tdg_batch_desc* d, int64_t tile, int3
 static void autotune(tdb_ctx* c, const tdg_batch_desc* d, int64_t* tile, int32_t* ctas) {
     char key[128];
     tune_key(d, key, sizeof(key));
-    if (tune_load(key, tile, ctas)) return;
+    if (tdb_tune_load(key, tile, ctas)) return;
     *tile = 0;
     *ctas = 0;
     if (getenv("TD_NO_AUTOTUNE")) return;
@@ -293,7 +293,7 @@ static void autotune(tdb_ctx* c, const tdg_batch_desc* d, int64_t* tile, int32_t
             if (ms > 0 && (best < 0 || ms < best)) { best = ms; *tile = tiles[i]; *ctas = ctass[j]; }
         }
     chunk_drop(&scratch);
-    if (best > 0) tune_store(key, *tile, *ctas);
+    if (best > 0) tdb_tune_store(key, *tile, *ctas);
 }
 
 static int64_t agg_out_name(uint16_t op, int64_t base) {

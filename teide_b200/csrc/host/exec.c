@@ -585,6 +585,98 @@ static bentry_t* bc_acquire(ex_t* x, const jrun_t* jr, const tdg_group_desc* d, 
     return e;
 }
 
+/* ---- launch-shape autotuner of the streaming kernels ------------------------------------
+ * The vector kernels of the group-by and of the fused join probe run as many
+ * persistent CTAs per SM as fit unless the plan says otherwise.  The first
+ * time a shape class -- method, log2 of the rows and of the slots, the
+ * number of aggregates, join or not -- of at least 2^22 rows is met, the
+ * query runs once per candidate CTAs-per-SM value with CUDA events around
+ * the call; the fastest is kept in memory and in the tuner's JSON file
+ * ($TD_TUNE_CACHE), so later queries of that class, in this process or a
+ * later one, launch with it.  Every candidate run computes the whole
+ * result, so the query's answer is the last run's.  Teide's counterparts
+ * are fixed constants (td.h:190-197 morsel sizes, exec.c:4230-4233 radix
+ * fan-out).  TD_NO_AUTOTUNE in the environment keeps the defaults. */
+#define TDB_TUNE_MIN_ROWS ((int64_t)1 << 22)
+#define TDB_TUNE_MEM 64
+static pthread_mutex_t tn_mu = PTHREAD_MUTEX_INITIALIZER;
+static struct { char key[64]; int32_t cps; } tn_mem[TDB_TUNE_MEM];
+static int tn_n;
+
+static int ilog2(int64_t x) { int k = 0; while (x > 1) { x >>= 1; k++; } return k; }
+
+static void tune_key(const tdg_group_desc* d, const tdg_group_plan* p, int join, char* key, size_t n) {
+    snprintf(key, n, "stream:m%d:s%d:r%d:g%d:k%d:a%d:j%d", p->method, p->smem, ilog2(d->nrows), ilog2(p->n_slots),
+             d->n_keys, d->n_aggs, join);
+}
+
+/* 1 and *cps when the class is known (in memory, else in the JSON file). */
+static int tune_lookup(const char* key, int32_t* cps) {
+    int found = 0;
+    pthread_mutex_lock(&tn_mu);
+    for (int i = 0; i < tn_n && !found; i++)
+        if (!strcmp(tn_mem[i].key, key)) { *cps = tn_mem[i].cps; found = 1; }
+    pthread_mutex_unlock(&tn_mu);
+    if (found) return 1;
+    int64_t tile = 0;
+    if (!tdb_tune_load(key, &tile, cps)) return 0;
+    pthread_mutex_lock(&tn_mu);
+    if (tn_n < TDB_TUNE_MEM) { snprintf(tn_mem[tn_n].key, sizeof(tn_mem[0].key), "%s", key); tn_mem[tn_n++].cps = *cps; }
+    pthread_mutex_unlock(&tn_mu);
+    return 1;
+}
+
+static void tune_remember(const char* key, int32_t cps) {
+    pthread_mutex_lock(&tn_mu);
+    if (tn_n < TDB_TUNE_MEM) { snprintf(tn_mem[tn_n].key, sizeof(tn_mem[0].key), "%s", key); tn_mem[tn_n++].cps = cps; }
+    pthread_mutex_unlock(&tn_mu);
+    tdb_tune_store(key, 0, cps);
+}
+
+typedef struct {
+    const jrun_t* jr;
+    const tdg_expr* pp;
+    const uint64_t* dsel;
+    const tdg_group_desc* d;
+    tdg_group_plan* plan;
+    void* ws;
+    const tdg_group_out* out;
+    void* stream;
+} grun_t;
+
+static int grun(void* a) {
+    grun_t* r = a;
+    if (r->jr)
+        return tdg_join_group_run(r->jr->jd, r->jr->jp, r->jr->jws, r->pp, r->dsel, r->d, r->plan, r->ws, r->out,
+                                  r->stream);
+    return tdg_group_run(r->d, r->pp, r->dsel, r->plan, r->ws, r->out, r->stream);
+}
+
+/* Runs the query, first choosing the plan's launch shape for its class. */
+static int run_tuned(ex_t* x, grun_t* r) {
+    if (r->d->nrows < TDB_TUNE_MIN_ROWS || getenv("TD_NO_AUTOTUNE")) return grun(r);
+    char key[64];
+    tune_key(r->d, r->plan, r->jr != NULL, key, sizeof(key));
+    int32_t cps = 0;
+    if (tune_lookup(key, &cps)) {
+        r->plan->ctas_per_sm = cps;
+        return grun(r);
+    }
+    static const int32_t cand[] = {1, 2, 4, 0};      /* 0 (all that fit) last: its result is kept */
+    float best = -1.f;
+    int32_t best_cps = 0;
+    int st = TD_OK;
+    for (int i = 0; i < 4; i++) {
+        r->plan->ctas_per_sm = cand[i];
+        const float ms = tdb_time_call(&x->c, grun, r, &st);
+        if (st) return st;
+        if (ms > 0 && (best < 0 || ms < best)) { best = ms; best_cps = cand[i]; }
+    }
+    if (best > 0) tune_remember(key, best_cps);
+    r->plan->ctas_per_sm = best_cps;
+    return TD_OK;
+}
+
 static void bc_release(bentry_t* e) {
     pthread_mutex_lock(&bc_mu);
     e->users--;
@@ -702,11 +794,14 @@ static td_t* run_group(ex_t* x, td_op_ext_t* ext, td_t* tbl, const tdg_expr* pre
             st = CALL(tdg_join_group_run(&jd, &be->jp, be->jws, pp, dsel, &d, &plan, ws, &out, x->c.stream));
             bc_release(be);
         }
-        if (!be || st == TD_ERR_RANGE)      /* no kept map, or this plan cannot use it */
-            st = CALL(tdg_join_group_run(jr->jd, jr->jp, jr->jws, pp, dsel, &d, &plan, ws, &out, x->c.stream));
+        if (!be || st == TD_ERR_RANGE) {    /* no kept map, or this plan cannot use it */
+            grun_t r = { jr, pp, dsel, &d, &plan, ws, &out, x->c.stream };
+            st = CALL(run_tuned(x, &r));
+        }
         tdb_note_methods(plan.method, jr->jp->method, 1);
     } else {
-        st = CALL(tdg_group_run(&d, pp, dsel, &plan, ws, &out, x->c.stream));
+        grun_t r = { NULL, pp, dsel, &d, &plan, ws, &out, x->c.stream };
+        st = CALL(run_tuned(x, &r));
         tdb_note_methods(plan.method, 0, pp != NULL);
     }
     if (st) return TD_ERR_PTR(st);

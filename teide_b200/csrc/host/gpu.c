@@ -864,6 +864,28 @@ void td_gpu_unpin(td_t* tbl) {
     for (int64_t j = 0; j < td_table_ncols(tbl); j++) tdb_mirror_forget(td_table_get_col_idx(tbl, j));
 }
 
+float tdb_time_call(tdb_ctx* c, int (*run)(void*), void* arg, int* st) {
+    cudaEvent_t a = NULL, b = NULL;
+    cudaStream_t s = (cudaStream_t)c->stream;
+    float ms = -1.f;
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess) {
+        cudaGetLastError();
+        if (a) cudaEventDestroy(a);
+        *st = run(arg);
+        return -1.f;
+    }
+    cudaEventRecord(a, s);
+    *st = run(arg);
+    cudaEventRecord(b, s);
+    if (cudaEventSynchronize(b) != cudaSuccess || cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();
+        ms = -1.f;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return ms;
+}
+
 /* ---- execution control ------------------------------------------------------------------- */
 td_err_t td_pool_init(uint32_t n_workers) { (void)n_workers; return TD_OK; }
 void td_pool_destroy(void) {}

@@ -131,6 +131,15 @@ int   tdb_col_resident(td_t* col);
  * one); 0 when the column has none or is a slice. */
 uint64_t tdb_col_stamp(td_t* col);
 
+/* ---- autotuner persistence (host/batch.c) ------------------------------------------
+ * One JSON object in $TD_TUNE_CACHE (else ~/.cache/teide_b200_tune.json), one
+ * entry per shape class: {"tile_rows": T, "ctas_per_sm": C}. */
+int   tdb_tune_load(const char* key, int64_t* tile, int32_t* ctas);
+void  tdb_tune_store(const char* key, int64_t tile, int32_t ctas);
+/* Milliseconds the GPU spends on run(arg), queued on c's stream (CUDA events
+ * on both sides); *st receives run's status.  Negative when not measured. */
+float tdb_time_call(tdb_ctx* c, int (*run)(void*), void* arg, int* st);
+
 /* ---- shared join builds (host/exec.c) ----------------------------------------------
  * While a thread's flag is set, fused join -> group-by queries over resident
  * build tables reuse one payload map per build side (td_server's workers set

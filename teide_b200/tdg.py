@@ -40,7 +40,8 @@ class GroupDesc(C.Structure):
 
 class GroupPlan(C.Structure):
     _fields_ = [("method", C.c_int32), ("smem", C.c_int32), ("n_slots", C.c_int64),
-                ("max_groups", C.c_int64), ("ws_bytes", C.c_size_t)]
+                ("max_groups", C.c_int64), ("ws_bytes", C.c_size_t), ("ctas_per_sm", C.c_int32),
+                ("pad", C.c_int32)]
 
 
 class GroupOut(C.Structure):

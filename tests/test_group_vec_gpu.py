@@ -187,3 +187,25 @@ def test_partition_long_runs(gpu):
         _same(_run(gpu, t, [("flag", "ne", 3)], AGGS5), _want(d, [("flag", "ne", 3)], AGGS5))
     finally:
         gpu.release(t)
+
+
+def test_autotuned_launch_shape(gpu, tmp_path, monkeypatch):
+    """A streaming group-by of 2^22 rows or more is first run once per
+    candidate CTAs-per-SM value; the fastest is recorded in the tuner's JSON
+    file under a "stream:" key and reused.  The tuned call and a later call
+    of the same shape class both equal the oracle."""
+    import json
+    cache = tmp_path / "tune.json"
+    monkeypatch.setenv("TD_TUNE_CACHE", str(cache))
+    n = (1 << 22) + 6
+    d = _data(n, 97, lo=-3, span=301)           # a shape class no other test in this file uses
+    aggs = [(OP_SUM, "qty"), (OP_MIN, "amount"), (OP_MAX, "qty"), (OP_COUNT, "qty"), (OP_SUM, "amount")]
+    tbl = gpu.table(d)
+    first = _run(gpu, tbl, [("flag", "ne", 2)], aggs)
+    entries = json.loads(cache.read_text())
+    stream = {k: v for k, v in entries.items() if k.startswith("stream:")}
+    assert len(stream) == 1 and list(stream.values())[0]["ctas_per_sm"] in (0, 1, 2, 4)
+    again = _run(gpu, tbl, [("flag", "ne", 2)], aggs)
+    gpu.release(tbl)
+    _same(first, _want(d, [("flag", "ne", 2)], aggs))
+    _same(again, _want(d, [("flag", "ne", 2)], aggs))
