@@ -795,8 +795,8 @@ __device__ __forceinline__ uint64_t evict_last_policy() {
 }
 
 // The four rows of a thread once their key (fk) and value columns (cv) are
-// in registers: predicate, slot, and the aggregate updates.  vec_tile loads
-// them from global memory; the ring kernel from its shared-memory stages.
+// in registers (vec_stream loads them): predicate, slot, and the aggregate
+// updates.
 template <int NT, int NC, int MODE, bool MAP, typename PT>
 __device__ __forceinline__ void vec_rows(const GroupK& G, const SmemView& V, const Pred& P, const VecAgg& A,
                                          const int64_t (&row)[4], const long long (&fk)[4],
@@ -973,43 +973,25 @@ __device__ __forceinline__ void vec_load(const VecAgg& A, const tdg_col& kcol, i
     }
 }
 
-template <int NT, int NC, int MODE, bool MAP, typename PT = uint32_t>
-__device__ __forceinline__ void vec_tile(const GroupK& G, const SmemView& V, const Pred& P, const VecAgg& A,
-                                         const tdg_col& kcol, int64_t kmin, int64_t n_map,
-                                         const PT* __restrict__ map, int64_t n, int64_t base,
-                                         uint64_t pol = 0) {
-    int64_t row[4];
-    long long fk[4], cv[NC > 0 ? NC : 1][4];
-    vec_load<NC>(A, kcol, n, base, fk, cv);
-    tile_rows(base, row);
-    vec_rows<NT, NC, MODE, MAP, PT>(G, V, P, A, row, fk, cv, kmin, n_map, map, n, pol);
-}
-
-// The probe's double buffer holds a second tile of columns in registers, so
-// it is bounded for 4 resident CTAs (64 registers) instead of TDG_MINB.
-constexpr int kProbeMinBlocks = 4;
-
-template <int NT, int NC, typename PT>
-__global__ void __launch_bounds__(kThreads, kProbeMinBlocks) k_probe_vec(const GroupK G, const Pred P, const VecAgg A,
-                                                                  const tdg_col lkey, int64_t kmin, int64_t n_map,
-                                                                  const PT* __restrict__ map, int64_t n) {
-    extern __shared__ unsigned long long sm[];
-    const SmemView V = smem_setup<0>(G, sm);
-    const uint64_t pol = evict_last_policy();
+// The grid-stride loop of the vector kernels.  Registers double-buffer the
+// columns: the next tile's loads are issued before this tile's map reads and
+// shared-memory updates wait on theirs.  (An L2 bulk prefetch of the next
+// tile instead re-read about 16% of the streamed bytes from DRAM in the join
+// probe: prefetched lines left L2 before their loads.)
+template <int NT, int NC, int MODE, bool MAP, typename PT>
+__device__ __forceinline__ void vec_stream(const GroupK& G, const SmemView& V, const Pred& P, const VecAgg& A,
+                                           const tdg_col& kcol, int64_t kmin, int64_t n_map,
+                                           const PT* __restrict__ map, int64_t n, uint64_t pol) {
     const int64_t tile = (int64_t)kThreads * 4, stride = (int64_t)gridDim.x * tile;
-    // Registers double-buffer the columns: the next tile's loads are issued
-    // before this tile's map reads and shared-memory updates wait on theirs.
-    // (An L2 bulk prefetch of the next tile instead re-read about 16% of the
-    // streamed bytes from DRAM: prefetched lines left L2 before their loads.)
     long long fk[4], cv[NC > 0 ? NC : 1][4];
     int64_t base = (int64_t)blockIdx.x * tile;
-    if (base < n) vec_load<NC>(A, lkey, n, base, fk, cv);
+    if (base < n) vec_load<NC>(A, kcol, n, base, fk, cv);
     for (; base < n; base += stride) {
         long long fk2[4] = {0, 0, 0, 0}, cv2[NC > 0 ? NC : 1][4] = {};
-        if (base + stride < n) vec_load<NC>(A, lkey, n, base + stride, fk2, cv2);
+        if (base + stride < n) vec_load<NC>(A, kcol, n, base + stride, fk2, cv2);
         int64_t row[4];
         tile_rows(base, row);
-        vec_rows<NT, NC, 0, true, PT>(G, V, P, A, row, fk, cv, kmin, n_map, map, n, pol);
+        vec_rows<NT, NC, MODE, MAP, PT>(G, V, P, A, row, fk, cv, kmin, n_map, map, n, pol);
 #pragma unroll
         for (int i = 0; i < 4; i++) {
             fk[i] = fk2[i];
@@ -1017,6 +999,20 @@ __global__ void __launch_bounds__(kThreads, kProbeMinBlocks) k_probe_vec(const G
             for (int c = 0; c < NC; c++) cv[c][i] = cv2[c][i];
         }
     }
+}
+
+// The double buffer holds a second tile of columns in registers, so the
+// probe is bounded for 4 resident CTAs (64 registers) where the others use
+// TDG_MINB.
+constexpr int kVecMinBlocks = 4;
+
+template <int NT, int NC, typename PT>
+__global__ void __launch_bounds__(kThreads, kVecMinBlocks) k_probe_vec(const GroupK G, const Pred P, const VecAgg A,
+                                                                       const tdg_col lkey, int64_t kmin, int64_t n_map,
+                                                                       const PT* __restrict__ map, int64_t n) {
+    extern __shared__ unsigned long long sm[];
+    const SmemView V = smem_setup<0>(G, sm);
+    vec_stream<NT, NC, 0, true, PT>(G, V, P, A, lkey, kmin, n_map, map, n, evict_last_policy());
     smem_flush<0>(G, V);
 }
 
@@ -1024,6 +1020,10 @@ __global__ void __launch_bounds__(kThreads, kProbeMinBlocks) k_probe_vec(const G
 // use more registers.
 constexpr int kVecHotMinBlocks = 3;
 
+// The plain group-by keeps single-buffered tiles with an L2 bulk prefetch of
+// the CTA's next tile: the double buffer of the probe measured no faster for
+// MODE 0 and 13% slower for MODE 3, which is issue-bound and loses occupancy
+// to the extra registers.
 template <int NT, int NC, int MODE>
 __global__ void __launch_bounds__(kThreads, MODE == 0 ? TDG_MINB : kVecHotMinBlocks)
 k_group_vec(const GroupK G, const Pred P, const VecAgg A, int64_t n) {
@@ -1033,7 +1033,11 @@ k_group_vec(const GroupK G, const Pred P, const VecAgg A, int64_t n) {
     for (int64_t base = (int64_t)blockIdx.x * tile; base < n; base += (int64_t)gridDim.x * tile) {
         const int64_t nb = base + (int64_t)gridDim.x * tile;
         prefetch_rows(G.pf, nb, nb + tile < n ? nb + tile : n);
-        vec_tile<NT, NC, MODE, false>(G, V, P, A, G.key[0], G.kmin[0], G.krange[0], (const uint32_t*)nullptr, n, base);
+        long long fk[4], cv[NC > 0 ? NC : 1][4];
+        int64_t row[4];
+        vec_load<NC>(A, G.key[0], n, base, fk, cv);
+        tile_rows(base, row);
+        vec_rows<NT, NC, MODE, false, uint32_t>(G, V, P, A, row, fk, cv, G.kmin[0], G.krange[0], nullptr, n, 0);
     }
     if (MODE == 0 || V.n_hot) smem_flush<MODE>(G, V);
 }
