@@ -399,6 +399,7 @@ struct EventTimer {
     void start(cudaStream_t s);
     void stop(cudaStream_t s);
     float ms();                        // valid after the stream has synchronized
+    ~EventTimer();                     // returns the events if ms() was not called
 };
 bool timing_on();
 void set_last_main_ms(float ms);

@@ -28,10 +28,40 @@ int sm_count() {
     return g_sms;
 }
 
-int grid_for(const void* kernel, int threads, size_t smem, int64_t work_items) {
+// Resident CTAs per SM of (kernel, threads, shared memory) on the current
+// device; the occupancy query costs microseconds of host time, which sit on
+// the critical path of a query's first launch, so each thread keeps its
+// answers.
+static int occupancy(const void* kernel, int threads, size_t smem) {
+    struct Entry { const void* k; int threads; int dev; size_t smem; int per_sm; };
+    constexpr int kCap = 64;
+    static thread_local Entry cache[kCap];
+    static thread_local int n_cached, next_victim;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    for (int i = 0; i < n_cached; i++) {
+        const Entry& e = cache[i];
+        if (e.k == kernel && e.threads == threads && e.smem == smem && e.dev == dev) return e.per_sm;
+    }
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1)
-        per_sm = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        return 1;                               // not cached: the next call asks again
+    }
+    // a full cache replaces its entries in turn
+    int at;
+    if (n_cached < kCap) {
+        at = n_cached++;
+    } else {
+        at = next_victim;
+        next_victim = (next_victim + 1) % kCap;
+    }
+    cache[at] = Entry{kernel, threads, dev, smem, per_sm};
+    return per_sm;
+}
+
+int grid_for(const void* kernel, int threads, size_t smem, int64_t work_items) {
+    const int per_sm = occupancy(kernel, threads, smem);
     int64_t g = (int64_t)per_sm * sm_count();
     int64_t need = (work_items + threads - 1) / threads;
     if (need < g) g = need < 1 ? 1 : need;
@@ -64,21 +94,68 @@ void set_last_build_ms(float ms) { g_build_ms.store(ms); }
 static std::atomic<float> g_sort_ms{0.f};
 void set_last_sort_ms(float ms) { g_sort_ms.store(ms); }
 
+// CUDA events for the timers, kept per host thread and device: creating and
+// destroying two events per timed launch cost several microseconds of host
+// time before the launch.  Freed when the thread exits.
+namespace {
+struct EventPool {
+    cudaEvent_t ev[16] = {};
+    int dev[16] = {};
+    bool used[16] = {};
+    ~EventPool() {
+        for (int i = 0; i < 16; i++)
+            if (ev[i]) cudaEventDestroy(ev[i]);
+    }
+};
+thread_local EventPool t_events;
+
+cudaEvent_t event_take() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    EventPool& P = t_events;
+    for (int i = 0; i < 16; i++)
+        if (P.ev[i] && !P.used[i] && P.dev[i] == dev) { P.used[i] = true; return P.ev[i]; }
+    for (int i = 0; i < 16; i++)
+        if (!P.ev[i]) {
+            if (cudaEventCreate(&P.ev[i]) != cudaSuccess) { cudaGetLastError(); P.ev[i] = nullptr; return nullptr; }
+            P.dev[i] = dev;
+            P.used[i] = true;
+            return P.ev[i];
+        }
+    cudaEvent_t e = nullptr;                    // pool full: a transient event
+    if (cudaEventCreate(&e) != cudaSuccess) { cudaGetLastError(); return nullptr; }
+    return e;
+}
+
+void event_give(cudaEvent_t e) {
+    if (!e) return;
+    EventPool& P = t_events;
+    for (int i = 0; i < 16; i++)
+        if (P.ev[i] == e) { P.used[i] = false; return; }
+    cudaEventDestroy(e);
+}
+}  // namespace
+
 void EventTimer::start(cudaStream_t s) {
     on = timing_on();
     if (!on) return;
-    if (!a) cudaEventCreate(&a);
-    if (!b) cudaEventCreate(&b);
+    if (!a) a = event_take();
+    if (!b) b = event_take();
+    if (!a || !b) { on = false; return; }
     cudaEventRecord(a, s);
 }
 void EventTimer::stop(cudaStream_t s) {
     if (on) cudaEventRecord(b, s);
 }
+EventTimer::~EventTimer() {
+    event_give(a);
+    event_give(b);
+}
 float EventTimer::ms() {
     float t = 0.f;
     if (on && cudaEventElapsedTime(&t, a, b) != cudaSuccess) { cudaGetLastError(); t = 0.f; }
-    if (a) cudaEventDestroy(a);
-    if (b) cudaEventDestroy(b);
+    event_give(a);
+    event_give(b);
     a = b = nullptr;
     return t;
 }

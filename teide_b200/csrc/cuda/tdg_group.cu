@@ -127,6 +127,8 @@ struct OutK {
     void* keys[TDG_MAX_KEYS];
     int32_t kesz[TDG_MAX_KEYS];
     void* aggs[TDG_MAX_AGGS];
+    const int32_t* err;           // the run's error word and repeated-key flag ...
+    int32_t* herr;                // ... copied here (device-mapped host words) by the emit, if set
 };
 
 __device__ __forceinline__ unsigned long long* grec(const GroupK& G, int64_t s) { return G.rec + s * G.W; }
@@ -611,7 +613,12 @@ __global__ void __launch_bounds__(kThreads) k_payload_build(const GroupK G, cons
 
 // The common build shape -- an 8-byte join key and one 8-byte group key on
 // the build side, both 16-byte aligned -- four rows per thread: two 16-byte
-// loads per column, then four independent CASes in flight at once.
+// loads per column, then four independent map writes in flight at once.
+// STORE (the key range holds exactly as many slots as there are build rows):
+// plain stores, since then the keys are distinct exactly when every slot is
+// written, which k_map_holes checks afterwards; otherwise a CAS per key both
+// stores the slot and detects a repeated key.
+template <bool STORE>
 __global__ void __launch_bounds__(kThreads) k_payload_build_vec(const long long* __restrict__ jk,
                                                                 const long long* __restrict__ gk, int64_t jmin,
                                                                 int64_t n_slots, int64_t gmin, int64_t grange,
@@ -639,10 +646,30 @@ __global__ void __launch_bounds__(kThreads) k_payload_build_vec(const long long*
             const int64_t kk = k[i] - jmin, d = g[i] - gmin;
             on[i] = r0 + i < n;
             if (on[i] && (kk < 0 || kk >= n_slots || d < 0 || d >= grange)) { set_err(err, E_DOMAIN); on[i] = false; }
-            old[i] = on[i] ? atomicCAS(map + kk, 0xFFFFFFFFu, (uint32_t)(d * gstride)) : 0xFFFFFFFFu;
+            if (STORE) {
+                if (on[i]) map[kk] = (uint32_t)(d * gstride);
+                old[i] = 0xFFFFFFFFu;
+            } else {
+                old[i] = on[i] ? atomicCAS(map + kk, 0xFFFFFFFFu, (uint32_t)(d * gstride)) : 0xFFFFFFFFu;
+            }
         }
-        if ((old[0] & old[1] & old[2] & old[3]) != 0xFFFFFFFFu) atomicExch(dup, 1);
+        if (!STORE && (old[0] & old[1] & old[2] & old[3]) != 0xFFFFFFFFu) atomicExch(dup, 1);
     }
+}
+
+// After a STORE build: an empty entry means some key was written twice (n
+// keys into n slots), so the repeated-key flag is raised.  16-byte loads; the
+// map was just written and is read from L2.
+__global__ void __launch_bounds__(kThreads) k_map_holes(const uint32_t* __restrict__ map, int64_t n, int32_t* dup) {
+    bool hole = false;
+    const int64_t n4 = n >> 2;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n4; i += (int64_t)gridDim.x * blockDim.x) {
+        const uint4 v = ((const uint4*)map)[i];
+        hole |= v.x == 0xFFFFFFFFu || v.y == 0xFFFFFFFFu ||
+                v.z == 0xFFFFFFFFu || v.w == 0xFFFFFFFFu;
+    }
+    if (blockIdx.x == 0 && (int64_t)threadIdx.x < (n & 3)) hole |= map[(n4 << 2) + threadIdx.x] == 0xFFFFFFFFu;
+    if (__syncthreads_or(hole) && threadIdx.x == 0) atomicExch(dup, 1);
 }
 
 static void launch_payload_build(const GroupK& G, const JoinK& J, uint32_t* map, int64_t n_right, cudaStream_t s) {
@@ -653,10 +680,21 @@ static void launch_payload_build(const GroupK& G, const JoinK& J, uint32_t* map,
                      J.rkeys[0].type != T_F64 && elem_size(G.key[gi].type, G.key[gi].attrs) == 8 &&
                      (((uintptr_t)J.rkeys[0].data | (uintptr_t)G.key[gi].data) & 15) == 0;
     if (vec) {
-        const int g = grid_for((const void*)k_payload_build_vec, kThreads, 0, (n_right + 3) / 4);
-        (note_launch(), k_payload_build_vec<<<g, kThreads, 0, s>>>(
-            (const long long*)J.rkeys[0].data, (const long long*)G.key[gi].data, J.kmin, J.n_slots, G.kmin[gi],
-            G.krange[gi], G.stride[gi], map, n_right, G.err, G.err + 1));
+        const bool store = J.n_slots == n_right && ((uintptr_t)map & 15) == 0;
+        const void* k = store ? (const void*)k_payload_build_vec<true> : (const void*)k_payload_build_vec<false>;
+        const int g = grid_for(k, kThreads, 0, (n_right + 3) / 4);
+        if (store)
+            (note_launch(), k_payload_build_vec<true><<<g, kThreads, 0, s>>>(
+                (const long long*)J.rkeys[0].data, (const long long*)G.key[gi].data, J.kmin, J.n_slots, G.kmin[gi],
+                G.krange[gi], G.stride[gi], map, n_right, G.err, G.err + 1));
+        else
+            (note_launch(), k_payload_build_vec<false><<<g, kThreads, 0, s>>>(
+                (const long long*)J.rkeys[0].data, (const long long*)G.key[gi].data, J.kmin, J.n_slots, G.kmin[gi],
+                G.krange[gi], G.stride[gi], map, n_right, G.err, G.err + 1));
+        if (store) {
+            const int gh = grid_for((const void*)k_map_holes, kThreads, 0, (J.n_slots + 3) / 4);
+            (note_launch(), k_map_holes<<<gh, kThreads, 0, s>>>(map, J.n_slots, G.err + 1));
+        }
     } else {
         const int g = grid_for((const void*)k_payload_build<uint32_t>, kThreads, 0, n_right);
         (note_launch(), k_payload_build<uint32_t><<<g, kThreads, 0, s>>>(G, J, map, n_right, G.err + 1));
@@ -1313,6 +1351,7 @@ __global__ void __launch_bounds__(kThreads) k_group_unmatched(GroupK G, const Jo
 // 32*W consecutive words, so every store instruction writes 256 contiguous
 // bytes (no partial-sector read-modify-write in L2).
 __global__ void k_group_init(const GroupK G) {
+    if (blockIdx.x == 0 && threadIdx.x < 64) G.err[threadIdx.x] = 0;     // the 256-byte error area
     const int lane = threadIdx.x & 31;
     const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -1445,10 +1484,14 @@ __global__ void __launch_bounds__(1024) k_emit_small(const GroupK G, const OutK 
         if (c) emit_one(G, O, s, r, c, out + pre);
         out += tot;
     }
-    if (threadIdx.x == 0) *d_total = out;
+    if (threadIdx.x == 0) {
+        *d_total = out;
+        if (O.herr) { O.herr[0] = O.err[0]; O.herr[1] = O.err[1]; }
+    }
 }
 
-__global__ void __launch_bounds__(1024) k_scan_counts_g(int64_t* counts, int64_t m, int64_t* d_total) {
+__global__ void __launch_bounds__(1024) k_scan_counts_g(int64_t* counts, int64_t m, int64_t* d_total,
+                                                        const int32_t* err, int32_t* herr) {
     __shared__ long long part[1024];
     const int64_t per = (m + blockDim.x - 1) / blockDim.x;
     const int64_t b = threadIdx.x * per, e = b + per < m ? b + per : m;
@@ -1465,6 +1508,7 @@ __global__ void __launch_bounds__(1024) k_scan_counts_g(int64_t* counts, int64_t
     long long run = threadIdx.x ? part[threadIdx.x - 1] : 0;
     for (int64_t i = b; i < e; i++) { long long c = counts[i]; counts[i] = run; run += c; }
     if (threadIdx.x == blockDim.x - 1 && d_total) *d_total = part[blockDim.x - 1];
+    if (threadIdx.x == 0 && herr) { herr[0] = err[0]; herr[1] = err[1]; }
 }
 
 // ---- host side: layout, plan, launch ----------------------------------------------------
@@ -1729,7 +1773,6 @@ static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws
 }
 
 static tdg_status prepare(const GroupK& G, cudaStream_t s) {
-    cudaMemsetAsync(G.err, 0, 256, s);
     const int g = grid_for((const void*)k_group_init, kThreads, 0, G.S);
     (note_launch(), k_group_init<<<g, kThreads, 0, s>>>(G));
     if (G.hot_cap) {
@@ -1741,12 +1784,42 @@ static tdg_status prepare(const GroupK& G, cudaStream_t s) {
     return launch_status();
 }
 
-// A few page-locked words per host thread for status read-backs.
-static int32_t* pinned_words() {
-    static thread_local int32_t* w = nullptr;
+// A few device-mapped page-locked words per host thread: kernels write
+// status words there and the host reads them once the stream has
+// synchronized, with no copy.  Freed when the thread exits.
+namespace {
+struct MappedWords {
+    int32_t* h = nullptr;
+    int32_t* d = nullptr;
+    ~MappedWords() {
+        if (h) cudaFreeHost(h);
+    }
+};
+}  // namespace
+
+static MappedWords* mapped_words() {
+    static thread_local MappedWords w;
     if (no_alloc()) return nullptr;
-    if (!w && cudaMallocHost((void**)&w, 64) != cudaSuccess) { cudaGetLastError(); w = nullptr; }
-    return w;
+    if (!w.h) {
+        void *h = nullptr, *d = nullptr;
+        if (cudaHostAlloc(&h, 64, cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        if (cudaHostGetDevicePointer(&d, h, 0) != cudaSuccess) {
+            cudaGetLastError();
+            cudaFreeHost(h);
+            return nullptr;
+        }
+        w.h = (int32_t*)h;
+        w.d = (int32_t*)d;
+    }
+    return &w;
+}
+
+static int32_t* pinned_words() {
+    MappedWords* m = mapped_words();
+    return m ? m->h : nullptr;
 }
 
 static tdg_status finish(const GroupK& G, const tdg_group_desc* d, void* ws, const tdg_group_out* out,
@@ -1758,6 +1831,11 @@ static tdg_status finish(const GroupK& G, const tdg_group_desc* d, void* ws, con
         O.kesz[k] = elem_size(d->keys[k].type, d->keys[k].attrs);
     }
     for (int a = 0; a < G.na; a++) O.aggs[a] = out->aggs[a];
+    // the emit copies the error word and the repeated-key flag into mapped
+    // host words; without them (no allocation allowed) they are copied
+    MappedWords* mw = mapped_words();
+    O.err = G.err;
+    O.herr = mw ? mw->d : nullptr;
     if (G.S <= kSmallEmit) {
         (note_launch(), k_emit_small<<<1, 1024, 0, s>>>(G, O, out->d_n_groups));
     } else {
@@ -1765,19 +1843,18 @@ static tdg_status finish(const GroupK& G, const tdg_group_desc* d, void* ws, con
         int64_t* counts = (int64_t*)((char*)ws + L.emit);
         const int64_t chunks = (G.S + kEmitChunk - 1) / kEmitChunk;
         (note_launch(), k_emit_count<<<(unsigned)chunks, kThreads, 0, s>>>(G, counts));
-        (note_launch(), k_scan_counts_g<<<1, 1024, 0, s>>>(counts, chunks, out->d_n_groups));
+        (note_launch(), k_scan_counts_g<<<1, 1024, 0, s>>>(counts, chunks, out->d_n_groups, O.err, O.herr));
         (note_launch(), k_emit<<<(unsigned)chunks, kThreads, 0, s>>>(G, O, counts));
     }
     tdg_status st = launch_status();
     if (st) return st;
-    int32_t* err = pinned_words();               // page-locked: the copy is asynchronous
     int32_t local[2] = {0, 0};
-    int32_t* dst = err ? err : local;
-    dst[0] = dst[1] = 0;
-    if (cudaMemcpyAsync(dst, G.err, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess) return E_IO;
+    if (!mw && cudaMemcpyAsync(local, G.err, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        return E_IO;
     if (cudaStreamSynchronize(s) != cudaSuccess) return E_IO;
-    if (flag1) *flag1 = dst[1];
-    return dst[0];
+    const volatile int32_t* w = mw ? mw->h : local;
+    if (flag1) *flag1 = w[1];
+    return w[0];
 }
 
 static bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
@@ -2001,7 +2078,8 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     tdg_status st = prepare(G, s);
     if (st) return st;
     // 32-bit entries: a native atomicCAS per build key both stores the slot
-    // and detects a repeated key, and 4 bytes per key keeps a 10M-row build
+    // and detects a repeated key (or, for dense keys, a plain store and a
+    // check for empty entries), and 4 bytes per key keeps a 10M-row build
     // side's map (40 MB) in L2.  (A 16-bit map with plain stores and a
     // duplicate bitmap measured slower on both passes.)  A prebuilt map was
     // checked for repeated keys when it was built.

@@ -226,7 +226,8 @@ __global__ void k_join_total(const int64_t* counts, int64_t chunks, int64_t* d_c
     *d_count = counts[chunks] + counts[chunks + 1];
 }
 
-__global__ void k_scan_counts_g(int64_t* counts, int64_t m, int64_t* d_total);   // tdg_group.cu
+__global__ void k_scan_counts_g(int64_t* counts, int64_t m, int64_t* d_total, const int32_t* err,
+                                int32_t* herr);   // tdg_group.cu
 
 static tdg_status jstatus(const JoinK& J, cudaStream_t s) {
     int32_t err = 0;
@@ -328,7 +329,7 @@ extern "C" tdg_status tdg_join_count(const tdg_join_desc* d, const tdg_join_plan
         else if (pk == 1) (note_launch(), k_join_count<1><<<(unsigned)chunks, kThreads, 0, s>>>(J, P, pr, d->n_left, counts));
         else (note_launch(), k_join_count<2><<<(unsigned)chunks, kThreads, 0, s>>>(J, P, pr, d->n_left, counts));
     }
-    (note_launch(), k_scan_counts_g<<<1, 1024, 0, s>>>(counts, chunks, counts + chunks));
+    (note_launch(), k_scan_counts_g<<<1, 1024, 0, s>>>(counts, chunks, counts + chunks, nullptr, nullptr));
     if (d->join_type == 2 && d->n_right > 0)
         (note_launch(), k_unmatched_count<<<1, kThreads, 0, s>>>(J.matched, d->n_right, counts + chunks + 1));
     (note_launch(), k_join_total<<<1, 1, 0, s>>>(counts, chunks, d_count));

@@ -89,3 +89,28 @@ def test_unaligned_probe_view_falls_back(gpu):
         gpu.release(view)
         gpu.release(bt)
         gpu.release(pt)
+
+
+@pytest.mark.parametrize("n_build", [50_000, 50_003, 7])
+def test_dense_build_keys_with_a_repeat(gpu, n_build):
+    """Build keys spanning exactly as many values as there are build rows are
+    written with plain stores and then checked for empty map entries: one key
+    written twice leaves one entry empty, and the query must then give the
+    join's true multiplicity (the general join), equal to the oracle's.  The
+    odd sizes reach the hole check's tail entries; without the repeat the
+    map path runs and must agree too."""
+    b, p = workloads.join_tables(n_build=n_build, n_probe=200_001, seed=83)
+    preds, aggs = CASES[0]
+    for repeat in (False, True):
+        bb = dict(b)
+        if repeat:
+            pk = bb["pk"].copy()
+            pk[pk == n_build - 2] = 1                   # min 0 and max n-1 stay: the span is still n_build
+            assert pk.min() == 0 and pk.max() == n_build - 1 and len(np.unique(pk)) == n_build - 1
+            bb["pk"] = pk
+        bt, pt = gpu.table(bb), gpu.table(p)
+        try:
+            _same(_run(gpu, bt, pt, preds, aggs), _want(bb, p, preds, aggs))
+        finally:
+            gpu.release(bt)
+            gpu.release(pt)
