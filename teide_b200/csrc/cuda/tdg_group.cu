@@ -64,7 +64,15 @@ constexpr int64_t kSampleMinRows = (int64_t)1 << 22;
 constexpr int kHotHist = 1024;                // sampled-count histogram buckets (hot threshold)
 // MODE 3 (partitioned cold rows)
 constexpr int64_t kPartMinRows = (int64_t)1 << 20;   // smaller inputs keep MODE 1
-constexpr size_t kPartSmem = 192 * 1024;      // a partition's shared-memory table (4096 slots at 5 words)
+// A partition's shared-memory table: 96 KB (2048 slots at 5 words), or 192 KB
+// from kPartWideSlots slots on.  Measured on 200M Zipf rows: with 2^14 and
+// 2^20 keys the partition pass aggregates dense items in the table, and the
+// larger table's one CTA per SM took 3.7 -> 6.3 ms and 4.4 -> 4.5 ms; with
+// 2^24 keys the items are sparse, and half as many partitions took
+// 5.7 -> 5.4 ms.
+constexpr size_t kPartSmem = 96 * 1024;
+constexpr size_t kPartSmemWide = 192 * 1024;
+constexpr int64_t kPartWideSlots = (int64_t)1 << 23;
 constexpr int kPartThreads = 512;
 constexpr int64_t kPartItem = 16384;          // entries per aggregation work item
 constexpr int kPartRegions = 1024;            // partitions below this are split into stripes
@@ -1196,6 +1204,18 @@ __global__ void __launch_bounds__(kPartThreads) k_part_agg(const GroupK G, const
         const int64_t e0 = K.base[r] + k * kPartItem;
         const int64_t e1 = K.base[r] + ((k + 1) * kPartItem < f ? (k + 1) * kPartItem : f);
         const bool sole = K.stripes == 1 && K.item_start[r + 1] - K.item_start[r] == 1;
+        if (threadIdx.x == 0) {
+            // the records of this item's partition and of the next claimed
+            // item's are brought into L2 with bulk prefetches, so the record
+            // updates below find their lines there instead of each waiting
+            // on DRAM
+            const int64_t n_ls = G.S - slot0 < PS ? G.S - slot0 : PS;
+            if (k == 0) l2_prefetch(grec(G, slot0), n_ls * G.W * 8);
+            if (next < n_items) {
+                const int64_t r2 = K.item_region[next], p2 = r2 / K.stripes, s2 = p2 << K.shift;
+                if (r2 != r) l2_prefetch(grec(G, s2), (G.S - s2 < PS ? G.S - s2 : PS) * G.W * 8);
+            }
+        }
         if (e1 - e0 < PS * kPartDense) {
             // sparse: a table would cost more to clear and merge than the
             // entries themselves; they update the records directly, which
@@ -1573,13 +1593,14 @@ struct PartLayout {
 
 // The MODE 3 section, placed after the rest of the workspace.  A partition
 // spans the slots whose shared-memory table (32-bit count, 8-byte
-// accumulators) fits kPartSmem; the entry buffers hold one entry per input row.
+// accumulators) fits kPartSmem (kPartSmemWide for wide key ranges); the entry buffers hold one entry per input row.
 static PartLayout part_layout(const tdg_group_desc* d, int64_t S, int n_acc, int64_t nrows) {
     PartLayout L;
     memset(&L, 0, sizeof(L));
     const size_t per = 4 + 8 * (size_t)n_acc;
     int shift = 0;
-    while (((size_t)2 << shift) * per <= kPartSmem) shift++;
+    const size_t table = S >= kPartWideSlots ? kPartSmemWide : kPartSmem;
+    while (((size_t)2 << shift) * per <= table) shift++;
     L.k.shift = shift;
     L.k.P = (S + ((int64_t)1 << shift) - 1) >> shift;
     int st = 1;
