@@ -10,7 +10,13 @@
 //                short queries balance across the 148 SMs;
 //   accumulate   a query with at most smem_slots slots (and a tile at least
 //                twice that long) aggregates its tile in shared memory and
-//                merges once; other tiles update the query's slot records in
+//                merges once; a query with more slots but at least
+//                kRowsPerSlot rows per slot is cut into key slices of at most
+//                smem_slots slots as well, and an item is then a (tile, slice)
+//                pair that aggregates only its slice's rows in shared memory
+//                (the slices of a tile are consecutive items, so the tile's
+//                columns are read from DRAM once and from L2 by the others);
+//                the remaining tiles update the query's slot records in
 //                global memory (L2-resident per query);
 //   emit         one CTA per query writes its non-empty slots, keys ascending,
 //                at the query's offset from an exclusive scan of group counts.
@@ -30,6 +36,7 @@ constexpr int kBatchMaxThreads = 1024;
 constexpr int64_t kDefaultTile = 16384;
 constexpr int kStaticSmemReserve = 256;   // the kernel's own __shared__ words
 constexpr int64_t kRowsPerSlot = 8;       // shared-path tiles hold >= 8 rows per slot
+constexpr int64_t kMaxSlices = 8;         // more key slices than this: global records instead
 constexpr int kBR = 4;                    // rows per thread per chunk
 constexpr int kEmitBlock = 256;
 constexpr int64_t kMaxDenseSlots = 1 << 20;
@@ -39,6 +46,7 @@ enum : int32_t { BK_COUNT = 0, BK_SUM_I, BK_SUM_F, BK_MIN_I, BK_MAX_I, BK_MIN_F,
 struct BQ {
     tdg_col key, val;
     int64_t nrows, key_min, n_slots, acc_off, first_item, tile_rows;
+    int64_t n_slices, slice_slots;    // key slices per tile (1: the whole key range)
 };
 
 struct BatchK {
@@ -195,10 +203,14 @@ __global__ void __launch_bounds__(kBatchMaxThreads) k_batch_agg(const BatchK B) 
         if (item >= B.n_items) break;
         const int q = B.item_q[item];
         const BQ Q = B.q[q];
-        const int64_t r0 = (item - Q.first_item) * Q.tile_rows;
+        const int64_t local = item - Q.first_item;
+        const int64_t tix = local / Q.n_slices, six = local - tix * Q.n_slices;
+        const int64_t r0 = tix * Q.tile_rows;
         const int64_t r1 = r0 + Q.tile_rows < Q.nrows ? r0 + Q.tile_rows : Q.nrows;
-        const bool use_smem = Q.n_slots <= B.smem_slots && (r1 - r0) >= 2 * Q.n_slots;
-        const int64_t S = Q.n_slots;
+        const bool sliced = Q.n_slices > 1;
+        const int64_t s_lo = six * Q.slice_slots;
+        const bool use_smem = sliced || (Q.n_slots <= B.smem_slots && (r1 - r0) >= 2 * Q.n_slots);
+        const int64_t S = sliced ? (Q.n_slots - s_lo < Q.slice_slots ? Q.n_slots - s_lo : Q.slice_slots) : Q.n_slots;
         if (use_smem) {
             for (int64_t s = threadIdx.x; s < S; s += blockDim.x) scnt[s] = 0;
             for (int a = 0; a < B.na; a++)
@@ -239,7 +251,17 @@ __global__ void __launch_bounds__(kBatchMaxThreads) k_batch_agg(const BatchK B) 
             }
 #pragma unroll
             for (int j = 0; j < kBR; j++)
-                if (ok[j] && (k[j] < 0 || k[j] >= S)) { atomicCAS(B.err, 0, E_DOMAIN); ok[j] = false; }
+                if (ok[j] && (k[j] < 0 || k[j] >= Q.n_slots)) {
+                    if (six == 0) atomicCAS(B.err, 0, E_DOMAIN);     // reported once, by the first slice
+                    ok[j] = false;
+                }
+            if (sliced) {
+#pragma unroll
+                for (int j = 0; j < kBR; j++) {
+                    k[j] -= s_lo;
+                    ok[j] = ok[j] && k[j] >= 0 && k[j] < S;        // another slice's row
+                }
+            }
             if (use_smem) {
 #pragma unroll
                 for (int j = 0; j < kBR; j++) if (ok[j]) atomicAdd(&scnt[k[j]], 1u);
@@ -288,7 +310,7 @@ __global__ void __launch_bounds__(kBatchMaxThreads) k_batch_agg(const BatchK B) 
             for (int64_t s = threadIdx.x; s < S; s += blockDim.x) {
                 const uint32_t c = scnt[s];
                 if (!c) continue;
-                unsigned long long* rec = B.rec + (Q.acc_off + s) * B.W;
+                unsigned long long* rec = B.rec + (Q.acc_off + s_lo + s) * B.W;
                 atomicAdd(rec, (unsigned long long)c);
                 for (int a = 0; a < B.na; a++)
                     if (B.ai[a] >= 0) bmerge(rec + 1 + B.ai[a], B.kind[a], sacc[B.ai[a] * S + s]);
@@ -388,14 +410,29 @@ __global__ void __launch_bounds__(kEmitBlock) k_batch_emit(const BatchK B, const
 
 using namespace tdg;
 
-// Per-query tile: a query whose slots fit in shared memory gets tiles of at
-// least kRowsPerSlot rows per slot (fewer flushes of its shared aggregates).
+// Key slices per tile: more than one when the query's slots exceed shared
+// memory but it has at least kRowsPerSlot rows per slot.
+static int64_t query_slices(const tdg_batch_query& q, const tdg_batch_plan* p) {
+    if (q.n_slots <= p->smem_slots || p->smem_slots < 1 || q.nrows < kRowsPerSlot * q.n_slots) return 1;
+    const int64_t n = (q.n_slots + p->smem_slots - 1) / p->smem_slots;
+    return n <= kMaxSlices ? n : 1;
+}
+
+// Per-query tile: a query aggregated in shared memory (whole or by key slice)
+// gets tiles of at least kRowsPerSlot rows per slot of its key range (fewer
+// flushes of its shared aggregates).
 static int64_t query_tile(const tdg_batch_query& q, const tdg_batch_plan* p) {
-    if (q.n_slots <= p->smem_slots) {
+    if (q.n_slots <= p->smem_slots || query_slices(q, p) > 1) {
         const int64_t t = q.n_slots * kRowsPerSlot;
         return t > p->tile_rows ? t : p->tile_rows;
     }
     return p->tile_rows;
+}
+
+// Work items of a query: its tiles times its key slices.
+static int64_t query_items(const tdg_batch_query& q, const tdg_batch_plan* p) {
+    const int64_t t = query_tile(q, p);
+    return (q.nrows + t - 1) / t * query_slices(q, p);
 }
 
 extern "C" tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_rows, int32_t ctas_per_sm,
@@ -444,8 +481,7 @@ extern "C" tdg_status tdg_batch_plan_make(const tdg_batch_desc* d, int64_t tile_
         // direct-indexed records only: a key range far wider than the query
         // (sparse keys) belongs to the hash-table group-by, not the batch
         if (q.n_slots > kMaxDenseSlots && q.n_slots > 4 * q.nrows) return E_NYI;
-        const int64_t t = query_tile(q, p);
-        p->n_items += (q.nrows + t - 1) / t;
+        p->n_items += query_items(q, p);
         p->total_slots += q.n_slots;
         pieces += (q.n_slots + kPiece - 1) / kPiece;
     }
@@ -472,9 +508,12 @@ extern "C" tdg_status tdg_batch_prepare(const tdg_batch_desc* d, const tdg_batch
         b.acc_off = acc;
         b.first_item = item;
         b.tile_rows = query_tile(q, p);
-        const int64_t tiles = (q.nrows + b.tile_rows - 1) / b.tile_rows;
-        for (int64_t t = 0; t < tiles; t++) item_q[(size_t)(item + t)] = i;
-        item += tiles;
+        b.n_slices = query_slices(q, p);
+        b.slice_slots = (q.n_slots + b.n_slices - 1) / b.n_slices;
+        const int64_t items = query_items(q, p);
+        if (item + items > p->n_items) return E_RANGE;
+        for (int64_t t = 0; t < items; t++) item_q[(size_t)(item + t)] = i;
+        item += items;
         acc += q.n_slots;
         for (int64_t s0 = 0; s0 < q.n_slots && piece < p->n_pieces; s0 += kPiece, piece++) {
             piece_q[(size_t)piece] = i;

@@ -120,3 +120,50 @@ def test_batch_equals_per_query_execute_narrow_types(gpu):
                 assert np.array_equal(got[name][sel], col), (i, name)
     for t in tables:
         gpu.release(t)
+
+
+@pytest.mark.parametrize("ctas", [1, 0])
+def test_batch_key_slices(gpu, tmp_path, monkeypatch, ctas):
+    """Queries whose key range exceeds shared memory but has at least 8 rows
+    per slot are aggregated by key slice (an item is a (tile, slice) pair):
+    with one CTA per SM (about 11K slots on chip) the 30000- and 15000-slot
+    queries take 3 and 2 slices; with the default 48 KB (about 2.4K slots) the
+    15000-slot one takes 7 and the 30000-slot one (13 would be needed) the
+    global records.  The launch shape is fixed through the tuner's file.
+    Every query equals the oracle's group-by."""
+    import json
+    import math
+    specs = [(30000, 300_000), (15000, 200_000), (5000, 60_000), (100, 50_000), (30000, 250_000),
+             (15000, 130_000), (2500, 40_000), (60, 10_000)]
+    r = np.random.default_rng(400 + ctas)
+    datas = []
+    for k, n in specs:
+        key = r.integers(0, k, n, dtype=np.int64)
+        key[0], key[1] = 0, k - 1                        # the key range is exactly [0, k)
+        datas.append({"key": key, "val": r.random(n) * 100.0})
+    nq = len(specs)
+    tkey = "batch:q%d:r%d:s%d:a%d" % (int(math.log2(nq)), int(math.log2(sum(n for _, n in specs) / nq)),
+                                      int(math.log2(sum(k for k, _ in specs) / nq)), 3)
+    cache = tmp_path / "tune.json"
+    # the tuner's file format: one JSON object, one entry per line
+    cache.write_text('{\n  "%s": {"tile_rows": 16384, "ctas_per_sm": %d}\n}\n' % (tkey, ctas))
+    assert json.loads(cache.read_text())[tkey]["ctas_per_sm"] == ctas
+    monkeypatch.setenv("TD_TUNE_CACHE", str(cache))
+    tables = [gpu.table(d) for d in datas]
+    L = _bind(gpu)
+    for t in tables:
+        assert L.td_gpu_pin(t) == 0
+    try:
+        got = run_batch(gpu, tables)
+        q = got["_query"]
+        for i, d in enumerate(datas):
+            sel = q == i
+            want = oracle.group({"key": d["key"]}, [(OP_SUM, "val", d["val"]), (OP_COUNT, "val", None),
+                                                    (OP_MAX, "val", d["val"])])
+            assert np.array_equal(got["key"][sel], want["key"]), i
+            assert np.array_equal(got["val_count"][sel], want["val_count"]), i
+            assert np.array_equal(got["val_max"][sel], want["val_max"]), i
+            assert f64_tolerance_ok(got["val_sum"][sel], want["val_sum"], np.abs(want["val_sum"])), i
+    finally:
+        for t in tables:
+            gpu.release(t)
