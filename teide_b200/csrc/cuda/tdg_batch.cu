@@ -11,13 +11,14 @@
 //   accumulate   a query with at most smem_slots slots (and a tile at least
 //                twice that long) aggregates its tile in shared memory and
 //                merges once; a query with more slots but at least
-//                kRowsPerSlot rows per slot is cut into key slices of at most
-//                smem_slots slots as well, and an item is then a (tile, slice)
-//                pair that aggregates only its slice's rows in shared memory
-//                (the slices of a tile are consecutive items, so the tile's
-//                columns are read from DRAM once and from L2 by the others);
-//                the remaining tiles update the query's slot records in
-//                global memory (L2-resident per query);
+//                kRowsPerSlot rows per slot is cut into at most
+//                kMaxSlices key slices of at most smem_slots slots, and an
+//                item is then a (tile, slice) pair that aggregates only its
+//                slice's rows in shared memory (the slices of a tile are
+//                consecutive items, so the tile's columns are read from DRAM
+//                once and from L2 by the others); the remaining tiles update
+//                the query's slot records in global memory (L2-resident per
+//                query);
 //   emit         one CTA per query writes its non-empty slots, keys ascending,
 //                at the query's offset from an exclusive scan of group counts.
 //
@@ -56,7 +57,8 @@ struct BatchK {
     unsigned long long* rec;
     unsigned long long* counter;
     int32_t* err;
-    const volatile int32_t* cancel;  // polled per work item (pool.c:485-489's per-task check)
+    const volatile int32_t* cancel;  // host-mapped cancel word (pool.c:485-489's per-task check)
+    int32_t* stop;                   // device copy of a seen cancel, read per work item
     const int32_t* piece_q;       // emit piece -> query
     const int64_t* piece_s0;      // emit piece -> first slot within the query
     int64_t* pcount;              // groups per piece, then exclusive offsets
@@ -100,6 +102,7 @@ static BatchK make_bk(const tdg_batch_plan* p, void* ws) {
     char* w = (char*)ws;
     B.counter = (unsigned long long*)(w + L.hdr);
     B.err = (int32_t*)(w + L.hdr + 16);
+    B.stop = (int32_t*)(w + L.hdr + 32);
     B.cancel = p->cancel;
     B.q = (const BQ*)(w + L.q);
     B.item_q = (const int32_t*)(w + L.item_q);
@@ -195,7 +198,13 @@ __global__ void __launch_bounds__(kBatchMaxThreads) k_batch_agg(const BatchK B) 
         __syncthreads();
         if (threadIdx.x == 0) {
             long long it = (long long)atomicAdd(B.counter, 1ULL);
-            if (B.cancel && *B.cancel) it = B.n_items;     // cancelled: take no further item
+            if (B.cancel) {
+                // the host word is read over the link by every 64th claim only
+                // (one read per claim measured 2x slower on a 4096-query
+                // batch); a cancel seen there stops every CTA at its next claim
+                if ((it & 63) == 0 && *B.cancel) atomicExch(B.stop, 1);
+                if (*(volatile int32_t*)B.stop) it = B.n_items;   // cancelled: take no further item
+            }
             s_item = it;
         }
         __syncthreads();
@@ -411,7 +420,8 @@ __global__ void __launch_bounds__(kEmitBlock) k_batch_emit(const BatchK B, const
 using namespace tdg;
 
 // Key slices per tile: more than one when the query's slots exceed shared
-// memory but it has at least kRowsPerSlot rows per slot.
+// memory but it has at least kRowsPerSlot rows per slot.  (Slicing from two
+// rows per slot measured no faster on the 4096-query batch.)
 static int64_t query_slices(const tdg_batch_query& q, const tdg_batch_plan* p) {
     if (q.n_slots <= p->smem_slots || p->smem_slots < 1 || q.nrows < kRowsPerSlot * q.n_slots) return 1;
     const int64_t n = (q.n_slots + p->smem_slots - 1) / p->smem_slots;
