@@ -587,6 +587,58 @@ def serve_summary(v):
             "how": "td_server over resident tables; plain = the same trace through one slot (one query at a time)"}
 
 
+def serve_small(td, L, n_queries=1024, slots=8, seed=6):
+    """The served form on a stream of small group-by requests: the first
+    `n_queries` of the batched workload's queries (one table each, rows
+    log-uniform in [1K, 2M], 16 to 65536 keys), submitted to td_server at
+    once (closed loop) against the same requests run one td_execute after
+    another; then offered at 0.8x the served rate (open loop) for the latency
+    percentiles.  The server packs same-shape requests that wait behind each
+    other into td_execute_batch launches."""
+    import numpy as np
+    from teide_b200 import serve
+    b = Batch(td, seed=seed, first=n_queries)
+    for t in b.tables:
+        st = L.td_gpu_pin(t)
+        if st:
+            raise RuntimeError(f"td_gpu_pin failed: {st}")
+
+    class Req:
+        __slots__ = ("graph", "root", "arrival", "kind")
+
+    reqs = []
+    for g, root in zip(b.graphs, b.roots):
+        q = Req()
+        q.graph, q.root, q.arrival, q.kind = g, root, 0.0, "group"
+        reqs.append(q)
+    b.plain()                                           # warm-up: uploads, statistics, plans
+    t0 = time.perf_counter()
+    b.plain()
+    plain_s = time.perf_counter() - t0
+    with serve.Server(td, slots=slots) as srv:
+        serve.run_closed(srv, reqs)                     # warm-up: tuning, batch plans
+        closed = min(serve.run_closed(srv, reqs) for _ in range(3))
+        rate = 0.8 * len(reqs) / closed
+        r = np.random.default_rng(seed)
+        arrivals = np.cumsum(r.exponential(1.0 / rate, len(reqs)))
+        for q, a in zip(reqs, arrivals):
+            q.arrival = float(a - arrivals[0])
+        lat, makespan, _ = serve.run_open_loop(srv, reqs)
+    for t in b.tables:
+        L.td_gpu_unpin(t)
+    out = {"requests": len(reqs), "slots": slots, "qps": len(reqs) / closed, "plain_qps": len(reqs) / plain_s,
+           "speedup": plain_s / closed,
+           "sustained": {"offered_qps": rate, "qps": len(reqs) / makespan if makespan else None,
+                         "p50_ms": float(np.percentile(lat, 50) * 1e3), "p99_ms": float(np.percentile(lat, 99) * 1e3)},
+           "how": "td_server packs queued same-shape group-by requests into td_execute_batch launches; "
+                  "plain = one td_execute per request in arrival order"}
+    for g in b.graphs:
+        g.free()
+    for t in b.tables:
+        td.release(t)
+    return out
+
+
 # ---- CPU reference ---------------------------------------------------------------------
 
 SERVE_REF_ROWS, SERVE_REF_REQUESTS = 60_000_000, 16
@@ -979,8 +1031,11 @@ def main():
         line["batch"] = batch_summary(batch_main(_sub(args, scale=args.batch_scale), td, L, rank, world, local,
                                                  barrier, max_over_ranks))
         L.td_gpu_trim()
+        small = serve_small(td, L)
+        L.td_gpu_trim()
         line["serve"] = serve_summary(serve_main(_sub(args, requests=args.serve_requests), td, L, rank, world,
                                                  local, barrier, max_over_ranks))
+        line["serve"]["small_requests"] = small
     if rank == 0:
         print(json.dumps(line))
     if dist:

@@ -229,6 +229,41 @@ static int lower_one(tdb_ctx* c, td_graph_t* g, td_op_t* root, uint16_t* ops, in
     return TD_OK;
 }
 
+/* The shape of a group graph that td_execute_batch takes, as a nonzero
+ * signature (0 when it takes no such graph): its aggregate list and its key
+ * and value columns' names and types -- the output schema of the batch, so
+ * graphs with equal signatures give the same columns batched or alone.
+ * Host-only, no device work: the server calls it when a request arrives. */
+uint64_t tdb_batch_signature(td_graph_t* g, td_op_t* root) {
+    if (!g || !root || root->opcode != OP_GROUP || !g->table) return 0;
+    td_op_ext_t* ext = tdb_find_ext(g, root->id);
+    if (!ext || ext->n_keys != 1 || ext->n_aggs < 1 || ext->n_aggs > TDG_MAX_AGGS) return 0;
+    td_op_ext_t* kx = tdb_find_ext(g, ext->keys[0]->id);
+    if (!kx || kx->base.opcode != OP_SCAN) return 0;
+    td_t* kcol = td_table_get_col(g->table, kx->sym);
+    if (!kcol || TD_IS_ERR(kcol) || kcol->type <= 0 || kcol->type == TD_F64 || kcol->type >= TD_TABLE) return 0;
+    td_t* vcol = NULL;
+    int64_t vname = -1;
+    for (int a = 0; a < ext->n_aggs; a++) {
+        const uint16_t op = ext->agg_ops[a];
+        if (op != OP_SUM && op != OP_COUNT && op != OP_MIN && op != OP_MAX && op != OP_AVG) return 0;
+        td_op_ext_t* ax = tdb_find_ext(g, ext->agg_ins[a]->id);
+        if (op == OP_COUNT && (!ax || ax->base.opcode != OP_SCAN)) continue;
+        if (!ax || ax->base.opcode != OP_SCAN) return 0;
+        td_t* v = td_table_get_col(g->table, ax->sym);
+        if (!v || TD_IS_ERR(v) || (vcol && v != vcol)) return 0;
+        vcol = v;
+        vname = ax->sym;
+    }
+    if (!vcol) vcol = kcol, vname = kx->sym;
+    if (vcol->type <= 0 || vcol->type >= TD_TABLE) return 0;
+    const int64_t f[6] = { kx->sym, vname, kcol->type | (int64_t)(kcol->attrs & TD_SYM_W_MASK) << 8,
+                           vcol->type | (int64_t)(vcol->attrs & TD_SYM_W_MASK) << 8, ext->n_aggs, 0 };
+    uint64_t h = sig64(1469598103934665603ULL, f, sizeof(f));
+    h = sig64(h, ext->agg_ops, sizeof(uint16_t) * (size_t)ext->n_aggs);
+    return h ? h : 1;
+}
+
 static int alloc_outputs(bchunk_t* ch, int64_t* d_rows) {
     size_t rows = (size_t)(ch->plan.total_slots > 0 ? ch->plan.total_slots : 1);
     ch->n_bufs = 0;
@@ -270,13 +305,13 @@ static float time_config(tdb_ctx* c, const tdg_batch_desc* d, int64_t tile, int3
     return best;
 }
 
-static void autotune(tdb_ctx* c, const tdg_batch_desc* d, int64_t* tile, int32_t* ctas) {
+static void autotune(tdb_ctx* c, const tdg_batch_desc* d, int64_t* tile, int32_t* ctas, int once) {
     char key[128];
     tune_key(d, key, sizeof(key));
     if (tdb_tune_load(key, tile, ctas)) return;
     *tile = 0;
     *ctas = 0;
-    if (getenv("TD_NO_AUTOTUNE")) return;
+    if (once || getenv("TD_NO_AUTOTUNE")) return;   /* a one-off batch takes the defaults */
     bchunk_t scratch;
     memset(&scratch, 0, sizeof(scratch));
     int64_t* d_rows = tdb_dev_alloc(c, 8);
@@ -308,7 +343,22 @@ static int64_t agg_out_name(uint16_t op, int64_t base) {
     return td_sym_intern(buf, (size_t)n + strlen(sfx));
 }
 
+/* once: a batch that will not repeat (td_server packing the requests that
+ * wait in its queue): one chunk, run directly rather than captured into a CUDA
+ * graph, outputs from the arena and the row count in a mapped scalar of the
+ * call, nothing kept in the cache, and the defaults when its shape was never
+ * tuned. */
+static td_t* exec_batch(td_graph_t** graphs, td_op_t** roots, int64_t n, int once);
+
 td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
+    return exec_batch(graphs, roots, n, 0);
+}
+
+td_t* tdb_execute_batch_once(td_graph_t** graphs, td_op_t** roots, int64_t n) {
+    return exec_batch(graphs, roots, n, 1);
+}
+
+static td_t* exec_batch(td_graph_t** graphs, td_op_t** roots, int64_t n, int once) {
     if (!graphs || !roots || n < 0 || n > INT32_MAX) return TD_ERR_PTR(TD_ERR_RANGE);
     tdb_cancel_reset();
     tdb_trace_begin();
@@ -317,6 +367,7 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
     if (st) return TD_ERR_PTR(st);
     pthread_mutex_lock(&bcache_mu);
     td_t* res = NULL;
+    bchunk_t* once_ch = NULL;         /* the one-off chunk's arena buffers, freed at the end */
     bq_host_t* hq = calloc((size_t)(n ? n : 1), sizeof(bq_host_t));
     tdg_batch_query* qs = calloc((size_t)(n ? n : 1), sizeof(tdg_batch_query));
     uint16_t ops[TDG_MAX_AGGS];
@@ -344,15 +395,45 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
      * compute.  Timing (tdg_set_timing) runs one chunk so its kernel time
      * covers the whole batch. */
     const int timing = tdg_timing_enabled();
-    int K = timing ? 1 : (int)(n / 64 < BATCH_CHUNKS ? n / 64 : BATCH_CHUNKS);
+    int K = timing || once ? 1 : (int)(n / 64 < BATCH_CHUNKS ? n / 64 : BATCH_CHUNKS);
     if (K < 1) K = 1;
+    bcache_t once_e;
+    static _Thread_local cudaEvent_t once_done;
     uint64_t sig = sig64(1469598103934665603ULL, qs, sizeof(tdg_batch_query) * (size_t)n);
     sig = sig64(sig, &d.agg_ops, sizeof(d.agg_ops));
     sig = sig64(sig, &K, sizeof(K));
     bcache_t* e = NULL;
-    for (int i = 0; i < BATCH_CACHE; i++)
+    for (int i = 0; i < BATCH_CACHE && !once; i++)
         if (bcache[i].n_chunks && bcache[i].sig == sig && bcache[i].n == n) e = &bcache[i];
-    if (!e) {
+    if (once) {
+        memset(&once_e, 0, sizeof(once_e));
+        e = &once_e;
+        int64_t tile;
+        int32_t ctas;
+        autotune(&c, &d, &tile, &ctas, 1);
+        void* d_rows = NULL;
+        e->h_rows = (int64_t*)tdb_host_scalar(&c, &d_rows);
+        e->d_rows = d_rows;
+        if (!once_done && cudaEventCreateWithFlags(&once_done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            once_done = NULL;
+        }
+        e->done[0] = once_done;
+        bchunk_t* ch = &e->ch[0];
+        once_ch = ch;
+        e->n_chunks = 1;
+        ch->nq = (int32_t)n;
+        if (!e->h_rows || !once_done) st = TD_ERR_OOM;
+        if (!st) st = tdg_batch_plan_make(&d, tile, ctas, &ch->plan);
+        if (!st) {
+            ch->plan.cancel = tdb_cancel_word();
+            ch->ws = tdb_dev_alloc_persistent(ch->plan.ws_bytes);
+            if (!ch->ws || alloc_outputs(ch, (int64_t*)e->d_rows)) st = TD_ERR_OOM;
+        }
+        if (!st) st = tdg_batch_prepare(&d, &ch->plan, ch->ws, c.stream);
+        e->total_slots = ch->plan.total_slots;
+        if (st) goto done;
+    } else if (!e) {
         /* chunk boundaries: contiguous query ranges of about equal rows */
         int32_t q0s[BATCH_CHUNKS + 1];
         double total = 0, acc = 0;
@@ -370,7 +451,7 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
         d0.queries = qs;
         int64_t tile;
         int32_t ctas;
-        autotune(&c, &d0, &tile, &ctas);
+        autotune(&c, &d0, &tile, &ctas, 0);
         int victim = 0;
         for (int i = 1; i < BATCH_CACHE; i++) if (bcache[i].used < bcache[victim].used) victim = i;
         e = &bcache[victim];
@@ -419,7 +500,7 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
         }
         if (st) { bcache_drop(e); goto done; }
     }
-    e->used = ++bstamp;
+    if (!once) e->used = ++bstamp;
     tdb_trace("batch lowered");
     if ((st = tdb_check_cancel())) goto done;
     tdb_note_kernel();
@@ -519,6 +600,11 @@ td_t* td_execute_batch(td_graph_t** graphs, td_op_t** roots, int64_t n) {
     for (int j = 0; j < nc; j++) if (cols[j].v) td_release(cols[j].v);
     tdb_trace("batch assembled");
 done:
+    if (once_ch) {
+        cudaStreamSynchronize((cudaStream_t)c.stream);   /* nothing of the batch still running */
+        cudaGetLastError();
+        chunk_drop(once_ch);
+    }
     pthread_mutex_unlock(&bcache_mu);
     if (st && res) { td_release(res); res = NULL; }
     free(hq);

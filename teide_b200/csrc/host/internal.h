@@ -145,6 +145,12 @@ float tdb_time_call(tdb_ctx* c, int (*run)(void*), void* arg, int* st);
  * build tables reuse one payload map per build side (td_server's workers set
  * it).  tdb_build_cache_clear frees every kept map. */
 void  tdb_share_builds(int on);
+/* Nonzero shape signature of a group graph td_execute_batch takes (aggregate
+ * list, key and value column names and types), 0 otherwise; host-only. */
+uint64_t tdb_batch_signature(td_graph_t* g, td_op_t* root);
+/* td_execute_batch for a batch that will not repeat (no cached plan or CUDA
+ * graph, no tuning run): td_server's packed requests. */
+td_t* tdb_execute_batch_once(td_graph_t** graphs, td_op_t** roots, int64_t n);
 void  tdb_build_cache_clear(void);
 
 #endif

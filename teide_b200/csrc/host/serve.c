@@ -14,6 +14,16 @@
  * whose estimate alone exceeds the budget runs when nothing else is in
  * flight.
  *
+ * Small group-by requests of one shape -- one integer key, aggregates over one
+ * value column, the same aggregate list and column names -- that wait in the
+ * queue behind each other run together: a worker takes the head and every
+ * queued request of its shape right behind it (up to SERVE_BATCH_MAX, within
+ * the budget) into one td_execute_batch launch and splits the packed result
+ * into one table per request, the columns td_execute returns.  Requests of
+ * different sizes share the launch; the batch kernel balances their tiles.
+ * One packed batch runs at a time: the batch-shaped requests that arrive
+ * meanwhile wait at the head and leave together as the next batch.
+ *
  * Join queries over the same resident build table share one payload map (the
  * build side's key -> group-slot map): the first query builds it into a kept
  * workspace and every later one only probes it (host/exec.c, shared join
@@ -34,6 +44,7 @@ typedef struct {
     int64_t             ticket;
     td_graph_t*         g;
     td_op_t*            root;
+    uint64_t            sig;        /* td_execute_batch shape, 0 if none */
     size_t              est;
     int                 state;      /* 0 free, 1 queued, 2 running, 3 done */
     td_t*               result;
@@ -53,6 +64,7 @@ struct td_server {
     int             stop;
     size_t          budget, reserved, peak_reserved;
     int32_t         in_flight, peak_in_flight;
+    int32_t         batch_running;  /* a packed batch is in flight */
     uint64_t        completed;
 };
 
@@ -62,51 +74,129 @@ static int64_t now_ns(void) {
     return (int64_t)ts.tv_sec * 1000000000LL + ts.tv_nsec;
 }
 
+/* Requests a worker takes together at most, and the split of a batch's
+ * packed result (rows of query i, keys ascending, _query column first) into
+ * one table per request, with the columns td_execute would return. */
+#define SERVE_BATCH_MAX 1024
+
+static td_t* rows_of(td_t* b, int64_t r0, int64_t r1) {
+    const int64_t nc = td_table_ncols(b);
+    td_t* t = td_table_new(nc - 1);
+    if (!t || TD_IS_ERR(t)) return TD_ERR_PTR(TD_ERR_OOM);
+    for (int64_t j = 1; j < nc; j++) {
+        td_t* c = td_table_get_col_idx(b, j);
+        const size_t es = td_sym_elem_size(c->type, c->attrs);
+        td_t* v = td_vec_new(c->type, r1 - r0 > 0 ? r1 - r0 : 1);
+        if (!v || TD_IS_ERR(v)) { td_release(t); return TD_ERR_PTR(TD_ERR_OOM); }
+        if (c->type == TD_SYM) v->attrs = c->attrs;
+        if (r1 > r0) memcpy(td_data(v), (const char*)td_data(c) + (size_t)r0 * es, (size_t)(r1 - r0) * es);
+        v->len = r1 - r0;
+        td_t* t2 = td_table_add_col(t, td_table_col_name(b, j), v);
+        td_release(v);
+        if (TD_IS_ERR(t2)) { td_release(t); return t2; }
+        t = t2;
+    }
+    return t;
+}
+
+static void run_batch(td_graph_t** gs, td_op_t** rs, int64_t n, td_t** out) {
+    if (n == 1) { out[0] = td_execute(gs[0], rs[0]); return; }
+    td_t* b = tdb_execute_batch_once(gs, rs, n);
+    if (TD_IS_ERR(b)) {
+        /* a cancel ends them all; any other refusal runs them one by one */
+        for (int64_t i = 0; i < n; i++) out[i] = TD_ERR_CODE(b) == TD_ERR_CANCEL ? b : td_execute(gs[i], rs[i]);
+        return;
+    }
+    const int64_t rows = td_table_ncols(b) > 0 ? td_table_get_col_idx(b, 0)->len : 0;
+    const int64_t* q = rows ? (const int64_t*)td_data(td_table_get_col_idx(b, 0)) : NULL;
+    int64_t r = 0;
+    for (int64_t i = 0; i < n; i++) {
+        int64_t r1 = r;
+        while (r1 < rows && q[r1] == i) r1++;
+        out[i] = rows_of(b, r, r1);
+        r = r1;
+    }
+    td_release(b);
+}
+
 static void* worker_main(void* arg) {
     td_server_t* s = arg;
     tdb_share_builds(1);                /* join queries over one build table share its map */
+    int64_t* tix = malloc(SERVE_BATCH_MAX * sizeof(int64_t));
+    td_graph_t** gs = malloc(SERVE_BATCH_MAX * sizeof(td_graph_t*));
+    td_op_t** rs = malloc(SERVE_BATCH_MAX * sizeof(td_op_t*));
+    td_t** res = malloc(SERVE_BATCH_MAX * sizeof(td_t*));
     pthread_mutex_lock(&s->mu);
     for (;;) {
         req_t* r = NULL;
         if (s->next_admit < s->next_ticket) {
             req_t* head = &s->ring[s->next_admit % s->cap];
             const int fits = s->reserved + head->est <= s->budget || s->in_flight == 0;
-            if (s->in_flight < s->slots && fits) r = head;
+            /* one packed batch at a time (it fills the GPU): requests of a
+             * batch shape queue behind it and leave together as the next one */
+            const int wait_batch = head->sig && s->batch_running;
+            if (s->in_flight < s->slots && fits && !wait_batch) r = head;
         }
         if (!r) {
             if (s->stop && s->next_admit >= s->next_ticket) break;
             pthread_cond_wait(&s->cv_work, &s->mu);
             continue;
         }
-        s->next_admit++;
+        /* the head, and behind it every queued request of the same batch shape
+         * that fits the budget: they run as one td_execute_batch launch */
+        const uint64_t sig = (tix && gs && rs && res) ? r->sig : 0;
+        const int64_t now = now_ns();
+        int64_t nb = 0;
+        size_t est = 0;
+        for (;;) {
+            req_t* q = &s->ring[s->next_admit % s->cap];
+            if (tix) tix[nb] = q->ticket;
+            if (gs) gs[nb] = q->g;
+            if (rs) rs[nb] = q->root;
+            nb++;
+            est += q->est;
+            q->state = 2;
+            q->t.start_ns = now;
+            q->t.in_flight_at_start = s->in_flight + 1;
+            s->next_admit++;
+            if (!sig || nb >= SERVE_BATCH_MAX || s->next_admit >= s->next_ticket) break;
+            const req_t* nx = &s->ring[s->next_admit % s->cap];
+            if (nx->sig != sig || s->reserved + est + nx->est > s->budget) break;
+        }
         s->in_flight++;
-        s->reserved += r->est;
+        s->reserved += est;
+        if (sig) s->batch_running = 1;
         if (s->in_flight > s->peak_in_flight) s->peak_in_flight = s->in_flight;
         if (s->reserved > s->peak_reserved) s->peak_reserved = s->reserved;
-        r->state = 2;
-        r->t.start_ns = now_ns();
-        r->t.in_flight_at_start = s->in_flight;
-        td_graph_t* g = r->g;
-        td_op_t* root = r->root;
-        const size_t est = r->est;
-        const int64_t ticket = r->ticket;
+        const int64_t ticket0 = r->ticket;
+        td_graph_t* g0 = r->g;
+        td_op_t* root0 = r->root;
         pthread_mutex_unlock(&s->mu);
 
-        td_t* res = td_execute(g, root);
+        if (sig) run_batch(gs, rs, nb, res);
+        td_t* one = sig ? NULL : td_execute(g0, root0);
 
         pthread_mutex_lock(&s->mu);
-        r = &s->ring[ticket % s->cap];
-        r->result = res;
-        r->t.end_ns = now_ns();
-        r->t.status = TD_IS_ERR(res) ? (int32_t)TD_ERR_CODE(res) : 0;
-        r->state = 3;
+        const int64_t end = now_ns();
+        for (int64_t i = 0; i < nb; i++) {
+            req_t* d = &s->ring[(sig ? tix[i] : ticket0) % s->cap];
+            d->result = sig ? res[i] : one;
+            d->t.end_ns = end;
+            d->t.status = TD_IS_ERR(d->result) ? (int32_t)TD_ERR_CODE(d->result) : 0;
+            d->state = 3;
+        }
         s->in_flight--;
         s->reserved -= est;
-        s->completed++;
+        if (sig) s->batch_running = 0;
+        s->completed += (uint64_t)nb;
         pthread_cond_broadcast(&s->cv_done);
         pthread_cond_broadcast(&s->cv_work);
     }
     pthread_mutex_unlock(&s->mu);
+    free(tix);
+    free(gs);
+    free(rs);
+    free(res);
     return NULL;
 }
 
@@ -149,6 +239,7 @@ int64_t td_server_submit(td_server_t* s, td_graph_t* g, td_op_t* root, size_t es
     r->ticket = t;
     r->g = g;
     r->root = root;
+    r->sig = tdb_batch_signature(g, root);
     r->est = est_bytes;
     r->state = 1;
     r->t.submit_ns = now_ns();

@@ -178,3 +178,65 @@ def test_budget_serializes_and_stays_correct(tables):
                     assert s.stats().peak_in_flight == 1
     finally:
         serve.release(td, reqs)
+
+
+def test_small_group_requests_are_batched(gpu):
+    """Small group-by requests of one shape (one integer key, SUM/COUNT/MAX
+    of one value column, over tables of different sizes) queued behind each
+    other run as td_execute_batch launches: several requests share one start
+    time, and every request's table has the columns and rows td_execute
+    gives alone (keys, counts and MAX exactly, SUM within the 1e-12 rule).
+    A request of another shape in the middle ends the batch before it and
+    runs alone."""
+    from teide_b200.td import OP_COUNT as CNT, OP_MAX as MX, OP_SUM as SM
+    r = np.random.default_rng(71)
+    datas = []
+    for i in range(96):
+        n = int(r.integers(1_000, 300_000))
+        k = int(r.integers(4, 40_000))
+        key = r.integers(0, k, n, dtype=np.int64)
+        datas.append({"key": key, "val": r.random(n) * 50.0})
+    tabs = [gpu.table(d) for d in datas]
+    gpu.lib.td_gpu_pin.argtypes = [serve.P]
+    gpu.lib.td_gpu_unpin.argtypes = [serve.P]
+    for t in tabs:
+        assert gpu.lib.td_gpu_pin(t) == 0
+    graphs, roots = [], []
+    for i, t in enumerate(tabs):
+        g = gpu.graph(t)
+        if i == 40:                                   # another shape: MIN as well, two value columns
+            roots.append(g.group([g.scan("key")], [SM, MX], [g.scan("val"), g.scan("key")]))
+        else:
+            roots.append(g.group([g.scan("key")], [SM, CNT, MX], [g.scan("val")] * 3))
+        graphs.append(g)
+    try:
+        alone = []
+        for g, root in zip(graphs, roots):
+            res = g.execute(root)
+            alone.append(gpu.table_dict(res))
+            gpu.release(res)
+        with serve.Server(gpu, slots=1) as srv:
+            # the first request occupies the single slot; the rest queue behind it
+            tickets = [srv.submit(g, root) for g, root in zip(graphs, roots)]
+            got, starts = [], []
+            for t in tickets:
+                res, tm = srv.wait(t)
+                assert tm.status == 0
+                got.append(gpu.table_dict(res))
+                starts.append(tm.start_ns)
+                gpu.release(res)
+        assert len(set(starts)) < len(starts) // 4, "requests were not batched"
+        for i, (a, b) in enumerate(zip(alone, got)):
+            assert list(a) == list(b), i
+            for name in a:
+                if a[name].dtype.kind == "f" and name.endswith("_sum"):
+                    absum = oracle.group({"key": datas[i]["key"]}, [(SM, "val", np.abs(datas[i]["val"]))])["val_sum"]
+                    assert f64_tolerance_ok(b[name], a[name], absum), (i, name)
+                else:
+                    assert np.array_equal(a[name], b[name]), (i, name)
+    finally:
+        for g in graphs:
+            g.free()
+        for t in tabs:
+            gpu.lib.td_gpu_unpin(t)
+            gpu.release(t)
