@@ -525,8 +525,14 @@ td_t*   td_table_schema(td_t* tbl);
  * directory of column files and a ".d" file of column-name symbol ids. */
 td_err_t td_col_save(td_t* vec, const char* path);
 td_t*    td_col_load(const char* path);
+/* Zero-copy: the vector's data is the file's own pages, mapped copy-on-write
+ * (mmod = 1); td_release unmaps it. */
+td_t*    td_col_mmap(const char* path);
 td_err_t td_splay_save(td_t* tbl, const char* dir, const char* sym_path);
 td_t*    td_splay_load(const char* dir);
+/* td_splay_load with every column mapped by td_col_mmap; sym_path (or NULL)
+ * is a symbol file loaded first. */
+td_t*    td_read_splayed(const char* dir, const char* sym_path);
 /* The symbol table file ("TSYM", count, then length-prefixed strings). */
 td_err_t td_sym_save(const char* path);
 td_err_t td_sym_load(const char* path);

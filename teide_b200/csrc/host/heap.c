@@ -215,7 +215,9 @@ static void release_block(td_t* v) {
     p->magic = 0;
     atomic_fetch_add(&st_free, 1);
     atomic_fetch_sub(&st_bytes, block);
-    if (p->kind == TDB_BLK_MMAP) {
+    if (p->kind == TDB_BLK_FILE) {
+        munmap(p->raw, p->raw_size);          /* the prefix page and the file mapping */
+    } else if (p->kind == TDB_BLK_MMAP) {
         void* raw = p->raw;
         size_t raw_size = p->raw_size, pinned = atomic_load(&p->pinned);
         atomic_fetch_sub(&st_direct, 1);
@@ -227,6 +229,25 @@ static void release_block(td_t* v) {
     } else {
         free(p->raw);
     }
+}
+
+td_t* tdb_file_block(void* base, size_t total) {
+    tdb_block_prefix* p = (tdb_block_prefix*)((char*)base + 4096 - sizeof(tdb_block_prefix));
+    memset(p, 0, sizeof(*p));
+    p->magic = TDB_BLK_MAGIC;
+    p->kind = TDB_BLK_FILE;
+    p->raw = base;
+    p->raw_size = total;
+    p->serial = atomic_fetch_add(&st_serial, 1) + 1;
+    td_t* v = (td_t*)(p + 1);
+    /* the block's capacity: the largest power of two the mapping holds, so
+     * code that writes within a block's capacity stays inside it */
+    uint8_t order = 5;
+    while (((size_t)2 << order) <= total - 4096) order++;
+    v->order = order;
+    atomic_fetch_add(&st_alloc, 1);
+    atomic_fetch_add(&st_bytes, (size_t)1 << order);
+    return v;
 }
 
 void td_free(td_t* v) {

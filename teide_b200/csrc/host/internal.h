@@ -17,7 +17,7 @@
  * copies of large columns run at PCIe/C2C link speed. */
 typedef struct tdb_block_prefix {
     uint32_t magic;
-    uint32_t kind;          /* TDB_BLK_MALLOC or TDB_BLK_MMAP */
+    uint32_t kind;          /* TDB_BLK_MALLOC, TDB_BLK_MMAP or TDB_BLK_FILE */
     void*    raw;           /* start of the OS allocation */
     size_t   raw_size;      /* bytes of the OS allocation */
     _Atomic(size_t) pinned; /* bytes page-locked with cudaHostRegister */
@@ -33,6 +33,12 @@ _Static_assert(sizeof(tdb_block_prefix) == 64, "block prefix must be 64 bytes");
 #define TDB_BLK_MAGIC 0x7D6B1C0Au
 #define TDB_BLK_MALLOC 1u
 #define TDB_BLK_MMAP   2u
+#define TDB_BLK_FILE   3u       /* a column file mapped copy-on-write (td_col_mmap) */
+
+/* The mapping at `base` (page aligned, `total` bytes) holds a column file at
+ * base + 4096; its prefix goes at the end of the first (anonymous) page.
+ * Returns the file's header as a heap block; td_free unmaps the whole range. */
+td_t* tdb_file_block(void* base, size_t total);
 
 static inline tdb_block_prefix* tdb_prefix(td_t* v) {
     return (tdb_block_prefix*)((char*)v - sizeof(tdb_block_prefix));

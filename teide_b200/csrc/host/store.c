@@ -28,6 +28,7 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/mman.h>
 #include <sys/stat.h>
 #include <unistd.h>
 
@@ -156,6 +157,42 @@ td_t* td_col_load(const char* path) {
     return v;
 }
 
+/* Zero-copy column load (col.c:555-632's td_col_mmap): the file is mapped
+ * copy-on-write one page into a reserved range whose first page holds the
+ * heap prefix, so the vector is an ordinary heap block whose data are the
+ * file's own pages; writing the header (mmod, rc, order) copies only its
+ * page.  The file must be exactly the header plus its elements, as
+ * td_col_save writes it. */
+td_t* td_col_mmap(const char* path) {
+    if (!path) return TD_ERR_PTR(TD_ERR_IO);
+    int fd = open(path, O_RDONLY);
+    if (fd < 0) return TD_ERR_PTR(TD_ERR_IO);
+    struct stat sb;
+    td_t h;
+    if (fstat(fd, &sb) != 0 || sb.st_size < 32 || read_at(fd, &h, 32, 0)) { close(fd); return TD_ERR_PTR(TD_ERR_CORRUPT); }
+    if (!serializable(h.type)) { close(fd); return TD_ERR_PTR(TD_ERR_NYI); }
+    if (h.len < 0) { close(fd); return TD_ERR_PTR(TD_ERR_CORRUPT); }
+    if ((h.attrs & TD_ATTR_HAS_NULLS) && (h.attrs & TD_ATTR_NULLMAP_EXT)) { close(fd); return TD_ERR_PTR(TD_ERR_NYI); }
+    const size_t esz = td_sym_elem_size(h.type, h.attrs);
+    if (esz && (uint64_t)h.len > (SIZE_MAX - 32 - 8192) / esz) { close(fd); return TD_ERR_PTR(TD_ERR_IO); }
+    const size_t bytes = 32 + (size_t)h.len * esz;
+    if ((uint64_t)sb.st_size != (uint64_t)bytes) { close(fd); return TD_ERR_PTR(TD_ERR_CORRUPT); }
+    const size_t total = 4096 + ((bytes + 4095) & ~(size_t)4095);
+    char* base = mmap(NULL, total, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+    if (base == MAP_FAILED) { close(fd); return TD_ERR_PTR(TD_ERR_OOM); }
+    if (mmap(base + 4096, bytes, PROT_READ | PROT_WRITE, MAP_PRIVATE | MAP_FIXED, fd, 0) == MAP_FAILED) {
+        munmap(base, total);
+        close(fd);
+        return TD_ERR_PTR(TD_ERR_IO);
+    }
+    close(fd);
+    td_t* v = tdb_file_block(base, total);
+    v->mmod = 1;
+    v->attrs &= (uint8_t)~(TD_ATTR_SLICE | TD_ATTR_NULLMAP_EXT);
+    atomic_store_explicit(&v->rc, 1, memory_order_relaxed);
+    return v;
+}
+
 /* A column name usable as a file name (splay.c:79-85). */
 static int plain_name(const char* s, size_t n) {
     return n && s[0] != '.' && !memchr(s, '/', n) && !memchr(s, '\\', n) && !memchr(s, '\0', n);
@@ -236,7 +273,21 @@ td_err_t td_splay_save(td_t* tbl, const char* dir, const char* sym_path) {
     return TD_OK;
 }
 
-td_t* td_splay_load(const char* dir) {
+static td_t* splay_read(const char* dir, td_t* (*load)(const char*));
+
+td_t* td_splay_load(const char* dir) { return splay_read(dir, td_col_load); }
+
+/* splay.c's td_read_splayed: the columns mapped rather than read. */
+td_t* td_read_splayed(const char* dir, const char* sym_path) {
+    if (!dir) return TD_ERR_PTR(TD_ERR_IO);
+    if (sym_path) {
+        const td_err_t e = td_sym_load(sym_path);
+        if (e != TD_OK) return TD_ERR_PTR(e);
+    }
+    return splay_read(dir, td_col_mmap);
+}
+
+static td_t* splay_read(const char* dir, td_t* (*load)(const char*)) {
     if (!dir) return TD_ERR_PTR(TD_ERR_IO);
     char path[1024];
     if (snprintf(path, sizeof(path), "%s/.d", dir) >= (int)sizeof(path)) return TD_ERR_PTR(TD_ERR_RANGE);
@@ -257,7 +308,7 @@ td_t* td_splay_load(const char* dir) {
             tbl = TD_ERR_PTR(TD_ERR_RANGE);
             break;
         }
-        td_t* col = td_col_load(path);
+        td_t* col = load(path);
         if (!col || TD_IS_ERR(col)) {
             td_release(tbl);
             tbl = col ? col : TD_ERR_PTR(TD_ERR_IO);

@@ -91,6 +91,7 @@ class Td:
             "td_splay_save": (C.c_int, [P, C.c_char_p, C.c_char_p]), "td_splay_load": (P, [C.c_char_p]),
             "td_sym_save": (C.c_int, [C.c_char_p]), "td_sym_load": (C.c_int, [C.c_char_p]),
             "td_part_load": (P, [C.c_char_p, C.c_char_p]),
+            "td_col_mmap": (P, [C.c_char_p]), "td_read_splayed": (P, [C.c_char_p, C.c_char_p]),
         }
         for name in ("td_eq", "td_ne", "td_lt", "td_le", "td_gt", "td_ge", "td_and", "td_or",
                      "td_add", "td_sub", "td_mul", "td_div", "td_mod", "td_min2", "td_max2"):

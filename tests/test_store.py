@@ -250,3 +250,50 @@ def test_reference_parted_group_matches_oracle(ref, tmp_path, q):
             assert np.allclose(got[k], want[k], rtol=1e-12, atol=1e-12), k
         else:
             assert np.array_equal(got[k].astype(want[k].dtype), want[k]), k
+
+
+@pytest.mark.parametrize("name", ["i64", "f64", "i32", "u8", "empty"])
+def test_col_mmap_matches_file_and_reference(td, ref, tmp_path, name):
+    """td_col_mmap maps a column file copy-on-write: the same elements as
+    td_col_load and as Teide's own td_col_mmap of the same file, mmod = 1,
+    and writing an element changes the mapped vector but not the file."""
+    arr, typ = COLS[name]
+    path = str(tmp_path / "c.col")
+    a = _vec(td, arr, typ)
+    try:
+        assert td.lib.td_col_save(a, path.encode()) == 0
+        before = open(path, "rb").read()
+        v = td.check(td.lib.td_col_mmap(path.encode()), "td_col_mmap")
+        w = ref.check(ref.lib.td_col_mmap(path.encode()), "td_col_mmap (Teide)")
+        got, theirs = td.to_numpy(v), ref.to_numpy(w)
+        assert np.array_equal(got, theirs) and np.array_equal(got.astype(arr.dtype), arr)
+        if len(arr):
+            view = td.vec_view(v)                   # the mapped pages themselves
+            view[0] = view[0] + 1
+            assert td.to_numpy(v)[0] == got[0] + 1
+        td.release(v)
+        ref.release(w)
+        assert open(path, "rb").read() == before
+    finally:
+        td.release(a)
+
+
+def test_read_splayed_maps_every_column(td, tmp_path):
+    """td_read_splayed gives the table td_splay_load gives, with every column
+    mapped from its file; the symbol file is loaded first when named."""
+    d = {"k": np.arange(5000, dtype=np.int64) % 37, "v": np.linspace(-1, 1, 5000), "n": np.arange(5000, dtype=np.int32)}
+    t = td.table({"k": d["k"], "v": d["v"], "n": td.vec(d["n"], I32)})
+    dirp, symp = str(tmp_path / "tbl"), str(tmp_path / "sym")
+    try:
+        assert td.lib.td_splay_save(t, dirp.encode(), symp.encode()) == 0
+        r = td.check(td.lib.td_read_splayed(dirp.encode(), symp.encode()), "td_read_splayed")
+        s = td.check(td.lib.td_splay_load(dirp.encode()), "td_splay_load")
+        got, want = td.table_dict(r), td.table_dict(s)
+        td.release(r)
+        td.release(s)
+        assert list(got) == list(want) == ["k", "v", "n"]
+        for k in got:
+            assert np.array_equal(got[k], want[k]), k
+        assert np.array_equal(got["k"], d["k"]) and np.array_equal(got["n"], d["n"])
+    finally:
+        td.release(t)

@@ -128,3 +128,34 @@ def test_parted_group_by(gpu, tmp_path, pinned):
     if pinned:
         L.td_gpu_unpin(t)
         gpu.release(t)
+
+
+def test_mapped_splayed_table_queries(gpu, tmp_path):
+    """A splayed table opened with td_read_splayed (every column mapped from
+    its file, copy-on-write) uploads from the mapped pages and groups like
+    the oracle; pinned, the next query uploads nothing."""
+    L = gpu.lib
+    L.td_gpu_pin.argtypes = [C.c_void_p]
+    L.td_gpu_unpin.argtypes = [C.c_void_p]
+    d = workloads.readme_table(n=3_000_001, seed=63)
+    t = gpu.table(d)
+    dirp = str(tmp_path / "mapped")
+    assert L.td_splay_save(t, dirp.encode(), None) == 0
+    gpu.release(t)
+    r = gpu.check(L.td_read_splayed(dirp.encode(), None), "td_read_splayed")
+    try:
+        m = d["flag"] == 0
+        want = oracle.group({"region": d["region"][m]}, [(OP_SUM, "amount", d["amount"][m])])
+        absum = oracle.group({"region": d["region"][m]}, [(OP_SUM, "amount", np.abs(d["amount"][m]))])
+        got = readme_group(gpu, r, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+        assert np.array_equal(got["region"], want["region"])
+        assert f64_tolerance_ok(got["amount_sum"], want["amount_sum"], absum["amount_sum"])
+        assert L.td_gpu_pin(r) == 0
+        got = readme_group(gpu, r, ("flag", "eq", 0), ["region"], [(OP_SUM, "amount")])
+        s = St()
+        L.td_gpu_last_stats(C.byref(s))
+        assert s.h2d == 0
+        assert np.array_equal(got["region"], want["region"])
+    finally:
+        L.td_gpu_unpin(r)
+        gpu.release(r)
