@@ -197,10 +197,9 @@ tdg_status tdg_group_run(const tdg_group_desc* d, const tdg_expr* pred, const ui
  * loads the library holds until the process exits.  `out` must hold
  * plan.max_groups rows, where tdg_group_plan_make(d, 0, &plan) gives the plan
  * (and its ws_bytes); a group-by that needs more scratch than the array holds
- * is refused with TD_ERR_RANGE.  The first call on a device looks up the
- * array's device address; make it before any stream capture.  Each call
- * waits for its stream before it returns (it reads the group count back to
- * size the emit).  Every call
+ * is refused with TD_ERR_RANGE.  Each call waits for its stream before it
+ * returns (it reads the group count and the error word back), so no call may
+ * be made while its stream is being captured into a CUDA graph.  Every call
  * shares the array, and each call re-initializes what it reads, but calls
  * that overlap on the GPU race: serialize them. */
 #define TDG_STATIC_SCRATCH_BYTES (16u << 20)

@@ -19,10 +19,10 @@
 //     but calls that overlap on the GPU -- on two streams or from two host
 //     threads -- race on it and must be serialized by the caller;
 //   - the first call on a device looks up the array's device address with
-//     cudaGetSymbolAddress (a host-side symbol is not a device address); make
-//     that first call before any stream capture;
-//   - each call waits for its stream before it returns (the group count is
-//     read back to size the emit).
+//     cudaGetSymbolAddress (a host-side symbol is not a device address);
+//   - each call waits for its stream before it returns (the group count and
+//     the error word are read back), so no call may be made while its stream
+//     is being captured into a CUDA graph.
 #include "tdg_hash.cuh"
 #include <mutex>
 
