@@ -83,7 +83,9 @@ void     td_gpu_batch_cache_clear(void);
  * while others run starts as soon as a slot frees up and its estimated device
  * bytes fit in the budget (hbm_budget, or 0 for 90% of the GPU's free memory
  * when the server starts).  The queue head is never bypassed; a request that
- * alone exceeds the budget runs when nothing else is in flight.
+ * alone exceeds the budget runs when nothing else is in flight.  Requests of
+ * one td_execute_batch shape (below) that wait behind each other run as one
+ * batched launch, one at a time, each still getting its own result table.
  *
  * Each submitted graph must stay alive, and must not be executed elsewhere,
  * until td_server_wait has returned its result.  est_bytes = 0 asks
@@ -118,6 +120,14 @@ typedef struct {
 td_server_t* td_server_new(int32_t slots, size_t hbm_budget, int64_t queue_cap);
 int64_t      td_server_submit(td_server_t* s, td_graph_t* g, td_op_t* root, size_t est_bytes);
 td_t*        td_server_wait(td_server_t* s, int64_t ticket, td_server_timing_t* timing);
+/* n requests in one call (tickets[i] as td_server_submit returns them; the
+ * call stops at the first refusal and returns how many were submitted), and
+ * their results in one call (results[i], timings[i] may be NULL), in ticket
+ * order: a client with many small queries pays one call, not n. */
+int64_t      td_server_submit_many(td_server_t* s, td_graph_t** graphs, td_op_t** roots, int64_t n,
+                                   int64_t* tickets);
+void         td_server_wait_many(td_server_t* s, const int64_t* tickets, int64_t n, td_t** results,
+                                 td_server_timing_t* timings);
 void         td_server_stats(td_server_t* s, td_server_stats_t* out);
 void         td_server_free(td_server_t* s);
 /* Device bytes a query may need beyond resident columns: uploads of columns

@@ -305,13 +305,38 @@ static float time_config(tdb_ctx* c, const tdg_batch_desc* d, int64_t tile, int3
     return best;
 }
 
+/* Shape classes already looked up in the tuner's file by this process
+ * (found or not), so a stream of one-off batches reads the file once per
+ * class; callers hold bcache_mu. */
+#define TUNE_MEMO 64
+static struct { char key[64]; int64_t tile; int32_t ctas; int found; } tmemo[TUNE_MEMO];
+static int n_tmemo;
+
 static void autotune(tdb_ctx* c, const tdg_batch_desc* d, int64_t* tile, int32_t* ctas, int once) {
     char key[128];
     tune_key(d, key, sizeof(key));
+    if (once) {
+        for (int i = 0; i < n_tmemo; i++)
+            if (!strcmp(tmemo[i].key, key)) {
+                *tile = tmemo[i].found ? tmemo[i].tile : 0;
+                *ctas = tmemo[i].found ? tmemo[i].ctas : 0;
+                return;
+            }
+        const int found = tdb_tune_load(key, tile, ctas);
+        if (!found) { *tile = 0; *ctas = 0; }
+        if (n_tmemo < TUNE_MEMO && strlen(key) < sizeof(tmemo[0].key)) {
+            snprintf(tmemo[n_tmemo].key, sizeof(tmemo[0].key), "%s", key);
+            tmemo[n_tmemo].tile = *tile;
+            tmemo[n_tmemo].ctas = *ctas;
+            tmemo[n_tmemo].found = found;
+            n_tmemo++;
+        }
+        return;                                    /* a one-off batch never times configurations */
+    }
     if (tdb_tune_load(key, tile, ctas)) return;
     *tile = 0;
     *ctas = 0;
-    if (once || getenv("TD_NO_AUTOTUNE")) return;   /* a one-off batch takes the defaults */
+    if (getenv("TD_NO_AUTOTUNE")) return;
     bchunk_t scratch;
     memset(&scratch, 0, sizeof(scratch));
     int64_t* d_rows = tdb_dev_alloc(c, 8);

@@ -99,9 +99,8 @@ static td_t* rows_of(td_t* b, int64_t r0, int64_t r1) {
     return t;
 }
 
-static void run_batch(td_graph_t** gs, td_op_t** rs, int64_t n, td_t** out) {
-    if (n == 1) { out[0] = td_execute(gs[0], rs[0]); return; }
-    td_t* b = tdb_execute_batch_once(gs, rs, n);
+/* The packed result b of n requests into one table per request (b released). */
+static void split_batch(td_t* b, td_graph_t** gs, td_op_t** rs, int64_t n, td_t** out) {
     if (TD_IS_ERR(b)) {
         /* a cancel ends them all; any other refusal runs them one by one */
         for (int64_t i = 0; i < n; i++) out[i] = TD_ERR_CODE(b) == TD_ERR_CANCEL ? b : td_execute(gs[i], rs[i]);
@@ -173,8 +172,21 @@ static void* worker_main(void* arg) {
         td_op_t* root0 = r->root;
         pthread_mutex_unlock(&s->mu);
 
-        if (sig) run_batch(gs, rs, nb, res);
-        td_t* one = sig ? NULL : td_execute(g0, root0);
+        td_t* one = NULL;
+        if (sig && nb > 1) {
+            td_t* b = tdb_execute_batch_once(gs, rs, nb);
+            /* the GPU is free: the next batch may start while this one's
+             * result is split into its requests' tables */
+            pthread_mutex_lock(&s->mu);
+            s->batch_running = 0;
+            pthread_cond_broadcast(&s->cv_work);
+            pthread_mutex_unlock(&s->mu);
+            split_batch(b, gs, rs, nb, res);
+        } else if (sig) {
+            res[0] = td_execute(g0, root0);
+        } else {
+            one = td_execute(g0, root0);
+        }
 
         pthread_mutex_lock(&s->mu);
         const int64_t end = now_ns();
@@ -187,7 +199,7 @@ static void* worker_main(void* arg) {
         }
         s->in_flight--;
         s->reserved -= est;
-        if (sig) s->batch_running = 0;
+        if (sig && nb == 1) s->batch_running = 0;   /* a packed batch cleared it when its launch ended */
         s->completed += (uint64_t)nb;
         pthread_cond_broadcast(&s->cv_done);
         pthread_cond_broadcast(&s->cv_work);
@@ -262,6 +274,26 @@ td_t* td_server_wait(td_server_t* s, int64_t ticket, td_server_timing_t* timing)
     r->result = NULL;
     pthread_mutex_unlock(&s->mu);
     return res;
+}
+
+int64_t td_server_submit_many(td_server_t* s, td_graph_t** graphs, td_op_t** roots, int64_t n, int64_t* tickets) {
+    if (!s || !graphs || !roots || !tickets || n < 0) return 0;
+    int64_t i = 0;
+    for (; i < n; i++) {
+        tickets[i] = td_server_submit(s, graphs[i], roots[i], 0);
+        if (tickets[i] < 0) break;
+    }
+    return i;
+}
+
+void td_server_wait_many(td_server_t* s, const int64_t* tickets, int64_t n, td_t** results,
+                         td_server_timing_t* timings) {
+    if (!s || !tickets) return;
+    for (int64_t i = 0; i < n; i++) {
+        td_t* r = td_server_wait(s, tickets[i], timings ? &timings[i] : NULL);
+        if (results) results[i] = r;
+        else if (r && !TD_IS_ERR(r)) td_release(r);
+    }
 }
 
 void td_server_stats(td_server_t* s, td_server_stats_t* out) {

@@ -240,3 +240,43 @@ def test_small_group_requests_are_batched(gpu):
         for t in tabs:
             gpu.lib.td_gpu_unpin(t)
             gpu.release(t)
+
+
+def test_submit_many_and_wait_many(gpu):
+    """td_server_submit_many / td_server_wait_many: one call for n requests
+    each way; every result equals td_execute alone."""
+    import ctypes as C
+    from teide_b200.td import OP_COUNT as CNT, OP_SUM as SM
+    L = gpu.lib
+    L.td_server_submit_many.restype = C.c_int64
+    L.td_server_submit_many.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
+    L.td_server_wait_many.restype = None
+    L.td_server_wait_many.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    r = np.random.default_rng(72)
+    datas = [{"key": r.integers(0, 500, 20_000, dtype=np.int64), "val": r.integers(-9, 9, 20_000, dtype=np.int64)}
+             for _ in range(24)]
+    tabs = [gpu.table(d) for d in datas]
+    graphs = [gpu.graph(t) for t in tabs]
+    roots = [g.group([g.scan("key")], [SM, CNT], [g.scan("val")] * 2) for g in graphs]
+    try:
+        n = len(graphs)
+        G = (C.c_void_p * n)(*[g.g for g in graphs])
+        R = (C.c_void_p * n)(*roots)
+        tickets = (C.c_int64 * n)()
+        results = (C.c_void_p * n)()
+        timings = (serve.Timing * n)()
+        with serve.Server(gpu, slots=4) as srv:
+            assert L.td_server_submit_many(srv.s, G, R, n, tickets) == n
+            L.td_server_wait_many(srv.s, tickets, n, results, timings)
+        for i in range(n):
+            assert timings[i].status == 0
+            got = gpu.table_dict(results[i])
+            gpu.release(results[i])
+            want = oracle.group({"key": datas[i]["key"]}, [(SM, "val", datas[i]["val"]), (CNT, "val", None)])
+            for k in want:
+                assert np.array_equal(got[k], want[k]), (i, k)
+    finally:
+        for g in graphs:
+            g.free()
+        for t in tabs:
+            gpu.release(t)
