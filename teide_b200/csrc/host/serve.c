@@ -99,6 +99,26 @@ static td_t* rows_of(td_t* b, int64_t r0, int64_t r1) {
     return t;
 }
 
+/* Requests [i0, i1) of a packed result, their rows [lo[i], lo[i + 1]). */
+typedef struct {
+    td_t*          b;
+    const int64_t* lo;
+    int64_t        i0, i1;
+    td_t**         out;
+} split_job_t;
+
+static void* split_range(void* arg) {
+    split_job_t* j = arg;
+    for (int64_t i = j->i0; i < j->i1; i++) j->out[i] = rows_of(j->b, j->lo[i], j->lo[i + 1]);
+    return NULL;
+}
+
+/* Host threads that split one packed result: building a request's table (the
+ * copy out of the packed columns and its allocations) is the served form's
+ * bound once the batch itself is on the GPU, and it parallelizes. */
+#define SPLIT_THREADS 4
+#define SPLIT_MIN_PER_THREAD 128
+
 /* The packed result b of n requests into one table per request (b released). */
 static void split_batch(td_t* b, td_graph_t** gs, td_op_t** rs, int64_t n, td_t** out) {
     if (TD_IS_ERR(b)) {
@@ -108,13 +128,34 @@ static void split_batch(td_t* b, td_graph_t** gs, td_op_t** rs, int64_t n, td_t*
     }
     const int64_t rows = td_table_ncols(b) > 0 ? td_table_get_col_idx(b, 0)->len : 0;
     const int64_t* q = rows ? (const int64_t*)td_data(td_table_get_col_idx(b, 0)) : NULL;
+    int64_t* lo = malloc(((size_t)n + 1) * sizeof(int64_t));
+    if (!lo) {
+        for (int64_t i = 0; i < n; i++) out[i] = TD_ERR_PTR(TD_ERR_OOM);
+        td_release(b);
+        return;
+    }
     int64_t r = 0;
     for (int64_t i = 0; i < n; i++) {
-        int64_t r1 = r;
-        while (r1 < rows && q[r1] == i) r1++;
-        out[i] = rows_of(b, r, r1);
-        r = r1;
+        lo[i] = r;
+        while (r < rows && q[r] == i) r++;
     }
+    lo[n] = r;
+    int nt = (int)(n / SPLIT_MIN_PER_THREAD);
+    if (nt < 1) nt = 1;
+    if (nt > SPLIT_THREADS) nt = SPLIT_THREADS;
+    split_job_t jobs[SPLIT_THREADS];
+    pthread_t th[SPLIT_THREADS];
+    int started[SPLIT_THREADS] = {0};
+    for (int t = 0; t < nt; t++) {
+        jobs[t] = (split_job_t){ b, lo, n * t / nt, n * (t + 1) / nt, out };
+        if (t > 0) started[t] = pthread_create(&th[t], NULL, split_range, &jobs[t]) == 0;
+    }
+    split_range(&jobs[0]);
+    for (int t = 1; t < nt; t++) {
+        if (started[t]) pthread_join(th[t], NULL);
+        else split_range(&jobs[t]);             /* no thread: this one does it */
+    }
+    free(lo);
     td_release(b);
 }
 
