@@ -636,7 +636,8 @@ def serve_small(td, L, n_queries=1024, slots=8, seed=6):
         return (max(t.end_ns for t in timings) - t0) / 1e9
 
     with serve.Server(td, slots=slots) as srv:
-        closed_loop(srv)                                # warm-up: batch plans
+        for _ in range(2):
+            closed_loop(srv)                            # warm-up: batch plans, host blocks
         closed = min(closed_loop(srv) for _ in range(3))
         rate = 0.5 * len(reqs) / closed
         r = np.random.default_rng(seed)
