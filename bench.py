@@ -593,8 +593,8 @@ def serve_small(td, L, n_queries=1024, slots=8, seed=6):
     log-uniform in [1K, 2M], 16 to 65536 keys), submitted to td_server at
     once (closed loop: one td_server_submit_many and one td_server_wait_many
     call) against the same requests run one td_execute after another; then
-    offered one by one from Python at half the served rate (open loop) for the
-    latency percentiles.  The server packs same-shape requests that wait behind each
+    offered one by one from Python (open loop) at half the served rate, at most
+    the one-at-a-time rate, for the latency percentiles.  The server packs same-shape requests that wait behind each
     other into td_execute_batch launches."""
     import numpy as np
     from teide_b200 import serve
@@ -639,7 +639,10 @@ def serve_small(td, L, n_queries=1024, slots=8, seed=6):
         for _ in range(2):
             closed_loop(srv)                            # warm-up: batch plans, host blocks
         closed = min(closed_loop(srv) for _ in range(3))
-        rate = 0.5 * len(reqs) / closed
+        # offered one by one from Python: at most the one-at-a-time rate (the
+        # load at which plain execution saturates; the Python client's own
+        # pacing falls behind from about 20K requests/s)
+        rate = min(0.5 * len(reqs) / closed, len(reqs) / plain_s)
         r = np.random.default_rng(seed)
         arrivals = np.cumsum(r.exponential(1.0 / rate, len(reqs)))
         for q, a in zip(reqs, arrivals):
