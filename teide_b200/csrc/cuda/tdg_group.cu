@@ -109,6 +109,7 @@ struct GroupK {
     int32_t W;                    // 8-byte words per global slot record
     int32_t hot_cap;              // hot slots a CTA caches (0: no cache)
     int32_t cps;                  // persistent CTAs per SM of the streaming kernel (0: all that fit)
+    int32_t rep0;                 // MODE 0: copies of the shared table, one per warp (kThreads / 32) or 1
     tdg_col key[TDG_MAX_KEYS];
     int64_t kmin[TDG_MAX_KEYS], krange[TDG_MAX_KEYS], stride[TDG_MAX_KEYS];
     int32_t op[TDG_MAX_AGGS];
@@ -330,9 +331,25 @@ __device__ SmemView smem_setup(const GroupK& G, unsigned long long* sm) {
     V.map_idx = nullptr;
     V.n_hot = 0;
     if (MODE == 0) {
+        // one copy of the table per warp when rep0 > 1: a few dozen slots
+        // updated by all 256 threads of a CTA otherwise serialize on the same
+        // shared addresses; the copies are summed at the flush
         V.cap = G.S;
-        V.cnt = (uint32_t*)sm;
-        V.acc = sm + ((G.S * 4 + 7) >> 3);
+        const size_t words = smem_full_bytes(G.S, G.n_acc) >> 3;
+        unsigned long long* base = sm + (G.rep0 > 1 ? (size_t)(threadIdx.x >> 5) * words : 0);
+        V.cnt = (uint32_t*)base;
+        V.acc = base + ((G.S * 4 + 7) >> 3);
+        if (G.rep0 > 1) {
+            for (int64_t i = threadIdx.x; i < (int64_t)G.rep0 * G.S; i += blockDim.x) {
+                unsigned long long* cb = sm + (size_t)(i / G.S) * words;
+                const int64_t k = i % G.S;
+                ((uint32_t*)cb)[k] = 0;
+                for (int a = 0; a < G.na; a++)
+                    if (G.ai[a] >= 0) (cb + ((G.S * 4 + 7) >> 3))[(int64_t)G.ai[a] * G.S + k] = acc_init_kind(G.kind[a]);
+            }
+            __syncthreads();
+            return V;
+        }
     } else {
         V.cap = G.hot_cap;
         if (!G.hot_cap) return V;
@@ -367,6 +384,39 @@ __device__ SmemView smem_setup(const GroupK& G, unsigned long long* sm) {
 template <int MODE>
 __device__ void smem_flush(const GroupK& G, const SmemView& V) {
     __syncthreads();
+    if (MODE == 0 && G.rep0 > 1) {
+        // the warps' copies summed per slot, then one merge into the record
+        extern __shared__ unsigned long long sm_base[];
+        const size_t words = smem_full_bytes(G.S, G.n_acc) >> 3;
+        for (int64_t s = threadIdx.x; s < G.S; s += blockDim.x) {
+            uint32_t c = 0;
+            for (int w = 0; w < G.rep0; w++) c += ((const uint32_t*)(sm_base + (size_t)w * words))[s];
+            if (!c) continue;
+            unsigned long long* r = grec(G, s);
+            atomicAdd(r, (unsigned long long)c);
+            for (int a = 0; a < G.na; a++) {
+                if (G.ai[a] < 0) continue;
+                const int kind = G.kind[a];
+                unsigned long long x = acc_init_kind(kind);
+                for (int w = 0; w < G.rep0; w++) {
+                    const unsigned long long y =
+                        (sm_base + (size_t)w * words + ((G.S * 4 + 7) >> 3))[(int64_t)G.ai[a] * G.S + s];
+                    switch (kind) {
+                        case K_SUM_F:
+                            x = (unsigned long long)__double_as_longlong(__longlong_as_double((long long)x) +
+                                                                         __longlong_as_double((long long)y));
+                            break;
+                        case K_SUM_I: x += y; break;
+                        case K_MIN_I: case K_MIN_F: if ((long long)y < (long long)x) x = y; break;
+                        case K_MAX_I: case K_MAX_F: if ((long long)y > (long long)x) x = y; break;
+                        default: break;
+                    }
+                }
+                merge(r + 1 + G.ai[a], kind, x);
+            }
+        }
+        return;
+    }
     const int64_t n = MODE == 0 ? G.S : V.n_hot;
     for (int64_t s = threadIdx.x; s < n; s += blockDim.x) {
         const uint32_t c = V.cnt[s];
@@ -1727,6 +1777,7 @@ static GroupK make_gk(const tdg_group_desc* d, const tdg_group_plan* p, void* ws
     GroupK G;
     memset(&G, 0, sizeof(G));
     G.cps = p->ctas_per_sm;
+    G.rep0 = p->smem && smem_full_bytes(p->n_slots, count_acc(d)) * (kThreads / 32) <= kSmemMax ? kThreads / 32 : 1;
     const int n_acc = count_acc(d);
     const bool sampled = group_sampled(d, p->method, p->smem != 0, p->n_slots, nrows_bound);
     const Layout L = layout_of(p->n_slots, n_acc, d->n_keys, p->method, sampled);
@@ -1892,7 +1943,7 @@ static bool group_w8(const GroupK& G, const Pred& P, const JoinK* J) {
 template <int PK, int MODE, bool JOIN, bool W8>
 static tdg_status launch_main(const GroupK& G, const Pred& P, const tdg_expr& prog, const JoinK& J, int64_t n,
                               cudaStream_t s) {
-    const size_t smem = MODE == 0 ? smem_full_bytes(G.S, G.n_acc) : (G.hot_cap ? smem_hot_bytes(G.hot_cap, G.n_acc) : 0);
+    const size_t smem = MODE == 0 ? smem_full_bytes(G.S, G.n_acc) * G.rep0 : (G.hot_cap ? smem_hot_bytes(G.hot_cap, G.n_acc) : 0);
     const void* fn = (const void*)k_group<PK, MODE, JOIN, W8>;
     const int g = grid_for(fn, kThreads, smem, (n + kItems - 1) / kItems);
     (note_launch(), k_group<PK, MODE, JOIN, W8><<<g, kThreads, smem, s>>>(G, P, prog, J, n));
@@ -1978,7 +2029,7 @@ static bool launch_group_vec(const GroupK& G, const Pred& P, int pk, int mode, i
     int nt, nc;
     if (!vec_plan(G, pk, P, A, &nt, &nc)) return false;
     if (mode == 1 && G.pk.P && G.hot_cap && A.ne <= G.pk.ne) mode = 3;
-    const size_t smem = mode == 0 ? smem_full_bytes(G.S, G.n_acc) : (G.hot_cap ? smem_hot_bytes(G.hot_cap, G.n_acc) : 0);
+    const size_t smem = mode == 0 ? smem_full_bytes(G.S, G.n_acc) * G.rep0 : (G.hot_cap ? smem_hot_bytes(G.hot_cap, G.n_acc) : 0);
     if (mode == 3) {
         const int64_t m_rows = n < kSampleRows ? n : kSampleRows;
         (note_launch(), k_part_plan<<<1, 1024, 0, s>>>(G, n, m_rows));
@@ -2123,7 +2174,7 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     const tdg_expr& prog = pred ? *pred : empty;
     const bool sm = p->smem != 0;
     const bool w8 = pk != 2 && group_w8(G, P, J);
-    const size_t smem = sm ? smem_full_bytes(G.S, G.n_acc) : 0;
+    const size_t smem = sm ? smem_full_bytes(G.S, G.n_acc) * G.rep0 : 0;
     set_prefetch(G, P, prog, pk, J);
     EventTimer tm;
     tm.start(s);
