@@ -730,7 +730,10 @@ __global__ void __launch_bounds__(kThreads) k_map_holes(const uint32_t* __restri
     if (__syncthreads_or(hole) && threadIdx.x == 0) atomicExch(dup, 1);
 }
 
-static void launch_payload_build(const GroupK& G, const JoinK& J, uint32_t* map, int64_t n_right, cudaStream_t s) {
+// Returns 1 when a plain-store build left its empty-entry check to the
+// caller (defer_holes: the vector probe scans the map as it starts), else 0.
+static int launch_payload_build(const GroupK& G, const JoinK& J, uint32_t* map, int64_t n_right, cudaStream_t s,
+                                bool defer_holes = false) {
     int gi = -1, nb = 0;
     for (int k = 0; k < G.nk; k++)
         if (G.key[k].side) { gi = k; nb++; }
@@ -749,6 +752,7 @@ static void launch_payload_build(const GroupK& G, const JoinK& J, uint32_t* map,
             (note_launch(), k_payload_build_vec<false><<<g, kThreads, 0, s>>>(
                 (const long long*)J.rkeys[0].data, (const long long*)G.key[gi].data, J.kmin, J.n_slots, G.kmin[gi],
                 G.krange[gi], G.stride[gi], map, n_right, G.err, G.err + 1));
+        if (store && defer_holes) return 1;
         if (store) {
             const int gh = grid_for((const void*)k_map_holes, kThreads, 0, (J.n_slots + 3) / 4);
             (note_launch(), k_map_holes<<<gh, kThreads, 0, s>>>(map, J.n_slots, G.err + 1));
@@ -757,6 +761,12 @@ static void launch_payload_build(const GroupK& G, const JoinK& J, uint32_t* map,
         const int g = grid_for((const void*)k_payload_build<uint32_t>, kThreads, 0, n_right);
         (note_launch(), k_payload_build<uint32_t><<<g, kThreads, 0, s>>>(G, J, map, n_right, G.err + 1));
     }
+    return 0;
+}
+
+static void launch_map_holes(const GroupK& G, const uint32_t* map, int64_t n_slots, cudaStream_t s) {
+    const int gh = grid_for((const void*)k_map_holes, kThreads, 0, (n_slots + 3) / 4);
+    (note_launch(), k_map_holes<<<gh, kThreads, 0, s>>>(map, n_slots, G.err + 1));
 }
 
 template <int PK, bool SMEM, typename PT, bool W8>
@@ -1105,8 +1115,23 @@ constexpr int kVecMinBlocks = 4;
 template <int NT, int NC, typename PT>
 __global__ void __launch_bounds__(kThreads, kVecMinBlocks) k_probe_vec(const GroupK G, const Pred P, const VecAgg A,
                                                                        const tdg_col lkey, int64_t kmin, int64_t n_map,
-                                                                       const PT* __restrict__ map, int64_t n) {
+                                                                       const PT* __restrict__ map, int64_t n,
+                                                                       int64_t holes) {
     extern __shared__ unsigned long long sm[];
+    if (holes) {
+        // a plain-store build's empty-entry check (k_map_holes' work) as the
+        // probe starts: the CTAs share the map (from L2) before streaming
+        bool hole = false;
+        const uint4* m4 = (const uint4*)map;
+        for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < (holes >> 2);
+             i += (int64_t)gridDim.x * blockDim.x) {
+            const uint4 v = m4[i];
+            hole |= v.x == 0xFFFFFFFFu || v.y == 0xFFFFFFFFu || v.z == 0xFFFFFFFFu || v.w == 0xFFFFFFFFu;
+        }
+        if (blockIdx.x == 0 && (int64_t)threadIdx.x < (holes & 3))
+            hole |= (uint32_t)map[((holes >> 2) << 2) + threadIdx.x] == 0xFFFFFFFFu;
+        if (__syncthreads_or(hole) && threadIdx.x == 0) atomicExch(G.err + 1, 1);
+    }
     const SmemView V = smem_setup<0>(G, sm);
     vec_stream<NT, NC, 0, true, PT>(G, V, P, A, lkey, kmin, n_map, map, n, evict_last_policy());
     smem_flush<0>(G, V);
@@ -2158,9 +2183,10 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     void* map = J->head;
     EventTimer tb;
     tb.start(s);
+    int holes_pending = 0;
     if (!prebuilt) {
         cudaMemsetAsync(map, 0xFF, (size_t)J->n_slots * 4, s);
-        if (n_right > 0) launch_payload_build(G, *J, (uint32_t*)map, n_right, s);
+        if (n_right > 0) holes_pending = launch_payload_build(G, *J, (uint32_t*)map, n_right, s, true);
     }
     tb.stop(s);
     st = launch_status();
@@ -2185,16 +2211,19 @@ tdg_status group_run_payload(const tdg_group_desc* d, const tdg_group_plan* p, v
     for (int k = 0; k < G.nk && vec; k++) vec = G.key[k].side == 1;
     vec = vec && vec_plan(G, pk, P, A, &nt, &nc);
     bool launched = false;
+    if (holes_pending && !vec) launch_map_holes(G, (const uint32_t*)map, J->n_slots, s);
+    const int64_t holes = holes_pending && vec ? J->n_slots : 0;
 #define TDG_PV(NTV, NCV)                                                                                  \
     if (vec && !launched && nt == NTV && nc == NCV) {                                                     \
         const int g = stream_grid((const void*)k_probe_vec<NTV, NCV, uint32_t>, kThreads, smem, (n_left + 3) / 4, \
                                   G.cps);                                                                 \
         (note_launch(), k_probe_vec<NTV, NCV, uint32_t><<<g, kThreads, smem, s>>>(G, P, A, J->lkeys[0], J->kmin, \
-                                                                                  J->n_slots, (const uint32_t*)map, n_left)); \
+                                                                                  J->n_slots, (const uint32_t*)map, n_left, holes)); \
         launched = true;                                                                                  \
     }
     TDG_PV(0, 0) TDG_PV(0, 1) TDG_PV(0, 2) TDG_PV(1, 1) TDG_PV(1, 2) TDG_PV(2, 1) TDG_PV(2, 2)
 #undef TDG_PV
+    if (!launched && holes) launch_map_holes(G, (const uint32_t*)map, J->n_slots, s);   // no vector form after all
 #define TDG_PL(PKV, SMV, PT, W)                                                                         \
     if (!launched && pk == PKV && sm == SMV && w8 == W) {                                                \
         const int g = grid_for((const void*)k_payload_probe<PKV, SMV, PT, W>, kThreads, smem,            \
