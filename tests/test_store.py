@@ -297,3 +297,33 @@ def test_read_splayed_maps_every_column(td, tmp_path):
         assert np.array_equal(got["k"], d["k"]) and np.array_equal(got["n"], d["n"])
     finally:
         td.release(t)
+
+
+def test_heap_reuses_blocks_across_threads(td):
+    """Freed small blocks are kept per size and handed out again (also to
+    other threads): vectors allocated, filled and released by four threads
+    at once keep their own contents."""
+    import threading
+    from teide_b200.td import I64
+    errors = []
+
+    def work(seed):
+        r = np.random.default_rng(seed)
+        for _ in range(300):
+            live = []
+            for _ in range(8):
+                n = int(r.integers(1, 20_000))
+                p, view = td.vec_alloc(I64, n)
+                view[:] = np.arange(n, dtype=np.int64) * seed
+                live.append((p, n))
+            for p, n in live:
+                if not np.array_equal(td.to_numpy(p), np.arange(n, dtype=np.int64) * seed):
+                    errors.append(seed)
+                td.release(p)
+
+    th = [threading.Thread(target=work, args=(s,)) for s in (3, 5, 7, 11)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errors
